@@ -1,0 +1,344 @@
+"""Benchmark: TreePM particle-updates/s on the 256³ clustered box (one GPU per rank).
+
+A step is one cosmological KDK step of every particle (leapfrog_cosmo_kdk_step
+of the reference + the periodic wrap): opening half kick, drift, one TreePM
+force evaluation (keys, sort, octree, short-range walk, PM), closing half kick.
+The fused step reuses the previous step's closing acceleration for its opening
+kick; the reference evaluates the force twice per step, and the JSON line also
+reports the per-force-evaluation rate.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload clustered256]
+  python bench.py --impl reference ...   # the CPU restatement of the reference
+
+Multi-GPU: independent replicas, one per rank (the force path has no
+exchange step on one box), so value = the particle-updates of all ranks / the
+slowest rank's time, and "scaling" is "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "gadget-ng_b200"))
+
+WORKLOADS = {
+    # name: (generator, mesh, a_start, a_end over 10 steps)
+    "clustered256": ("clustered_box_256", 256, 0.1, 0.12),
+    "treepm128": ("treepm_box_128", 128, 0.1, 0.12),
+    "clustered512": ("clustered_box_512", 512, 0.1, 0.12),
+    "pm64": ("pm_box_64", 64, 0.02, 0.0202),
+}
+FLOP_PER_INTERACTION = 37  # FMA = 2, MUFU = 1: the pair-kernel convention of the cost model
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def make_box(name):
+    from treepm import ics
+    gen, mesh, a0, a1 = WORKLOADS[name]
+    return getattr(ics, gen)(), mesh, a0, a1
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def profile_traffic(workload):
+    """DRAM bytes per walk launch from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(REPO, "profiles", "walk_traffic.json")) as f:
+            d = json.load(f)
+        return d.get(workload, {}).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_sample(box, mesh, phys, n_targets, threads):
+    """The oracle restatement on a bounded sample: full PM + full tree build +
+    the walk of n_targets seeded targets, extrapolated to all particles."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    oracle.build()
+    oracle.set_threads(threads)
+    pos = box.positions()
+    rng = np.random.default_rng(12345)
+    tg = np.sort(rng.choice(box.n, min(n_targets, box.n), replace=False))
+    r = oracle.treepm(pos, box.mass, phys["eps2"], phys["g"], mesh, box.box_size, phys["r_split"],
+                      phys["r_cut_factor"], targets=tg)
+    t_pm, t_build, t_walk, _ = (float(x) for x in r["times"])
+    t_force = t_pm + t_build + t_walk * box.n / len(tg)
+    return t_force, dict(pm_s=t_pm, build_s=t_build, walk_s=t_walk, targets=int(len(tg)), threads=threads)
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    box, mesh, a0, a1 = make_box(args.workload)
+    from treepm import ics
+    phys = ics.physics(box, mesh, a0)
+    threads = os.cpu_count() or 1
+    times = []
+    for i in range(args.warmup + args.steps):
+        t_force, info = cpu_sample(box, mesh, phys, args.cpu_targets, threads)
+        if i >= args.warmup:
+            times.append(2.0 * t_force)  # the reference evaluates the force twice per KDK step
+    step_s = float(np.mean(times))
+    value = box.n / step_s
+    line = {
+        "impl": "reference", "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": box.name, "particles": box.n, "mesh": mesh, "box_mpc_h": box.box_size,
+                   "r_s_cells": 1.25, "r_cut_over_r_s": 4.5},
+        "cpu_baseline": {"value": value, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+                         "sample": (f"oracle restatement (C++/OpenMP, FP64) of the reference TreePM: full CIC+FFT PM "
+                                    f"and full insertion-octree build over {box.n} particles, periodic walk of "
+                                    f"{info['targets']} seeded targets extrapolated to all; 2 force evaluations "
+                                    f"per KDK step as leapfrog.rs:79,86")},
+        "e2e": {"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def fp32_peak_tflops(lib_solver):
+    """FFMA throughput of this GPU, measured live (no FP32 figure is in MEASURED_PEAKS.json)."""
+    import torch
+    from treepm import _lib
+    L = _lib.load()
+    import ctypes
+    out = ctypes.c_double(0.0)
+    if L.tpm_fp32_peak(int(torch.cuda.current_device()), ctypes.byref(out)) != 0:
+        return None
+    return out.value
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    import treepm
+    from treepm import ics
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    box, mesh, a0, a1 = make_box(args.workload)
+    phys = ics.physics(box, mesh, a0)
+    n = box.n
+    solver = treepm.TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"],
+                                 device=local)
+    stream = torch.cuda.ExternalStream(solver.stream, device=torch.device("cuda", local))
+    # 10 steps from a0 to a1; the factors are float64 host integrals
+    dt = ics.time_between(a0, a1) / 10.0
+    a = a0
+    factors = []
+    for _ in range(args.warmup + args.steps + 1):
+        d, k1, k2 = treepm.drift_kick_factors(ics.OMEGA_M, ics.OMEGA_L, ics.H0_INTERNAL, a, dt)
+        factors.append((d, k1, k2, phys["G"] * a ** 3))
+        a = treepm.advance_a(ics.OMEGA_M, ics.OMEGA_L, ics.H0_INTERNAL, a, dt)
+
+    # ---- device-resident loop (value) -----------------------------------
+    solver.set_particles_fixed(box.q, box.mass)
+    for i in range(args.warmup):
+        d, k1, k2, g = factors[i]
+        solver.kdk_step(k1, d, k2, phys["eps2"], g)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    walk_ms, stats = [], []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for i in range(args.steps):
+            d, k1, k2, g = factors[args.warmup + i]
+            solver.kdk_step(k1, d, k2, phys["eps2"], g)
+            st = solver.stats()
+            stats.append(st)
+            walk_ms.append(st["ms_walk"])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    dev_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([dev_ms], device="cuda")
+    if world > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms = float(t.item())
+    ms_per_step = dev_ms / args.steps
+    value = world * n * args.steps / (dev_ms * 1e-3)
+
+    # ---- end to end through the host-buffer API (e2e) -------------------
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    vel = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    mass = torch.empty((n,), dtype=torch.float64, pin_memory=True).numpy()
+    pos[:] = box.positions()
+    vel[:] = 0.0
+    mass[:] = box.mass
+    d, k1, k2, g = factors[0]
+    solver.kdk_step_host(pos, vel, mass, k1, d, k2, phys["eps2"], g)  # warm
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(e2e_steps):
+        d, k1, k2, g = factors[1 + i]
+        solver.kdk_step_host(pos, vel, mass, k1, d, k2, phys["eps2"], g)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - t0
+    te = torch.tensor([e2e_wall], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * e2e_steps / float(te.item())
+    h2d = n * (24 + 24 + 8)
+    d2h = n * (24 + 24)
+
+    # ---- roofline of the dominant kernel (short-range walk) --------------
+    inter = float(np.mean([s["leaf_pairs"] + s["monopoles"] for s in stats]))
+    evaluated = float(np.mean([s["evaluated_pairs"] for s in stats]))
+    wms = float(np.mean(walk_ms))
+    achieved = inter * FLOP_PER_INTERACTION / (wms * 1e-3) / 1e12
+    peak = fp32_peak_tflops(solver)
+    st = stats[-1]
+    line = {
+        "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair arithmetic, int32 fixed-point positions, f64 decisions",
+        "data": "synthetic",
+        "config": {"workload": box.name, "particles": n, "mesh": mesh, "box_mpc_h": box.box_size,
+                   "r_s_cells": 1.25, "r_cut_over_r_s": 4.5, "softening": "mean spacing / 30",
+                   "a": [a0, a1], "parallelism": f"{world} independent replica(s)",
+                   "l2": "inputs larger than L2 (>= 0.8 GB touched per step)"},
+        "per_force_evaluation": {"value": value, "note": "one force evaluation per fused step; the reference "
+                                                         "evaluates twice per step"},
+        "stage_ms": {k: float(np.mean([s[k] for s in stats])) for k in
+                     ("ms_bbox_keys", "ms_sort", "ms_build", "ms_walk", "ms_pm", "ms_gather_kick", "ms_total")},
+        "walk": {"interactions_per_step": inter, "evaluated_pairs_per_step": evaluated,
+                 "interactions_per_particle": inter / n, "exact_fallbacks": st["exact_fallbacks"],
+                 "tree_nodes": st["n_tree_nodes"], "groups": st["n_groups"], "max_depth": st["max_tree_depth"]},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": (achieved / peak) if peak else None, "traffic": profile_traffic(box.name),
+                     "kernel": "k_walk (short-range erfc walk)",
+                     "note": f"{FLOP_PER_INTERACTION} FLOP per reference interaction (leaf pair or monopole); "
+                             "peak = FFMA throughput measured live on this GPU"},
+        "e2e": {"value": e2e_value, "unit": "particle-updates/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "path": "tpm_kdk_step_host: float64 positions, velocities and masses from pinned host memory, "
+                        "two force evaluations (no cached acceleration across calls), state back to host"},
+        "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        t_force, info = cpu_sample(box, mesh, phys, args.cpu_targets, os.cpu_count() or 1)
+        cv = n / (2.0 * t_force)
+        line["cpu_baseline"] = {"value": cv, "unit": "particle-updates/s", "cores": info["threads"], "kind": "port",
+                                "sample": (f"oracle restatement (C++/OpenMP, FP64): full PM + full octree build, "
+                                           f"walk of {info['targets']} targets extrapolated; 2 force evaluations "
+                                           f"per step; stages s: pm {info['pm_s']:.2f}, build {info['build_s']:.2f}, "
+                                           f"walk-sample {info['walk_s']:.2f}")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del stream
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="clustered256", choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-targets", type=int, default=65536)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

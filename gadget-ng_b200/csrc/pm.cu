@@ -1,0 +1,446 @@
+// Long-range PM on the device.
+//
+// Reference path: cic::assign (crates/gadget-ng-pm/src/cic.rs:37-93, :260-292)
+// -> fft_poisson::solve_forces_filtered (fft_poisson.rs:87-103, :306-476) ->
+// cic::interpolate (cic.rs:100-170, :298-346).
+//
+// The reference transforms a complex copy of the real density with three
+// passes of 1D c2c FFTs (x, y, z), multiplies by -4 pi G W(k)/k^2, forms
+// F_a = -i k_a phi, transforms back (z, y, x) and keeps the real part / N^3.
+// Here the density is real, so only the kx in [0, N/2] half spectrum is
+// carried (the other half is its conjugate): an x pass real -> half spectrum,
+// a y pass, one kernel that does the forward z pass, the Green's function,
+// the filter and the gradient for all three components and their inverse z
+// passes without leaving shared memory, then inverse y and x passes back to
+// three real force meshes.  Taking the real part in the reference zeroes the
+// derivative's Nyquist plane (F_x at kx = N/2 and so on); the derivative table
+// is zero there, so the half spectrum is exactly Hermitian.  Every 1D
+// transform is a radix-2 Stockham autosort FFT in shared memory.  Linear in G:
+// the meshes hold forces per unit G, the gather multiplies by g.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "pm.cuh"
+
+namespace tpm {
+namespace {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// Batched radix-2 Stockham FFT in shared memory.  ROWMAJOR: element (j, c) at
+// a[c * n + j]; otherwise at a[j * cols + c].  Returns the buffer holding the
+// result (a or b).
+template <bool ROWMAJOR>
+__device__ float2* fft_smem(float2* a, float2* b, int n, int logn, int cols, const float2* tw, bool inv) {
+  const int half = n >> 1;
+  const int total = half * cols;
+  int Ns = 1;
+  for (int s = 0; s < logn; ++s, Ns <<= 1) {
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      int j, c;
+      if (ROWMAJOR) {
+        j = idx & (half - 1);
+        c = idx >> (logn - 1);
+      } else {
+        c = idx % cols;
+        j = idx / cols;
+      }
+      const int k = j & (Ns - 1);
+      float2 w = tw[k << (logn - 1 - s)];
+      if (inv) w.y = -w.y;
+      float2 x0, x1;
+      if (ROWMAJOR) {
+        x0 = a[c * n + j];
+        x1 = a[c * n + j + half];
+      } else {
+        x0 = a[j * cols + c];
+        x1 = a[(j + half) * cols + c];
+      }
+      const float2 t = cmul(x1, w);
+      const int o = ((j - k) << 1) + k;
+      if (ROWMAJOR) {
+        b[c * n + o] = cadd(x0, t);
+        b[c * n + o + Ns] = csub(x0, t);
+      } else {
+        b[o * cols + c] = cadd(x0, t);
+        b[(o + Ns) * cols + c] = csub(x0, t);
+      }
+    }
+    __syncthreads();
+    float2* t = a;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+__device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* tw, int n) {
+  for (int i = threadIdx.x; i < (n >> 1); i += blockDim.x) s_tw[i] = tw[i];
+}
+
+// ---- CIC deposit (cic.rs:37-93) ------------------------------------------------
+struct Cic {
+  int ix[2], iy[2], iz[2];
+  float wx[2], wy[2], wz[2];
+};
+
+__device__ __forceinline__ void cic_axis(uint32_t q, double scale, double inv_cell, double nmf, int nm, int* i,
+                                         float* w) {
+  const double c = rem_euclid(dmul(decode(q, scale), inv_cell), nmf);
+  const double f = floor(c);
+  const int i0 = (int)f;
+  const double d = dsub(c, f);
+  i[0] = i0;
+  i[1] = (i0 + 1) % nm;
+  w[0] = (float)dsub(1.0, d);
+  w[1] = (float)d;
+}
+
+__device__ __forceinline__ Cic cic_of(uint32_t qx, uint32_t qy, uint32_t qz, double scale, double inv_cell, int nm) {
+  Cic c;
+  const double nmf = (double)nm;
+  cic_axis(qx, scale, inv_cell, nmf, nm, c.ix, c.wx);
+  cic_axis(qy, scale, inv_cell, nmf, nm, c.iy, c.wy);
+  cic_axis(qz, scale, inv_cell, nmf, nm, c.iz, c.wz);
+  return c;
+}
+
+__global__ void k_deposit(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                          const uint32_t* __restrict__ qz, const float* __restrict__ m, int64_t n, double scale,
+                          double inv_cell, int nm, float* __restrict__ rho) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Cic c = cic_of(qx[i], qy[i], qz[i], scale, inv_cell, nm);
+  const float mi = m[i];
+  const int64_t nm2 = (int64_t)nm * nm;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int d = 0; d < 2; ++d)
+        atomicAdd(&rho[c.iz[a] * nm2 + (int64_t)c.iy[b] * nm + c.ix[d]], mi * c.wx[d] * c.wy[b] * c.wz[a]);
+}
+
+__global__ void k_cells(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                        const uint32_t* __restrict__ qz, const uint32_t* __restrict__ id, int64_t n, double scale,
+                        double inv_cell, int nm, int32_t* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Cic c = cic_of(qx[i], qy[i], qz[i], scale, inv_cell, nm);
+  const int64_t o = 3 * (int64_t)id[i];
+  out[o] = c.ix[0];
+  out[o + 1] = c.iy[0];
+  out[o + 2] = c.iz[0];
+}
+
+// ---- x pass: real rows -> half spectrum ----------------------------------------
+__global__ void k_fft_x_r2c(const float* __restrict__ rho, float2* __restrict__ spec, int nm, int logn, int nh,
+                            int rows, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  float2* s_tw = sm;
+  float2* a = sm + (nm >> 1);
+  float2* b = a + rows * nm;
+  load_twiddles(s_tw, tw, nm);
+  const int64_t row0 = (int64_t)blockIdx.x * rows;
+  for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
+    const int r = idx / nm, j = idx % nm;
+    a[idx] = make_float2(rho[(row0 + r) * nm + j], 0.f);
+  }
+  __syncthreads();
+  const float2* res = fft_smem<true>(a, b, nm, logn, rows, s_tw, false);
+  for (int idx = threadIdx.x; idx < rows * nh; idx += blockDim.x) {
+    const int r = idx / nh, k = idx % nh;
+    spec[(row0 + r) * nh + k] = res[r * nm + k];
+  }
+}
+
+// ---- y pass (c2c) on [z][y][kx] half spectra, one component per blockIdx.z --------
+__global__ void k_fft_y(float2* __restrict__ spec, int64_t comp_stride, int nm, int logn, int nh, int tx,
+                        const float2* __restrict__ tw, int inv) {
+  extern __shared__ float2 sm[];
+  float2* s_tw = sm;
+  float2* a = sm + (nm >> 1);
+  float2* b = a + nm * tx;
+  load_twiddles(s_tw, tw, nm);
+  const int kx0 = blockIdx.x * tx, z = blockIdx.y;
+  float2* base = spec + blockIdx.z * comp_stride + (int64_t)z * nm * nh;
+  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+    const int y = idx / tx, c = idx % tx;
+    a[idx] = (kx0 + c < nh) ? base[(int64_t)y * nh + kx0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* res = fft_smem<false>(a, b, nm, logn, tx, s_tw, inv != 0);
+  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+    const int y = idx / tx, c = idx % tx;
+    if (kx0 + c < nh) base[(int64_t)y * nh + kx0 + c] = res[idx];
+  }
+}
+
+// ---- z pass + Green's function x filter x gradient + inverse z pass ---------------
+__global__ void k_fft_z_poisson(const float2* __restrict__ spec, float2* __restrict__ spec3, int nm, int logn,
+                                int nh, int tx, const float2* __restrict__ tw, const float* __restrict__ kval,
+                                const float* __restrict__ kfilter, const float* __restrict__ kderiv, float kcoef) {
+  extern __shared__ float2 sm[];
+  float2* s_tw = sm;
+  float2* a = sm + (nm >> 1);
+  float2* b = a + nm * tx;
+  float2* c3 = b + nm * tx;
+  load_twiddles(s_tw, tw, nm);
+  const int kx0 = blockIdx.x * tx, y = blockIdx.y;
+  const int64_t plane = (int64_t)nm * nh;
+  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+    const int z = idx / tx, c = idx % tx;
+    a[idx] = (kx0 + c < nh) ? spec[z * plane + (int64_t)y * nh + kx0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2* rho_k = fft_smem<false>(a, b, nm, logn, tx, s_tw, false);
+  float2* spare = rho_k == a ? b : a;
+  // phi(k) = rho(k) * kcoef * W(k) / k^2 ; F_a = -i D_a phi
+  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+    const int z = idx / tx, c = idx % tx;
+    const int kx = kx0 + c;
+    float2 v = make_float2(0.f, 0.f);
+    if (kx < nh) {
+      const float k2 = kval[kx] * kval[kx] + kval[y] * kval[y] + kval[z] * kval[z];
+      if (k2 > 0.f) {
+        const float s = kcoef * kfilter[kx] * kfilter[y] * kfilter[z] / k2;
+        v = make_float2(rho_k[idx].x * s, rho_k[idx].y * s);
+      }
+    }
+    rho_k[idx] = v;  // phi
+  }
+  __syncthreads();
+  for (int comp = 0; comp < 3; ++comp) {
+    for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+      const int z = idx / tx, c = idx % tx;
+      const int kx = kx0 + c < nh ? kx0 + c : 0;
+      const float d = comp == 0 ? kderiv[kx] : (comp == 1 ? kderiv[y] : kderiv[z]);
+      const float2 ph = rho_k[idx];
+      c3[idx] = make_float2(d * ph.y, -d * ph.x);
+    }
+    __syncthreads();
+    const float2* res = fft_smem<false>(c3, spare, nm, logn, tx, s_tw, true);
+    float2* out = spec3 + comp * (int64_t)nm * plane;
+    for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+      const int z = idx / tx, c = idx % tx;
+      if (kx0 + c < nh) out[z * plane + (int64_t)y * nh + kx0 + c] = res[idx];
+    }
+    __syncthreads();
+    if (res == spare) {  // keep c3 as the scratch input of the next component
+      float2* t = spare;
+      spare = c3;
+      c3 = t;
+    }
+  }
+}
+
+// ---- inverse x pass: half spectrum rows -> real rows -------------------------------
+__global__ void k_fft_x_c2r(const float2* __restrict__ spec3, float* __restrict__ force, int nm, int logn, int nh,
+                            int rows, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  float2* s_tw = sm;
+  float2* a = sm + (nm >> 1);
+  float2* b = a + rows * nm;
+  load_twiddles(s_tw, tw, nm);
+  const int comp = blockIdx.y;
+  const int64_t nrows = (int64_t)nm * nm;
+  const float2* in = spec3 + comp * nrows * nh;
+  float* out = force + comp * nrows * nm;
+  const int64_t row0 = (int64_t)blockIdx.x * rows;
+  for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
+    const int r = idx / nm, k = idx % nm;
+    float2 v;
+    if (k < nh) v = in[(row0 + r) * nh + k];
+    else {
+      v = in[(row0 + r) * nh + (nm - k)];
+      v.y = -v.y;
+    }
+    a[idx] = v;
+  }
+  __syncthreads();
+  const float2* res = fft_smem<true>(a, b, nm, logn, rows, s_tw, true);
+  for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
+    const int r = idx / nm, j = idx % nm;
+    out[(row0 + r) * nm + j] = res[idx].x;
+  }
+}
+
+// ---- gather (cic.rs:100-170) fused with the sum LR + SR and the kick -------------
+__global__ void k_gather_kick(GatherArgs a, const float* __restrict__ fx, const float* __restrict__ fy,
+                              const float* __restrict__ fz, double scale, double inv_cell, int nm) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const Cic c = cic_of(a.qx[i], a.qy[i], a.qz[i], scale, inv_cell, nm);
+  const int64_t nm2 = (int64_t)nm * nm;
+  float lx = 0.f, ly = 0.f, lz = 0.f;
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const float wt = c.wx[w] * c.wy[v] * c.wz[u];
+        const int64_t idx = c.iz[u] * nm2 + (int64_t)c.iy[v] * nm + c.ix[w];
+        lx = fmaf(fx[idx], wt, lx);
+        ly = fmaf(fy[idx], wt, ly);
+        lz = fmaf(fz[idx], wt, lz);
+      }
+  const float g = (float)a.g;
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+  if (a.srx) {
+    sx = a.srx[i];
+    sy = a.sry[i];
+    sz = a.srz[i];
+  }
+  const float tx = g * (lx + sx), ty = g * (ly + sy), tz = g * (lz + sz);
+  a.ax[i] = tx;
+  a.ay[i] = ty;
+  a.az[i] = tz;
+  if (a.lrx) {
+    a.lrx[i] = g * lx;
+    a.lry[i] = g * ly;
+    a.lrz[i] = g * lz;
+  }
+  if (a.vx) {
+    const float k = (float)a.kick;
+    a.vx[i] = fmaf(tx, k, a.vx[i]);
+    a.vy[i] = fmaf(ty, k, a.vy[i]);
+    a.vz[i] = fmaf(tz, k, a.vz[i]);
+  }
+}
+
+inline int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+inline int rows_for(int nm) { return nm >= 4096 ? 1 : 4096 / nm; }
+inline int tx_for(int nm) {
+  int t = 4096 / nm;
+  return t < 4 ? 4 : (t > 16 ? 16 : t);
+}
+
+}  // namespace
+
+void pm_plan_init(PmPlan& p, int nm, double box, double r_split, uint32_t flags, int device) {
+  (void)device;
+  p.nm = nm;
+  p.logn = ilog2(nm);
+  p.nh = nm / 2 + 1;
+  p.box = box;
+  const int64_t nm3 = (int64_t)nm * nm * nm;
+  const int64_t nspec = (int64_t)nm * nm * p.nh;
+  std::vector<float2> tw(nm / 2);
+  for (int m = 0; m < nm / 2; ++m) {
+    const double ang = -2.0 * M_PI * (double)m / (double)nm;
+    tw[m] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+  }
+  // float64 tables: k = 2 pi n / L with n = freq_index (fft_poisson.rs:724-730)
+  const double dk = 2.0 * M_PI / box, cell = box / nm;
+  std::vector<float> kval(nm), kfil(nm), kder(nm);
+  for (int i = 0; i < nm; ++i) {
+    const int64_t f = i <= nm / 2 ? i : (int64_t)i - nm;
+    const double k = dk * (double)f;
+    kval[i] = (float)k;
+    double fil = 1.0;
+    if (r_split > 0.0) fil *= std::exp(-0.5 * k * k * r_split * r_split);  // per-axis factor of exp(-k^2 r_s^2 / 2)
+    if (flags & 2u) {  // CIC deconvolution: divide by W_cic^2 = prod sinc^4
+      const double h = 0.5 * k * cell;
+      const double sn = i == 0 ? 1.0 : std::sin(h) / h;
+      fil /= (sn * sn) * (sn * sn);
+    }
+    kfil[i] = (float)fil;
+    double d = k;
+    if (flags & 4u) d = (8.0 * std::sin(k * cell) - std::sin(2.0 * k * cell)) / (6.0 * cell);
+    if (i == nm / 2) d = 0.0;  // the real part of the reference's c2c inverse drops it
+    kder[i] = (float)d;
+  }
+  const double vcell = cell * (cell * cell);
+  p.kcoef = (float)(-4.0 * M_PI / vcell / (double)nm3);
+  TPM_CUDA(cudaMalloc(&p.twiddle, sizeof(float2) * (nm / 2)));
+  TPM_CUDA(cudaMalloc(&p.kval, sizeof(float) * nm));
+  TPM_CUDA(cudaMalloc(&p.kfilter, sizeof(float) * nm));
+  TPM_CUDA(cudaMalloc(&p.kderiv, sizeof(float) * nm));
+  TPM_CUDA(cudaMalloc(&p.rho, sizeof(float) * nm3));
+  TPM_CUDA(cudaMalloc(&p.spec, sizeof(float2) * nspec));
+  TPM_CUDA(cudaMalloc(&p.spec3, sizeof(float2) * nspec * 3));
+  TPM_CUDA(cudaMalloc(&p.force, sizeof(float) * nm3 * 3));
+  TPM_CUDA(cudaMemcpy(p.twiddle, tw.data(), sizeof(float2) * (nm / 2), cudaMemcpyHostToDevice));
+  TPM_CUDA(cudaMemcpy(p.kval, kval.data(), sizeof(float) * nm, cudaMemcpyHostToDevice));
+  TPM_CUDA(cudaMemcpy(p.kfilter, kfil.data(), sizeof(float) * nm, cudaMemcpyHostToDevice));
+  TPM_CUDA(cudaMemcpy(p.kderiv, kder.data(), sizeof(float) * nm, cudaMemcpyHostToDevice));
+  // shared-memory opt-in for the largest variants
+  const int big = 227 * 1024;
+  TPM_CUDA(cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TPM_CUDA(cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TPM_CUDA(cudaFuncSetAttribute(k_fft_z_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  TPM_CUDA(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+}
+
+void pm_plan_free(PmPlan& p) {
+  cudaFree(p.twiddle);
+  cudaFree(p.kval);
+  cudaFree(p.kfilter);
+  cudaFree(p.kderiv);
+  cudaFree(p.rho);
+  cudaFree(p.spec);
+  cudaFree(p.spec3);
+  cudaFree(p.force);
+  p = PmPlan();
+}
+
+void pm_deposit(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const float* massf,
+                int64_t n, cudaStream_t s) {
+  const int64_t nm3 = (int64_t)p.nm * p.nm * p.nm;
+  TPM_CUDA(cudaMemsetAsync(p.rho, 0, sizeof(float) * nm3, s));
+  if (n == 0) return;
+  k_deposit<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, massf, n, p.box / TWO32, (double)p.nm / p.box,
+                                                        p.nm, p.rho);
+  TPM_LAUNCH_CHECK();
+}
+
+void pm_solve(const PmPlan& p, cudaStream_t s) {
+  const int nm = p.nm, nh = p.nh, logn = p.logn;
+  const int rows = rows_for(nm), tx = tx_for(nm);
+  const int64_t nrows = (int64_t)nm * nm;
+  const size_t sm_x = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)rows * nm);
+  const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
+  const size_t sm_z = sizeof(float2) * ((size_t)(nm / 2) + 3 * (size_t)nm * tx);
+  const int nblk_x = (int)((nrows + rows - 1) / rows);
+  const int ntx = (nh + tx - 1) / tx;
+  k_fft_x_r2c<<<nblk_x, 256, sm_x, s>>>(p.rho, p.spec, nm, logn, nh, rows, p.twiddle);
+  TPM_LAUNCH_CHECK();
+  k_fft_y<<<dim3(ntx, nm, 1), 256, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
+  TPM_LAUNCH_CHECK();
+  k_fft_z_poisson<<<dim3(ntx, nm), 256, sm_z, s>>>(p.spec, p.spec3, nm, logn, nh, tx, p.twiddle, p.kval, p.kfilter,
+                                                   p.kderiv, p.kcoef);
+  TPM_LAUNCH_CHECK();
+  k_fft_y<<<dim3(ntx, nm, 3), 256, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
+  TPM_LAUNCH_CHECK();
+  k_fft_x_c2r<<<dim3(nblk_x, 3), 256, sm_x, s>>>(p.spec3, p.force, nm, logn, nh, rows, p.twiddle);
+  TPM_LAUNCH_CHECK();
+}
+
+void pm_gather_kick(const PmPlan& p, const GatherArgs& a, cudaStream_t s) {
+  if (a.n == 0) return;
+  const int64_t nm3 = (int64_t)p.nm * p.nm * p.nm;
+  k_gather_kick<<<grid_for(a.n, 256, 1ll << 30), 256, 0, s>>>(a, p.force, p.force + nm3, p.force + 2 * nm3,
+                                                              p.box / TWO32, (double)p.nm / p.box, p.nm);
+  TPM_LAUNCH_CHECK();
+}
+
+void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const uint32_t* id,
+              int64_t n, int32_t* cells_by_id, cudaStream_t s) {
+  if (n == 0) return;
+  k_cells<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, id, n, p.box / TWO32, (double)p.nm / p.box, p.nm,
+                                                      cells_by_id);
+  TPM_LAUNCH_CHECK();
+}
+
+}  // namespace tpm

@@ -1,0 +1,55 @@
+// Long-range PM: CIC deposit, 3D FFT Poisson solve with the Gaussian
+// long-range filter and spectral gradient, CIC gather fused with the kick.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tpm {
+
+struct PmPlan {
+  int nm = 0, logn = 0, nh = 0;
+  double box = 0.0;
+  float2* twiddle = nullptr;  // e^{-2 pi i m / nm}, m < nm/2
+  float* kfilter = nullptr;   // per-axis factor of the filter (and CIC deconvolution)
+  float* kderiv = nullptr;    // per-axis derivative (exact i k or 4-point), 0 at Nyquist
+  float* kval = nullptr;      // per-axis wavenumber k (for k^2)
+  float* rho = nullptr;       // nm^3 real, mass per cell
+  float2* spec = nullptr;     // nm*nm*nh complex work array
+  float2* spec3 = nullptr;    // 3 x nm*nm*nh
+  float* force = nullptr;     // 3 x nm^3 real, per unit G
+  float kcoef = 0.f;          // -4 pi / V_cell / N^3
+};
+
+// Build tables for mesh nm, box L, split r_s (<= 0: no filter), flags.
+void pm_plan_init(PmPlan& p, int nm, double box, double r_split, uint32_t flags, int device);
+void pm_plan_free(PmPlan& p);
+
+struct GatherArgs {
+  int64_t n;
+  const uint32_t* qx;
+  const uint32_t* qy;
+  const uint32_t* qz;
+  const float* srx;  // short range (physical, per unit G); may be null
+  const float* sry;
+  const float* srz;
+  float* ax;  // total acceleration out
+  float* ay;
+  float* az;
+  float* lrx;  // long-range part out (optional)
+  float* lry;
+  float* lrz;
+  float* vx;  // kick target (optional)
+  float* vy;
+  float* vz;
+  double g;
+  double kick;
+};
+
+void pm_deposit(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const float* massf,
+                int64_t n, cudaStream_t s);
+void pm_solve(const PmPlan& p, cudaStream_t s);
+void pm_gather_kick(const PmPlan& p, const GatherArgs& a, cudaStream_t s);
+void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const uint32_t* id,
+              int64_t n, int32_t* cells_by_id, cudaStream_t s);
+
+}  // namespace tpm

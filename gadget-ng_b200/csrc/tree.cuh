@@ -1,0 +1,96 @@
+// Octree of the insertion algorithm of crates/gadget-ng-tree/src/octree.rs,
+// rebuilt in parallel from sorted octant-path keys.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tpm {
+
+constexpr uint32_t LEAF_BIT = 0x80000000u;
+constexpr uint32_t EMPTY_SLOT = 0xFFFFFFFFu;
+constexpr int KEY_LEVELS = 42;  // 21 octant digits in each of two 64-bit words
+
+// Geometry of one force evaluation, computed on the device.
+struct TreeParams {
+  double center[3];  // bounding_cube centre (octree.rs:1306-1332)
+  double half;       // bounding_cube half side, padded
+  double hlo[3];     // Hilbert normalisation origin (sfc.rs:187-204)
+  double hlen[3];    // Hilbert normalisation extent
+  uint32_t qmin[3], qmax[3];
+};
+
+// Particle arrays (structure of arrays, current storage order).
+struct Particles {
+  uint32_t* qx;
+  uint32_t* qy;
+  uint32_t* qz;
+  float* vx;
+  float* vy;
+  float* vz;
+  double* mass;
+  float* massf;
+  uint32_t* id;  // original index
+};
+
+struct TreeBuffers {
+  // keys (sorted order after the sort)
+  uint64_t* key_hi;
+  uint64_t* key_lo;      // by storage index before the permutation, sorted after
+  uint64_t* key_lo_tmp;
+  uint32_t* perm;
+  // binary radix tree over the sorted keys (n - 1 internal nodes)
+  uint32_t* bin_left;
+  uint32_t* bin_right;
+  int32_t* bin_prefix;
+  uint32_t* bin_first;
+  uint32_t* bin_last;
+  int32_t* bin_parent;
+  int32_t* leaf_bparent;
+  uint32_t* oct_count;
+  uint32_t* oct_base;
+  // octree internal nodes
+  int64_t cap_int;
+  int32_t* o_parent;
+  uint8_t* o_depth;
+  uint32_t* o_first;
+  uint32_t* o_last;
+  uint32_t* o_slots;  // 8 per node, EMPTY_SLOT or child id (LEAF_BIT | particle)
+  uint32_t* o_nchild;
+  uint32_t* o_child_first;
+  uint32_t* o_cnt;
+  uint32_t* child_ids;  // compacted, same encoding as o_slots
+  double* o_mass;
+  double* o_com;   // 3 per node
+  double* o_quad;  // 6 per node
+  uint4* o_walk;   // fixed-point COM (x, y, z) and float mass bits
+  // leaves
+  int32_t* leaf_oparent;
+  uint8_t* leaf_depth;
+  // walk groups
+  uint32_t* grp_count_per_node;
+  uint32_t* grp_base;
+  uint32_t* grp_first;
+  uint32_t* grp_size;
+  int64_t cap_groups;
+  // params and scalars
+  TreeParams* params;
+  uint32_t* bbox;       // 6 words
+  uint32_t* scalars;    // [0] octree internal count, [1] groups, [2] max depth, [3] child total
+  uint32_t* err;
+};
+
+void launch_bbox_root(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s);
+void launch_tree_keys(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s);
+void launch_fix_ties(int64_t n, TreeBuffers& t, cudaStream_t s);
+void launch_permute(const Particles& src, const Particles& dst, int64_t n, const uint32_t* perm, cudaStream_t s);
+void launch_karras(int64_t n, TreeBuffers& t, cudaStream_t s);
+void launch_octree_nodes(int64_t n, TreeBuffers& t, cudaStream_t s);
+void launch_octree_links(int64_t n, int64_t n_int, TreeBuffers& t, void* scan_scratch, cudaStream_t s);
+void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, TreeBuffers& t, cudaStream_t s);
+void launch_groups(int64_t n, int64_t n_int, int group_max, TreeBuffers& t, void* scan_scratch, cudaStream_t s);
+void launch_hilbert_keys(const Particles& p, int64_t n, double box, const TreeParams* prm, uint64_t* keys,
+                         uint32_t* vals, cudaStream_t s);
+void launch_export_paths(int64_t n, int64_t n_int, const TreeBuffers& t, uint64_t* node_hi, uint64_t* node_lo,
+                         uint64_t* leaf_hi, uint64_t* leaf_lo, cudaStream_t s);
+
+}  // namespace tpm

@@ -1,0 +1,953 @@
+// Host orchestration of one TreePM force evaluation and the C ABI.
+//
+// One handle = one solver (TreePmSolver / PmSolver of the reference) on one
+// device and one stream, with device-resident particle state.  A force
+// evaluation runs: bounding box -> octant-path keys -> radix sort -> particle
+// permutation -> radix tree -> octree -> bit-exact moments -> walk groups ->
+// short-range walk -> CIC deposit -> FFT Poisson -> gather (+ kick).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/treepm_b200.h"
+#include "common.cuh"
+#include "pm.cuh"
+#include "scan.cuh"
+#include "sort.cuh"
+#include "tree.cuh"
+#include "walk.cuh"
+
+namespace tpm {
+thread_local unsigned long long g_kernel_launches = 0;
+}
+
+using namespace tpm;
+
+namespace {
+
+constexpr int GROUP_MAX = 32;
+constexpr int STACK_CAP = 2048;
+constexpr uint32_t DEFERRED_CAP = 1u << 16;
+
+__global__ void k_encode(const double* __restrict__ pos, const double* __restrict__ vel,
+                         const double* __restrict__ mass, int64_t n, double box, Particles p,
+                         uint32_t* __restrict__ err) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t q[3];
+  for (int d = 0; d < 3; ++d) {
+    const double x = pos[3 * i + d];
+    if (!isfinite(x)) atomicOr(err, DEV_ERR_NONFINITE);
+    double u = x / box;
+    u = u - floor(u);
+    q[d] = (uint32_t)((unsigned long long)llrint(u * TWO32) & 0xFFFFFFFFull);
+  }
+  p.qx[i] = q[0];
+  p.qy[i] = q[1];
+  p.qz[i] = q[2];
+  p.vx[i] = vel ? (float)vel[3 * i] : 0.f;
+  p.vy[i] = vel ? (float)vel[3 * i + 1] : 0.f;
+  p.vz[i] = vel ? (float)vel[3 * i + 2] : 0.f;
+  const double m = mass[i];
+  if (!isfinite(m)) atomicOr(err, DEV_ERR_NONFINITE);
+  p.mass[i] = m;
+  p.massf[i] = (float)m;
+  p.id[i] = (uint32_t)i;
+}
+
+__global__ void k_decode_state(Particles p, int64_t n, double scale, const float* ax, const float* ay,
+                               const float* az, double* pos, double* vel, double* acc) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t o = 3 * (int64_t)p.id[i];
+  if (pos) {
+    pos[o] = decode(p.qx[i], scale);
+    pos[o + 1] = decode(p.qy[i], scale);
+    pos[o + 2] = decode(p.qz[i], scale);
+  }
+  if (vel) {
+    vel[o] = p.vx[i];
+    vel[o + 1] = p.vy[i];
+    vel[o + 2] = p.vz[i];
+  }
+  if (acc) {
+    acc[o] = ax[i];
+    acc[o + 1] = ay[i];
+    acc[o + 2] = az[i];
+  }
+}
+
+__global__ void k_scatter_xyz(const uint32_t* __restrict__ id, int64_t n, const float* x, const float* y,
+                              const float* z, double mul, double* out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t o = 3 * (int64_t)id[i];
+  out[o] = x[i] * mul;
+  out[o + 1] = y[i] * mul;
+  out[o + 2] = z[i] * mul;
+}
+
+__global__ void k_inverse_perm(const uint32_t* __restrict__ id, int64_t n, uint32_t* __restrict__ inv) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) inv[id[i]] = (uint32_t)i;
+}
+
+__global__ void k_pick(const uint32_t* __restrict__ inv, const uint64_t* __restrict__ idx, int64_t m,
+                       const float* ax, const float* ay, const float* az, double* out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const uint32_t s = inv[idx[k]];
+  out[3 * k] = ax[s];
+  out[3 * k + 1] = ay[s];
+  out[3 * k + 2] = az[s];
+}
+
+__global__ void k_kick_drift(Particles p, int64_t n, const float* __restrict__ ax, const float* __restrict__ ay,
+                             const float* __restrict__ az, float kick, double drift_q) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float vx = fmaf(ax[i], kick, p.vx[i]);
+  const float vy = fmaf(ay[i], kick, p.vy[i]);
+  const float vz = fmaf(az[i], kick, p.vz[i]);
+  p.vx[i] = vx;
+  p.vy[i] = vy;
+  p.vz[i] = vz;
+  // x += v * drift, then wrap into the box (exact modulo 2^32 in fixed point)
+  p.qx[i] += (uint32_t)(int64_t)llrint((double)vx * drift_q);
+  p.qy[i] += (uint32_t)(int64_t)llrint((double)vy * drift_q);
+  p.qz[i] += (uint32_t)(int64_t)llrint((double)vz * drift_q);
+}
+
+__global__ void k_scatter_u64(const uint32_t* __restrict__ id, int64_t n, const uint64_t* __restrict__ in,
+                              uint64_t* __restrict__ out, uint32_t* __restrict__ vals) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[id[i]] = in[i];
+  vals[i] = (uint32_t)i;
+}
+
+__global__ void k_export_nodes(int64_t n, int64_t n_int, double scale, const uint8_t* o_depth,
+                               const double* o_mass, const double* o_com, const double* o_quad,
+                               const uint8_t* leaf_depth, Particles p, int32_t* depth, double* mass, double* com,
+                               double* quad, int64_t* particle) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n_int + n) return;
+  if (i < n_int) {
+    depth[i] = o_depth[i];
+    mass[i] = o_mass[i];
+    for (int d = 0; d < 3; ++d) com[3 * i + d] = o_com[3 * i + d];
+    for (int k = 0; k < 6; ++k) quad[6 * i + k] = o_quad[6 * i + k];
+    particle[i] = -1;
+  } else {
+    const int64_t j = i - n_int;
+    depth[i] = leaf_depth ? leaf_depth[j] : 0;
+    mass[i] = p.mass[j];
+    com[3 * i] = decode(p.qx[j], scale);
+    com[3 * i + 1] = decode(p.qy[j], scale);
+    com[3 * i + 2] = decode(p.qz[j], scale);
+    for (int k = 0; k < 6; ++k) quad[6 * i + k] = 0.0;
+    particle[i] = p.id[j];
+  }
+}
+
+// LambdaCDM cosmology (crates/gadget-ng-core/src/cosmology.rs:150-233), FP64.
+struct Cosmo {
+  double om, ol, h0;
+  double da_dt(double a) const {
+    double h_sq = (om + 0.0) / (a * a * a) + ol;
+    return a * h0 * std::sqrt(std::max(h_sq, 0.0));
+  }
+  double advance_a(double a, double dt) const {
+    double k1 = da_dt(a);
+    double k2 = da_dt(a + 0.5 * dt * k1);
+    double k3 = da_dt(a + 0.5 * dt * k2);
+    double k4 = da_dt(a + dt * k3);
+    return a + dt / 6.0 * (k1 + 2.0 * k2 + 2.0 * k3 + k4);
+  }
+};
+
+}  // namespace
+
+struct tpm_handle {
+  tpm_config cfg{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double r_s = 0, r_cut = 0, rc2 = 0, thr = 0;
+  bool periodic = true, pm_only = false;
+  std::string err;
+  int64_t n = 0, cap = 0;
+  Particles P[2]{};
+  int cur = 0;
+  float *ax = nullptr, *ay = nullptr, *az = nullptr;
+  float *srx = nullptr, *sry = nullptr, *srz = nullptr;
+  float *lrx = nullptr, *lry = nullptr, *lrz = nullptr;
+  TreeBuffers T{};
+  PmPlan pm;
+  void* sort_scratch = nullptr;
+  size_t sort_bytes = 0;
+  void* scan_scratch = nullptr;
+  uint32_t* stack = nullptr;
+  int walk_grid = 0;
+  uint2* deferred = nullptr;
+  uint32_t* ndeferred = nullptr;
+  unsigned long long* stats_dev = nullptr;
+  uint32_t* work = nullptr;
+  double* staging = nullptr;  // float64 host-exchange buffer (n x 3 + n)
+  size_t staging_elems = 0;
+  bool forces_valid = false;
+  double g_acc = 0, eps2_acc = -1;
+  int64_t n_int = 0, n_groups = 0;
+  TreeParams params_host{};
+  tpm_stats stats{};
+  cudaEvent_t ev[8]{};
+  size_t mem_used = 0;
+  // every device allocation with its size; `group` 0 = persistent,
+  // 1 = sized by the particle capacity, 2 = sized by the octree
+  struct Alloc {
+    void* p;
+    size_t bytes;
+    int group;
+  };
+  std::vector<Alloc> allocs;
+  bool tree_valid = false;
+
+  template <class T_>
+  T_* alloc(size_t count, int group) {
+    size_t bytes = count * sizeof(T_);
+    if (bytes == 0) bytes = 16;
+    if (cfg.memory_cap_bytes > 0 && mem_used + bytes > (size_t)cfg.memory_cap_bytes)
+      throw Error(TPM_ERR_OUT_OF_MEMORY, "device memory cap of the handle reached (" +
+                                             std::to_string(cfg.memory_cap_bytes) + " bytes)");
+    void* p = nullptr;
+    TPM_CUDA(cudaMalloc(&p, bytes));
+    mem_used += bytes;
+    allocs.push_back({p, bytes, group});
+    return (T_*)p;
+  }
+  void release_group(int group) {
+    std::vector<Alloc> keep;
+    for (const Alloc& a : allocs) {
+      if (a.group == group) {
+        cudaFree(a.p);
+        mem_used -= std::min(mem_used, a.bytes);
+      } else {
+        keep.push_back(a);
+      }
+    }
+    allocs.swap(keep);
+  }
+};
+
+namespace {
+
+int fail(tpm_handle* h, const Error& e) {
+  if (h) h->err = e.what();
+  return e.code ? e.code : TPM_ERR_CUDA;
+}
+
+void check_dev_err(tpm_handle* h) {
+  uint32_t e = 0;
+  TPM_CUDA(cudaMemcpyAsync(&e, h->T.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  TPM_CUDA(cudaStreamSynchronize(h->stream));
+  if (!e) return;
+  TPM_CUDA(cudaMemsetAsync(h->T.err, 0, sizeof(uint32_t), h->stream));
+  if (e & DEV_ERR_NONFINITE) throw Error(TPM_ERR_NONFINITE, "non-finite position or mass");
+  if (e & DEV_ERR_COINCIDENT)
+    throw Error(TPM_ERR_COINCIDENT, "two particles share a position: the insertion octree cannot separate them");
+  if (e & DEV_ERR_TIE_RUN) throw Error(TPM_ERR_COINCIDENT, "too many particles share a 21-level octree cell");
+  if (e & DEV_ERR_STACK) throw Error(TPM_ERR_WALK_STACK, "tree-walk stack capacity exceeded");
+  if (e & DEV_ERR_DEFERRED) throw Error(TPM_ERR_DEFERRED, "exact-fallback work list overflowed");
+  throw Error(TPM_ERR_CUDA, "device error flag " + std::to_string(e));
+}
+
+void ensure_capacity(tpm_handle* h, int64_t n) {
+  if (n <= h->cap) return;
+  h->release_group(2);
+  h->release_group(1);
+  TreeBuffers& T = h->T;
+  T.cap_int = 0;
+  T.cap_groups = 0;
+  const int64_t c = n;
+  for (int k = 0; k < 2; ++k) {
+    Particles& P = h->P[k];
+    P.qx = h->alloc<uint32_t>(c, 1);
+    P.qy = h->alloc<uint32_t>(c, 1);
+    P.qz = h->alloc<uint32_t>(c, 1);
+    P.vx = h->alloc<float>(c, 1);
+    P.vy = h->alloc<float>(c, 1);
+    P.vz = h->alloc<float>(c, 1);
+    P.mass = h->alloc<double>(c, 1);
+    P.massf = h->alloc<float>(c, 1);
+    P.id = h->alloc<uint32_t>(c, 1);
+  }
+  h->ax = h->alloc<float>(c, 1);
+  h->ay = h->alloc<float>(c, 1);
+  h->az = h->alloc<float>(c, 1);
+  h->srx = h->alloc<float>(c, 1);
+  h->sry = h->alloc<float>(c, 1);
+  h->srz = h->alloc<float>(c, 1);
+  h->lrx = h->alloc<float>(c, 1);
+  h->lry = h->alloc<float>(c, 1);
+  h->lrz = h->alloc<float>(c, 1);
+  T.key_hi = h->alloc<uint64_t>(c, 1);
+  T.key_lo = h->alloc<uint64_t>(c, 1);
+  T.key_lo_tmp = h->alloc<uint64_t>(c, 1);
+  T.perm = h->alloc<uint32_t>(c, 1);
+  const int64_t cb = c > 1 ? c - 1 : 1;
+  T.bin_left = h->alloc<uint32_t>(cb, 1);
+  T.bin_right = h->alloc<uint32_t>(cb, 1);
+  T.bin_prefix = h->alloc<int32_t>(cb, 1);
+  T.bin_first = h->alloc<uint32_t>(cb, 1);
+  T.bin_last = h->alloc<uint32_t>(cb, 1);
+  T.bin_parent = h->alloc<int32_t>(cb, 1);
+  T.oct_count = h->alloc<uint32_t>(cb, 1);
+  T.oct_base = h->alloc<uint32_t>(cb, 1);
+  T.leaf_bparent = h->alloc<int32_t>(c, 1);
+  T.leaf_oparent = h->alloc<int32_t>(c, 1);
+  T.leaf_depth = h->alloc<uint8_t>(c, 1);
+  h->sort_bytes = radix_sort_scratch_bytes(c);
+  h->sort_scratch = h->alloc<char>(h->sort_bytes, 1);
+  h->scan_scratch = h->alloc<char>(scan_scratch_bytes(4 * c + 16), 1);
+  h->staging_elems = (size_t)9 * c;  // positions, velocities, accelerations (n x 3 float64 each)
+  h->staging = h->alloc<double>(h->staging_elems, 1);
+  h->cap = n;
+}
+
+void ensure_tree_capacity(tpm_handle* h, int64_t n_int) {
+  TreeBuffers& T = h->T;
+  if (n_int <= T.cap_int) return;
+  h->release_group(2);
+  const int64_t c = std::max<int64_t>(n_int + n_int / 8, 1024);
+  T.o_parent = h->alloc<int32_t>(c, 2);
+  T.o_depth = h->alloc<uint8_t>(c, 2);
+  T.o_first = h->alloc<uint32_t>(c, 2);
+  T.o_last = h->alloc<uint32_t>(c, 2);
+  T.o_slots = h->alloc<uint32_t>(8 * c, 2);
+  T.o_nchild = h->alloc<uint32_t>(c, 2);
+  T.o_child_first = h->alloc<uint32_t>(c, 2);
+  T.o_cnt = h->alloc<uint32_t>(c, 2);
+  T.child_ids = h->alloc<uint32_t>(c + h->cap + 8, 2);
+  T.o_mass = h->alloc<double>(c, 2);
+  T.o_com = h->alloc<double>(3 * c, 2);
+  T.o_quad = h->alloc<double>(6 * c, 2);
+  T.o_walk = h->alloc<uint4>(c, 2);
+  T.grp_count_per_node = h->alloc<uint32_t>(c, 2);
+  T.grp_base = h->alloc<uint32_t>(c, 2);
+  T.grp_first = h->alloc<uint32_t>(h->cap + 1, 2);
+  T.grp_size = h->alloc<uint32_t>(h->cap + 1, 2);
+  T.cap_int = c;
+  T.cap_groups = h->cap + 1;
+}
+
+float ms_between(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// One force evaluation of all resident particles.  kick != 0 applies
+// v += a * kick in the gather.
+void force_eval(tpm_handle* h, double eps2, double g, double kick) {
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  if (n == 0) throw Error(TPM_ERR_NOT_READY, "no particles set");
+  TreeBuffers& T = h->T;
+  const double box = h->cfg.box_size;
+  const unsigned long long launches0 = g_kernel_launches;
+  TPM_CUDA(cudaEventRecord(h->ev[0], s));
+  TPM_CUDA(cudaMemsetAsync(h->stats_dev, 0, 8 * sizeof(unsigned long long), s));
+  const bool need_tree = !h->pm_only;
+  h->tree_valid = false;
+  if (need_tree) {
+    // ---- keys and sort
+    launch_bbox_root(h->P[h->cur], n, box, T, s);
+    launch_tree_keys(h->P[h->cur], n, box, T, s);
+    TPM_CUDA(cudaEventRecord(h->ev[1], s));
+    radix_sort_u64(T.key_hi, T.perm, n, 63, h->sort_scratch, h->sort_bytes, s);
+    launch_fix_ties(n, T, s);
+    launch_permute(h->P[h->cur], h->P[1 - h->cur], n, T.perm, s);
+    h->cur = 1 - h->cur;
+    TPM_CUDA(cudaEventRecord(h->ev[2], s));
+    // ---- tree
+    h->n_int = 0;
+    if (n >= 2) {
+      TPM_CUDA(cudaMemsetAsync(T.scalars, 0, 4 * sizeof(uint32_t), s));
+      launch_karras(n, T, s);
+      exclusive_scan_u32(T.oct_count, T.oct_base, n - 1, &T.scalars[0], h->scan_scratch, s);
+      uint32_t sc[4];
+      TPM_CUDA(cudaMemcpyAsync(sc, T.scalars, sizeof(sc), cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaMemcpyAsync(&h->params_host, T.params, sizeof(TreeParams), cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+      h->n_int = sc[0];
+      ensure_tree_capacity(h, h->n_int);
+      launch_octree_nodes(n, T, s);
+      launch_octree_links(n, h->n_int, T, h->scan_scratch, s);
+      launch_aggregate(h->P[h->cur], n, h->n_int, box, T, s);
+      launch_groups(n, h->n_int, GROUP_MAX, T, h->scan_scratch, s);
+      TPM_CUDA(cudaMemcpyAsync(sc, T.scalars, sizeof(sc), cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+      h->n_groups = sc[1];
+      h->stats.max_tree_depth = (int32_t)sc[2];
+    } else {
+      TPM_CUDA(cudaMemcpyAsync(&h->params_host, T.params, sizeof(TreeParams), cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+      h->n_groups = 0;
+    }
+    h->tree_valid = true;
+    TPM_CUDA(cudaEventRecord(h->ev[3], s));
+    // ---- short-range walk
+    if (n >= 2) {
+      const double scale = box / TWO32;
+      const double h0 = h->params_host.half;
+      const int U = (int)std::lround(std::log2(h->r_cut / scale));
+      const double u = std::ldexp(scale, U);
+      WalkArgs a{};
+      a.n = n;
+      a.n_int = h->n_int;
+      const Particles& P = h->P[h->cur];
+      a.qx = P.qx; a.qy = P.qy; a.qz = P.qz; a.massf = P.massf;
+      a.walk = T.o_walk; a.depth = T.o_depth; a.nchild = T.o_nchild; a.child_first = T.o_child_first;
+      a.child_ids = T.child_ids; a.o_com = T.o_com; a.leaf_depth = T.leaf_depth;
+      a.gfirst = T.grp_first; a.gsize = T.grp_size; a.ngroups = h->n_groups; a.work = h->work;
+      a.scale = scale; a.box = box; a.rc2 = h->rc2; a.thr = h->thr; a.h0 = h0;
+      a.periodic = h->periodic ? 1 : 0;
+      a.u_inv = (float)std::ldexp(1.0, -U);
+      a.h0_u = (float)(h0 / u);
+      const double rc2_u = h->rc2 / (u * u);
+      a.rc2_lo = (float)(rc2_u * (1.0 - 1e-4));
+      a.rc2_hi = (float)(rc2_u * (1.0 + 1e-4));
+      a.grc2_lo = (float)(rc2_u * (1.0 - 4e-4));
+      a.grc2_hi = (float)(rc2_u * (1.0 + 4e-4));
+      a.eps2_u = (float)(eps2 / (u * u));
+      const double cx = u / (std::sqrt(2.0) * h->r_s);
+      a.pcx = (float)(0.3275911 * cx);
+      a.ex2k = (float)(-(cx * cx) / std::log(2.0));
+      const double tq = std::ldexp(4.0, -U);
+      a.tiny_u = (float)(tq * tq);
+      a.out_scale = (float)(1.0 / (u * u));
+      a.ax = h->srx; a.ay = h->sry; a.az = h->srz;
+      a.stats = h->stats_dev; a.err = T.err;
+      a.deferred = h->deferred; a.ndeferred = h->ndeferred; a.cap_deferred = DEFERRED_CAP;
+      a.stack = h->stack; a.stack_cap = STACK_CAP;
+      TPM_CUDA(cudaMemsetAsync(h->work, 0, sizeof(uint32_t), s));
+      TPM_CUDA(cudaMemsetAsync(h->ndeferred, 0, sizeof(uint32_t), s));
+      launch_walk(a, h->walk_grid, s);
+      uint32_t nd = 0;
+      TPM_CUDA(cudaMemcpyAsync(&nd, h->ndeferred, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+      if (nd) launch_deferred(a, std::min(nd, DEFERRED_CAP), s);
+      double thr_depth = h0;
+      int dstar = 0;
+      while (!(thr_depth < h->thr) && dstar < 200) {
+        thr_depth = std::ldexp(h0, -(++dstar));
+      }
+      h->stats.terminal_depth = dstar;
+    } else {
+      TPM_CUDA(cudaMemsetAsync(h->srx, 0, sizeof(float) * n, s));
+      TPM_CUDA(cudaMemsetAsync(h->sry, 0, sizeof(float) * n, s));
+      TPM_CUDA(cudaMemsetAsync(h->srz, 0, sizeof(float) * n, s));
+    }
+  } else {
+    TPM_CUDA(cudaEventRecord(h->ev[1], s));
+    TPM_CUDA(cudaEventRecord(h->ev[2], s));
+    TPM_CUDA(cudaEventRecord(h->ev[3], s));
+  }
+  TPM_CUDA(cudaEventRecord(h->ev[4], s));
+  // ---- long range
+  const Particles& P = h->P[h->cur];
+  pm_deposit(h->pm, P.qx, P.qy, P.qz, P.massf, n, s);
+  pm_solve(h->pm, s);
+  TPM_CUDA(cudaEventRecord(h->ev[5], s));
+  GatherArgs ga{};
+  ga.n = n;
+  ga.qx = P.qx; ga.qy = P.qy; ga.qz = P.qz;
+  ga.srx = h->pm_only ? nullptr : h->srx;
+  ga.sry = h->pm_only ? nullptr : h->sry;
+  ga.srz = h->pm_only ? nullptr : h->srz;
+  ga.ax = h->ax; ga.ay = h->ay; ga.az = h->az;
+  ga.lrx = h->lrx; ga.lry = h->lry; ga.lrz = h->lrz;
+  if (kick != 0.0) {
+    ga.vx = P.vx; ga.vy = P.vy; ga.vz = P.vz;
+  }
+  ga.g = g;
+  ga.kick = kick;
+  pm_gather_kick(h->pm, ga, s);
+  TPM_CUDA(cudaEventRecord(h->ev[6], s));
+  check_dev_err(h);
+  unsigned long long st[8];
+  TPM_CUDA(cudaMemcpy(st, h->stats_dev, sizeof(st), cudaMemcpyDeviceToHost));
+  h->stats.n_particles = n;
+  h->stats.n_tree_nodes = h->n_int;
+  h->stats.n_groups = h->n_groups;
+  h->stats.leaf_pairs = (int64_t)st[0];
+  h->stats.monopoles = (int64_t)st[1];
+  h->stats.evaluated_pairs = (int64_t)st[2];
+  h->stats.exact_fallbacks = (int64_t)st[3];
+  h->stats.deferred_opens = (int64_t)st[4];
+  h->stats.ms_bbox_keys = ms_between(h->ev[0], h->ev[1]);
+  h->stats.ms_sort = ms_between(h->ev[1], h->ev[2]);
+  h->stats.ms_build = ms_between(h->ev[2], h->ev[3]);
+  h->stats.ms_walk = ms_between(h->ev[3], h->ev[4]);
+  h->stats.ms_pm = ms_between(h->ev[4], h->ev[5]);
+  h->stats.ms_gather_kick = ms_between(h->ev[5], h->ev[6]);
+  h->stats.ms_total = ms_between(h->ev[0], h->ev[6]);
+  h->stats.kernel_launches = (int64_t)(g_kernel_launches - launches0);
+  h->forces_valid = true;
+  h->g_acc = g;
+  h->eps2_acc = eps2;
+}
+
+void upload(tpm_handle* h, const double* pos, const double* vel, const double* mass, int64_t n) {
+  if (n < 0 || n >= (int64_t)1 << 31) throw Error(TPM_ERR_INVALID_ARGUMENT, "particle count out of range");
+  if (n > 0 && (!pos || !mass)) throw Error(TPM_ERR_INVALID_ARGUMENT, "positions and masses are required");
+  ensure_capacity(h, std::max<int64_t>(n, 1));
+  h->n = n;
+  h->cur = 0;
+  h->forces_valid = false;
+  if (n == 0) return;
+  cudaStream_t s = h->stream;
+  double* dpos = h->staging;
+  double* dmass = h->staging + 3 * n;
+  TPM_CUDA(cudaMemcpyAsync(dpos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+  TPM_CUDA(cudaMemcpyAsync(dmass, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  double* dvel = nullptr;
+  if (vel) {
+    dvel = h->staging + 4 * n;
+    TPM_CUDA(cudaMemcpyAsync(dvel, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+  }
+  k_encode<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(dpos, dvel, dmass, n, h->cfg.box_size, h->P[0], h->T.err);
+  TPM_LAUNCH_CHECK();
+  check_dev_err(h);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int tpm_version(void) { return 10000; }
+
+int tpm_create(const tpm_config* cfg, tpm_handle** out) {
+  if (!cfg || !out) return TPM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  tpm_handle* h = new (std::nothrow) tpm_handle();
+  if (!h) return TPM_ERR_OUT_OF_MEMORY;
+  try {
+    h->cfg = *cfg;
+    const int nm = cfg->grid_size;
+    if (nm < 4 || nm > 1024 || (nm & (nm - 1)) != 0)
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "pm_grid_size must be a power of two in [4, 1024]");
+    if (!(cfg->box_size > 0.0) || !std::isfinite(cfg->box_size))
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "box_size must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      throw Error(TPM_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) throw Error(TPM_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    cudaDeviceProp prop;
+    TPM_CUDA(cudaGetDeviceProperties(&prop, cfg->device));
+    if (prop.major != 10) throw Error(TPM_ERR_NO_DEVICE, std::string("device is not sm_100: ") + prop.name);
+    TPM_CUDA(cudaSetDevice(cfg->device));
+    // solver.rs:56-62 (auto r_s = 2.5 cells), :80 (r_cut = 5 r_s)
+    h->r_s = cfg->r_split > 0.0 ? cfg->r_split : 2.5 * cfg->box_size / (double)nm;
+    const double f = cfg->r_cut_factor > 0.0 ? cfg->r_cut_factor : 5.0;
+    h->r_cut = f * h->r_s;
+    h->rc2 = h->r_cut * h->r_cut;
+    h->thr = 0.1 * std::sqrt(h->rc2);  // short_range.rs:320
+    h->periodic = !(cfg->flags & TPM_FLAG_APERIODIC_WALK);
+    h->pm_only = (cfg->flags & TPM_FLAG_PM_ONLY) != 0;
+    if (!h->pm_only && h->r_cut >= 0.5 * cfg->box_size)
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "r_cut must be below half the box");
+    TPM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+    for (auto& e : h->ev) TPM_CUDA(cudaEventCreate(&e));
+    h->T.params = h->alloc<TreeParams>(1, 0);
+    h->T.bbox = h->alloc<uint32_t>(6, 0);
+    h->T.scalars = h->alloc<uint32_t>(8, 0);
+    h->T.err = h->alloc<uint32_t>(1, 0);
+    h->stats_dev = h->alloc<unsigned long long>(8, 0);
+    h->work = h->alloc<uint32_t>(1, 0);
+    h->ndeferred = h->alloc<uint32_t>(1, 0);
+    h->deferred = h->alloc<uint2>(DEFERRED_CAP, 0);
+    int sms = prop.multiProcessorCount;
+    h->walk_grid = sms * walk_blocks_per_sm();
+    h->stack = h->alloc<uint32_t>(walk_stack_words(h->walk_grid, STACK_CAP), 0);
+    TPM_CUDA(cudaMemset(h->T.err, 0, sizeof(uint32_t)));
+    pm_plan_init(h->pm, nm, cfg->box_size, h->pm_only ? 0.0 : h->r_s, cfg->flags, cfg->device);
+    h->mem_used += (size_t)nm * nm * nm * 4 * 4 + (size_t)nm * nm * (nm / 2 + 1) * 8 * 4;  // PM meshes
+  } catch (const Error& e) {
+    int code = e.code;
+    delete h;
+    (void)code;
+    return code ? code : TPM_ERR_CUDA;
+  }
+  *out = h;
+  return TPM_OK;
+}
+
+void tpm_destroy(tpm_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (const auto& a : h->allocs) cudaFree(a.p);
+  pm_plan_free(h->pm);
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+const char* tpm_last_error(const tpm_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int tpm_set_stream(tpm_handle* h, void* stream) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    TPM_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)stream;
+    h->own_stream = false;
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+void* tpm_get_stream(const tpm_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int tpm_accelerations_for_indices(tpm_handle* h, const double* pos, const double* mass, int64_t n, double eps2,
+                                  double g, const uint64_t* idx, int64_t n_idx, double* out) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (n_idx < 0 || (n_idx > 0 && (!idx || !out))) throw Error(TPM_ERR_INVALID_ARGUMENT, "bad index arrays");
+    for (int64_t k = 0; k < n_idx; ++k)
+      if ((int64_t)idx[k] >= n) throw Error(TPM_ERR_INVALID_ARGUMENT, "global index out of range");
+    upload(h, pos, nullptr, mass, n);
+    if (n_idx == 0) return TPM_OK;
+    force_eval(h, eps2, g, 0.0);
+    cudaStream_t s = h->stream;
+    uint32_t* inv = h->T.perm;  // free after the build
+    k_inverse_perm<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, inv);
+    TPM_LAUNCH_CHECK();
+    uint64_t* didx = (uint64_t*)h->sort_scratch;
+    double* dout = h->staging;
+    for (int64_t k0 = 0; k0 < n_idx; k0 += n) {  // chunks of at most n indices
+      const int64_t m = std::min<int64_t>(n, n_idx - k0);
+      TPM_CUDA(cudaMemcpyAsync(didx, idx + k0, sizeof(uint64_t) * m, cudaMemcpyHostToDevice, s));
+      k_pick<<<grid_for(m, 256, 1ll << 30), 256, 0, s>>>(inv, didx, m, h->ax, h->ay, h->az, dout);
+      TPM_LAUNCH_CHECK();
+      TPM_CUDA(cudaMemcpyAsync(out + 3 * k0, dout, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, s));
+    }
+    TPM_CUDA(cudaStreamSynchronize(s));
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_set_particles(tpm_handle* h, const double* pos, const double* vel, const double* mass, int64_t n) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    upload(h, pos, vel, mass, n);
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_set_particles_fixed(tpm_handle* h, const uint32_t* q, const float* vel, const double* mass, int64_t n) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (n <= 0 || !q || !mass) throw Error(TPM_ERR_INVALID_ARGUMENT, "positions and masses are required");
+    ensure_capacity(h, n);
+    h->n = n;
+    h->cur = 0;
+    h->forces_valid = false;
+    cudaStream_t s = h->stream;
+    std::vector<uint32_t> tmp((size_t)n);
+    Particles& P = h->P[0];
+    uint32_t* dst[3] = {P.qx, P.qy, P.qz};
+    for (int d = 0; d < 3; ++d) {
+      for (int64_t i = 0; i < n; ++i) tmp[i] = q[3 * i + d];
+      TPM_CUDA(cudaMemcpyAsync(dst[d], tmp.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+    }
+    std::vector<float> fv((size_t)n);
+    float* vd[3] = {P.vx, P.vy, P.vz};
+    for (int d = 0; d < 3; ++d) {
+      for (int64_t i = 0; i < n; ++i) fv[i] = vel ? vel[3 * i + d] : 0.f;
+      TPM_CUDA(cudaMemcpyAsync(vd[d], fv.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+    }
+    TPM_CUDA(cudaMemcpyAsync(P.mass, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    for (int64_t i = 0; i < n; ++i) fv[i] = (float)mass[i];
+    TPM_CUDA(cudaMemcpyAsync(P.massf, fv.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s));
+    std::vector<uint32_t> ids((size_t)n);
+    for (int64_t i = 0; i < n; ++i) ids[i] = (uint32_t)i;
+    TPM_CUDA(cudaMemcpyAsync(P.id, ids.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
+    TPM_CUDA(cudaStreamSynchronize(s));
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_compute_forces(tpm_handle* h, double eps2, double g) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    force_eval(h, eps2, g, 0.0);
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_kdk_step(tpm_handle* h, double kick_half, double drift, double kick_half2, double eps2, double g) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (h->n == 0) throw Error(TPM_ERR_NOT_READY, "no particles set");
+    if (!h->forces_valid || h->eps2_acc != eps2 || h->g_acc == 0.0) force_eval(h, eps2, g, 0.0);
+    // opening half kick with the cached acceleration, rescaled to this step's coupling
+    const double k1 = kick_half * (g / h->g_acc);
+    const Particles& P = h->P[h->cur];
+    k_kick_drift<<<grid_for(h->n, 256, 1ll << 30), 256, 0, h->stream>>>(P, h->n, h->ax, h->ay, h->az, (float)k1,
+                                                                        drift * TWO32 / h->cfg.box_size);
+    TPM_LAUNCH_CHECK();
+    force_eval(h, eps2, g, kick_half2);
+    h->stats.kernel_launches += 1;  // the kick-drift kernel
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_get_state(tpm_handle* h, double* pos, double* vel, double* acc) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    const int64_t n = h->n;
+    if (n == 0) return TPM_OK;
+    if (acc && !h->forces_valid) throw Error(TPM_ERR_NOT_READY, "no forces computed");
+    cudaStream_t s = h->stream;
+    double* dp = h->staging;
+    double* dv = h->staging + 3 * n;
+    double* da = h->staging + 6 * n;
+    k_decode_state<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur], n, h->cfg.box_size / TWO32, nullptr,
+                                                               nullptr, nullptr, pos ? dp : nullptr,
+                                                               vel ? dv : nullptr, nullptr);
+    TPM_LAUNCH_CHECK();
+    if (pos) TPM_CUDA(cudaMemcpyAsync(pos, dp, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+    if (vel) TPM_CUDA(cudaMemcpyAsync(vel, dv, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaStreamSynchronize(s));
+    if (acc) {
+      double* buf = da;
+      k_scatter_xyz<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, h->ax, h->ay, h->az, 1.0, buf);
+      TPM_LAUNCH_CHECK();
+      TPM_CUDA(cudaMemcpyAsync(acc, buf, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+    }
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_kdk_step_host(tpm_handle* h, double* pos, double* vel, const double* mass, int64_t n, double kick_half,
+                      double drift, double kick_half2, double eps2, double g) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  int rc = tpm_set_particles(h, pos, vel, mass, n);
+  if (rc) return rc;
+  rc = tpm_kdk_step(h, kick_half, drift, kick_half2, eps2, g);
+  if (rc) return rc;
+  return tpm_get_state(h, pos, vel, nullptr);
+}
+
+int tpm_get_force_parts(tpm_handle* h, double* acc_lr, double* acc_sr) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (!h->forces_valid) throw Error(TPM_ERR_NOT_READY, "no forces computed");
+    const int64_t n = h->n;
+    cudaStream_t s = h->stream;
+    if (acc_lr) {
+      k_scatter_xyz<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, h->lrx, h->lry, h->lrz, 1.0,
+                                                                h->staging);
+      TPM_LAUNCH_CHECK();
+      TPM_CUDA(cudaMemcpyAsync(acc_lr, h->staging, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+    }
+    if (acc_sr) {
+      if (h->pm_only) {
+        std::memset(acc_sr, 0, sizeof(double) * 3 * n);
+      } else {
+        k_scatter_xyz<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, h->srx, h->sry, h->srz,
+                                                                  h->g_acc, h->staging);
+        TPM_LAUNCH_CHECK();
+        TPM_CUDA(cudaMemcpyAsync(acc_sr, h->staging, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+        TPM_CUDA(cudaStreamSynchronize(s));
+      }
+    }
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_get_stats(const tpm_handle* h, tpm_stats* out) {
+  if (!h || !out) return TPM_ERR_INVALID_ARGUMENT;
+  *out = h->stats;
+  return TPM_OK;
+}
+
+int tpm_drift_kick_factors(double omega_m, double omega_lambda, double h0, double a0, double dt, double* out3) {
+  if (!out3) return TPM_ERR_INVALID_ARGUMENT;
+  const Cosmo c{omega_m, omega_lambda, h0};
+  const uint32_t N_SUB = 16;
+  const double sub_dt = dt / (double)N_SUB;
+  double a = a0, drift = 0.0, kh = 0.0, kh2 = 0.0;
+  for (uint32_t sidx = 0; sidx < N_SUB; ++sidx) {
+    const double al = a, am = c.advance_a(a, sub_dt * 0.5), ar = c.advance_a(a, sub_dt);
+    drift += sub_dt / 6.0 * (1.0 / (al * al) + 4.0 / (am * am) + 1.0 / (ar * ar));
+    const double k = sub_dt / 6.0 * (1.0 / al + 4.0 / am + 1.0 / ar);
+    if (sidx < N_SUB / 2) kh += k; else kh2 += k;
+    a = ar;
+  }
+  out3[0] = drift;
+  out3[1] = kh;
+  out3[2] = kh2;
+  return TPM_OK;
+}
+
+double tpm_advance_a(double omega_m, double omega_lambda, double h0, double a, double dt) {
+  return Cosmo{omega_m, omega_lambda, h0}.advance_a(a, dt);
+}
+
+int tpm_hilbert_keys(tpm_handle* h, uint64_t* keys, int64_t* order) {
+  if (!h || !keys) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    const int64_t n = h->n;
+    if (n == 0) return TPM_OK;
+    cudaStream_t s = h->stream;
+    launch_bbox_root(h->P[h->cur], n, h->cfg.box_size, h->T, s);
+    uint64_t* k_store = h->T.key_lo_tmp;
+    uint64_t* k_by_id = h->T.key_hi;
+    uint32_t* vals = h->T.perm;
+    launch_hilbert_keys(h->P[h->cur], n, h->cfg.box_size, h->T.params, k_store, vals, s);
+    k_scatter_u64<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, k_store, k_by_id, vals);
+    TPM_LAUNCH_CHECK();
+    TPM_CUDA(cudaMemcpyAsync(keys, k_by_id, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, s));
+    if (order) {
+      radix_sort_u64(k_by_id, vals, n, 63, h->sort_scratch, h->sort_bytes, s);
+      std::vector<uint32_t> o((size_t)n);
+      TPM_CUDA(cudaMemcpyAsync(o.data(), vals, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+      for (int64_t i = 0; i < n; ++i) order[i] = o[i];
+    }
+    TPM_CUDA(cudaStreamSynchronize(s));
+    h->tree_valid = false;
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_cic_cells(tpm_handle* h, int32_t* cells) {
+  if (!h || !cells) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    const int64_t n = h->n;
+    if (n == 0) return TPM_OK;
+    int32_t* d = (int32_t*)h->staging;
+    const Particles& P = h->P[h->cur];
+    pm_cells(h->pm, P.qx, P.qy, P.qz, P.id, n, d, h->stream);
+    TPM_CUDA(cudaMemcpyAsync(cells, d, sizeof(int32_t) * 3 * n, cudaMemcpyDeviceToHost, h->stream));
+    TPM_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int64_t tpm_tree_node_count(const tpm_handle* h) {
+  if (!h || !h->tree_valid) return 0;
+  return h->n_int + h->n;
+}
+
+int64_t tpm_export_tree(tpm_handle* h, int64_t cap, int32_t* depth, double* mass, double* com, double* quad,
+                        int64_t* particle, uint64_t* path_hi, uint64_t* path_lo) {
+  if (!h) return -TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (!h->tree_valid) throw Error(TPM_ERR_NOT_READY, "no tree built");
+    const int64_t n = h->n, ni = h->n_int, tot = n + ni;
+    if (cap < tot) return tot;
+    if (!depth || !mass || !com || !quad || !particle || !path_hi || !path_lo)
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "null export array");
+    cudaStream_t s = h->stream;
+    int32_t* dd;
+    double *dm, *dc, *dq;
+    int64_t* dp;
+    uint64_t *nh, *nl;
+    TPM_CUDA(cudaMalloc(&dd, sizeof(int32_t) * tot));
+    TPM_CUDA(cudaMalloc(&dm, sizeof(double) * tot));
+    TPM_CUDA(cudaMalloc(&dc, sizeof(double) * 3 * tot));
+    TPM_CUDA(cudaMalloc(&dq, sizeof(double) * 6 * tot));
+    TPM_CUDA(cudaMalloc(&dp, sizeof(int64_t) * tot));
+    TPM_CUDA(cudaMalloc(&nh, sizeof(uint64_t) * tot));
+    TPM_CUDA(cudaMalloc(&nl, sizeof(uint64_t) * tot));
+    k_export_nodes<<<grid_for(tot, 256, 1ll << 30), 256, 0, s>>>(n, ni, h->cfg.box_size / TWO32, h->T.o_depth,
+                                                                 h->T.o_mass, h->T.o_com, h->T.o_quad,
+                                                                 n > 1 ? h->T.leaf_depth : nullptr, h->P[h->cur], dd,
+                                                                 dm, dc, dq, dp);
+    TPM_LAUNCH_CHECK();
+    launch_export_paths(n, ni, h->T, nh, nl, nh + ni, nl + ni, s);
+    TPM_CUDA(cudaMemcpyAsync(depth, dd, sizeof(int32_t) * tot, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaMemcpyAsync(mass, dm, sizeof(double) * tot, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaMemcpyAsync(com, dc, sizeof(double) * 3 * tot, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaMemcpyAsync(quad, dq, sizeof(double) * 6 * tot, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaMemcpyAsync(particle, dp, sizeof(int64_t) * tot, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaMemcpyAsync(path_hi, nh, sizeof(uint64_t) * tot, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaMemcpyAsync(path_lo, nl, sizeof(uint64_t) * tot, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaStreamSynchronize(s));
+    cudaFree(dd); cudaFree(dm); cudaFree(dc); cudaFree(dq); cudaFree(dp); cudaFree(nh); cudaFree(nl);
+    return tot;
+  } catch (const Error& e) {
+    fail(h, e);
+    return -(int64_t)(e.code ? e.code : TPM_ERR_CUDA);
+  }
+}
+
+int tpm_get_mesh(tpm_handle* h, float* density, float* fx, float* fy, float* fz) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (!h->forces_valid) throw Error(TPM_ERR_NOT_READY, "no forces computed");
+    const int64_t nm3 = (int64_t)h->pm.nm * h->pm.nm * h->pm.nm;
+    cudaStream_t s = h->stream;
+    if (density) TPM_CUDA(cudaMemcpyAsync(density, h->pm.rho, sizeof(float) * nm3, cudaMemcpyDeviceToHost, s));
+    float* f[3] = {fx, fy, fz};
+    for (int c = 0; c < 3; ++c)
+      if (f[c]) TPM_CUDA(cudaMemcpyAsync(f[c], h->pm.force + c * nm3, sizeof(float) * nm3, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaStreamSynchronize(s));
+    const float g = (float)h->g_acc;
+    for (int c = 0; c < 3; ++c)
+      if (f[c])
+        for (int64_t i = 0; i < nm3; ++i) f[c][i] *= g;
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+}  // extern "C"

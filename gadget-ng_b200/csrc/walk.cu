@@ -1,0 +1,554 @@
+// Short-range TreePM walk, one warp per target group.
+//
+// Semantics (crates/gadget-ng-treepm/src/short_range.rs:274-333, periodic;
+// :157-208, aperiodic): for each target particle the reference pops nodes
+// from a stack, drops a node whose AABB (centred on its centre of mass, half
+// side = the cell's half side) lies beyond r_cut, adds the pair force of a
+// leaf (periodic walk: only if the bare minimum-image distance is within
+// r_cut), takes an internal node whose half side is below 0.1 r_cut as a
+// monopole (unless its centre of mass sits on the target), and otherwise
+// opens it.  An internal node's cull hides all its descendants, so whether a
+// target interacts with a node depends on every ancestor on its path.
+//
+// Warp design: the 32 lanes hold up to 32 target particles from one compact
+// subtree.  The warp walks the tree once for all of them: each stack entry
+// carries a 32-bit mask of the targets that still see that node.  Nodes are
+// classified against the group's bounding box in FP32 with a safety margin
+// (certainly culled / certainly kept for every target / undecided); undecided
+// internal nodes get a per-target test when they are popped, which refines the
+// mask, so the hierarchical culls of the reference are reproduced exactly.
+// Terminal nodes (leaves and monopole-depth cells) go to an interaction list
+// in shared memory; every lane evaluates the whole list against its own
+// target with its own final test fused into the pair kernel.  Any decision
+// that falls inside a narrow band around r_cut is re-evaluated in float64
+// with the reference's exact expression, so the interaction set equals the
+// reference's.  Pair arithmetic is FP32: exact fixed-point differences split
+// into two floats, rsqrt / rcp / ex2 hardware approximations, the A&S 7.1.26
+// erfc, and Kahan-compensated per-target accumulators.
+#include "common.cuh"
+#include "tree.cuh"
+#include "walk.cuh"
+
+namespace tpm {
+namespace {
+
+constexpr int WALK_WARPS = 4;
+constexpr int WALK_THREADS = WALK_WARPS * 32;
+constexpr int CHUNK = 96;
+constexpr uint32_t AMB_FLAG = 0x40000000u;
+constexpr uint32_t NODE_MASK = 0x3FFFFFFFu;
+constexpr int32_t WIDE_GROUP = 1 << 29;  // quanta: 1/8 of the box
+
+enum : uint32_t { KIND_LEAF = 0, KIND_MONO = 1 };
+
+struct __align__(16) Entry {
+  float hx, hy, hz, m;   // source position (high part, walk units) and mass
+  float lx, ly, lz, h;   // low part, cull half side (0 for periodic leaves)
+  uint32_t mask, node, kind, pad;
+};
+
+__device__ __forceinline__ int32_t rel32(uint32_t a, uint32_t b, int periodic) {
+  if (periodic) return (int32_t)(a - b);  // minimum image modulo 2^32
+  int64_t d = (int64_t)a - (int64_t)b;
+  d = d > 0x7FFFFFFFll ? 0x7FFFFFFFll : (d < -0x7FFFFFFFll ? -0x7FFFFFFFll : d);
+  return (int32_t)d;
+}
+
+// exact float split: v = hi + lo with hi a multiple of 512 (<= 23 significant bits)
+__device__ __forceinline__ void split_rel(int32_t v, float u_inv, float* hi, float* lo) {
+  *hi = (float)(v & ~511) * u_inv;
+  *lo = (float)(v & 511) * u_inv;
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  return v;
+}
+
+// ---- float64 decisions with the reference's expressions -------------------
+__device__ __forceinline__ double aabb_axis(double dc, double h) {
+  double e = dsub(fabs(dc), h);
+  return e > 0.0 ? e : 0.0;
+}
+
+// min_dist2_to_aabb_periodic (short_range.rs:72-84) or its aperiodic twin (:173-181).
+__device__ double d2_aabb(const double xi[3], const double com[3], double h, double box, int periodic) {
+  double e[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double dc = dsub(com[a], xi[a]);
+    if (periodic) dc = minimum_image(dc, box);
+    e[a] = aabb_axis(dc, h);
+  }
+  return dadd(dadd(dmul(e[0], e[0]), dmul(e[1], e[1])), dmul(e[2], e[2]));
+}
+
+__device__ __forceinline__ void target_pos(const WalkArgs& a, uint32_t p, double xi[3]) {
+  xi[0] = decode(a.qx[p], a.scale);
+  xi[1] = decode(a.qy[p], a.scale);
+  xi[2] = decode(a.qz[p], a.scale);
+}
+
+__device__ __forceinline__ void node_com(const WalkArgs& a, uint32_t node, double c[3]) {
+  if (node & LEAF_BIT) {
+    uint32_t j = node & ~LEAF_BIT;
+    c[0] = decode(a.qx[j], a.scale);
+    c[1] = decode(a.qy[j], a.scale);
+    c[2] = decode(a.qz[j], a.scale);
+  } else {
+    c[0] = a.o_com[3 * (int64_t)node];
+    c[1] = a.o_com[3 * (int64_t)node + 1];
+    c[2] = a.o_com[3 * (int64_t)node + 2];
+  }
+}
+
+// Does target p keep open internal node `node` (cull test only)?
+__device__ bool exact_open_pass(const WalkArgs& a, uint32_t p, uint32_t node) {
+  double xi[3], c[3];
+  target_pos(a, p, xi);
+  node_com(a, node, c);
+  double h = ldexp(a.h0, -(int)a.depth[node]);
+  return !(d2_aabb(xi, c, h, a.box, a.periodic) > a.rc2);
+}
+
+// Terminal node decision: 0 = skip, 1 = interact, 2 = open for this target
+// (monopole whose centre of mass coincides with the target).
+__device__ int exact_terminal(const WalkArgs& a, uint32_t p, uint32_t node) {
+  double xi[3], c[3];
+  target_pos(a, p, xi);
+  node_com(a, node, c);
+  if (node & LEAF_BIT) {
+    uint32_t j = node & ~LEAF_BIT;
+    if (a.periodic) {
+      double r[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) r[k] = minimum_image(dsub(c[k], xi[k]), a.box);
+      double r2 = dadd(dadd(dmul(r[0], r[0]), dmul(r[1], r[1])), dmul(r[2], r[2]));
+      return r2 > a.rc2 ? 0 : 1;
+    }
+    double h = ldexp(a.h0, -(int)a.leaf_depth[j]);
+    return d2_aabb(xi, c, h, a.box, 0) > a.rc2 ? 0 : 1;
+  }
+  double h = ldexp(a.h0, -(int)a.depth[node]);
+  if (d2_aabb(xi, c, h, a.box, a.periodic) > a.rc2) return 0;
+  double d[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    d[k] = dsub(c[k], xi[k]);
+    if (a.periodic) d[k] = minimum_image(d[k], a.box);
+  }
+  double d2 = dadd(dadd(dmul(d[0], d[0]), dmul(d[1], d[1])), dmul(d[2], d[2]));
+  return d2 > 1e-30 ? 1 : 2;
+}
+
+__device__ __forceinline__ void defer(const WalkArgs& a, uint32_t p, uint32_t node) {
+  uint32_t slot = atomicAdd(a.ndeferred, 1u);
+  if (slot < a.cap_deferred) a.deferred[slot] = make_uint2(p, node);
+  else atomicOr(a.err, DEV_ERR_DEFERRED);
+}
+
+// FP32 pair term: returns m * erfc(r/(sqrt2 r_s)) / r^3 (walk units).
+__device__ __forceinline__ float pair_factor(const WalkArgs& a, float r2b, float m) {
+  float r2 = fmaxf(r2b + a.eps2_u, 1e-30f);
+  float ri = rsqrt_approx(r2);
+  float r = r2 * ri;
+  float tt = rcp_approx(fmaf(a.pcx, r, 1.0f));
+  float poly = tt * fmaf(tt, fmaf(tt, fmaf(tt, fmaf(tt, ErfcConst::A5, ErfcConst::A4), ErfcConst::A3), ErfcConst::A2),
+                         ErfcConst::A1);
+  float w = poly * ex2_approx(r2 * a.ex2k);
+  return m * w * (ri * ri * ri);
+}
+
+struct Acc {
+  float sx, sy, sz, cx, cy, cz;  // Kahan sums and compensations
+  __device__ void add(float x, float y, float z) {
+    float t, v;
+    v = x - cx; t = sx + v; cx = (t - sx) - v; sx = t;
+    v = y - cy; t = sy + v; cy = (t - sy) - v; sy = t;
+    v = z - cz; t = sz + v; cz = (t - sz) - v; sz = t;
+  }
+};
+
+// Evaluate the interaction list against this lane's target.
+__device__ __forceinline__ void flush(const WalkArgs& a, const Entry* L, int nl, int lane, bool has, uint32_t p,
+                                      float thx, float thy, float thz, float tlx, float tly, float tlz, Acc& acc,
+                                      uint32_t& nleaf, uint32_t& nmono, uint32_t& nexact) {
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  const uint32_t self = p | LEAF_BIT;
+#pragma unroll 2
+  for (int e = 0; e < nl; ++e) {
+    const float4 A = *reinterpret_cast<const float4*>(&L[e].hx);
+    const float4 B = *reinterpret_cast<const float4*>(&L[e].lx);
+    const uint4 C = *reinterpret_cast<const uint4*>(&L[e].mask);
+    const float dx = (A.x - thx) + (B.x - tlx);
+    const float dy = (A.y - thy) + (B.y - tly);
+    const float dz = (A.z - thz) + (B.z - tlz);
+    const float r2b = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float ex = fmaxf(fabsf(dx) - B.w, 0.f), ey = fmaxf(fabsf(dy) - B.w, 0.f), ez = fmaxf(fabsf(dz) - B.w, 0.f);
+    const float s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+    const bool in = (C.x >> lane) & 1u;
+    bool ok = in && s <= a.rc2_lo;
+    bool amb = in && s > a.rc2_lo && s <= a.rc2_hi;
+    if (C.z == KIND_MONO) amb = amb || (in && r2b < a.tiny_u);
+    if (amb) {
+      int d = exact_terminal(a, p, C.y);
+      ++nexact;
+      if (d == 2) defer(a, p, C.y);
+      ok = d == 1;
+    }
+    float f = pair_factor(a, r2b, A.w);
+    f = ok ? f : 0.f;
+    fx = fmaf(dx, f, fx);
+    fy = fmaf(dy, f, fy);
+    fz = fmaf(dz, f, fz);
+    if (ok && C.y != self) {
+      if (C.z == KIND_LEAF) ++nleaf; else ++nmono;
+    }
+  }
+  acc.add(fx, fy, fz);
+  (void)has;
+}
+
+// Walk the tree for targets [first, first + count) (count <= 32) with one warp.
+__device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, Entry* L, uint8_t* owner,
+                             uint32_t* stk_node, uint32_t* stk_mask) {
+  const int lane = threadIdx.x & 31;
+  const bool has = (uint32_t)lane < count;
+  const uint32_t p = first + (has ? (uint32_t)lane : 0u);
+  const uint32_t tq[3] = {a.qx[p], a.qy[p], a.qz[p]};
+  uint32_t oq[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) oq[d] = __shfl_sync(0xffffffffu, tq[d], 0);
+  int32_t tr[3];
+  float th[3], tl[3], bmin[3], bmax[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    tr[d] = rel32(tq[d], oq[d], a.periodic);
+    split_rel(tr[d], a.u_inv, &th[d], &tl[d]);
+    int32_t mn = __reduce_min_sync(0xffffffffu, has ? tr[d] : 0x7FFFFFFF);
+    int32_t mx = __reduce_max_sync(0xffffffffu, has ? tr[d] : -0x7FFFFFFF);
+    bmin[d] = (float)mn * a.u_inv;
+    bmax[d] = (float)mx * a.u_inv;
+  }
+  const uint32_t mask0 = count >= 32 ? 0xFFFFFFFFu : ((1u << count) - 1u);
+  Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  uint32_t nleaf = 0, nmono = 0, nexact = 0, neval = 0;
+  int nl = 0, sp = 0;
+
+  // the first item is the root (node 0, or the single leaf when n == 1)
+  bool have = lane == 0;
+  uint32_t item = a.n_int > 0 ? 0u : LEAF_BIT;
+  uint32_t imask = mask0;
+  // each iteration pops at least one node, so a walk over a well-formed tree
+  // ends within (internal nodes + 1) iterations; the cap turns a malformed
+  // tree into an error flag instead of an endless loop
+  const int64_t max_iter = a.n_int + 2;
+  int64_t iter = 0;
+
+  for (;;) {
+    if (++iter > max_iter) {
+      if (lane == 0) atomicOr(a.err, DEV_ERR_STACK);
+      break;
+    }
+    // ---- classify this lane's item against the group box
+    bool emit = false, push = false, ambig = false;
+    Entry ent;
+    if (have && imask != 0u) {
+      uint32_t cq[3];
+      float m, h;
+      uint32_t kind;
+      bool open = false;
+      if (item & LEAF_BIT) {
+        const uint32_t j = item & ~LEAF_BIT;
+        cq[0] = a.qx[j]; cq[1] = a.qy[j]; cq[2] = a.qz[j];
+        m = a.massf[j];
+        h = a.periodic ? 0.f : ldexpf(a.h0_u, -(int)a.leaf_depth[j]);
+        kind = KIND_LEAF;
+      } else {
+        const uint4 w = a.walk[item];
+        cq[0] = w.x; cq[1] = w.y; cq[2] = w.z;
+        m = __uint_as_float(w.w);
+        const int dep = a.depth[item];
+        h = ldexpf(a.h0_u, -dep);
+        open = !(ldexp(a.h0, -dep) < a.thr);
+        kind = KIND_MONO;
+      }
+      float emin2 = 0.f, emax2 = 0.f;
+      int32_t S[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        S[d] = rel32(cq[d], oq[d], a.periodic);
+        const float sf = (float)S[d] * a.u_inv;
+        float lo_gap = fmaxf(fmaxf(bmin[d] - (sf + h), (sf - h) - bmax[d]), 0.f);
+        float far = fmaxf(fmaxf(fabsf(sf - bmin[d]), fabsf(sf - bmax[d])) - h, 0.f);
+        emin2 = fmaf(lo_gap, lo_gap, emin2);
+        emax2 = fmaf(far, far, emax2);
+      }
+      if (!(emin2 > a.grc2_hi)) {
+        if (open) {
+          push = true;
+          ambig = !(emax2 < a.grc2_lo);
+        } else {
+          emit = true;
+          split_rel(S[0], a.u_inv, &ent.hx, &ent.lx);
+          split_rel(S[1], a.u_inv, &ent.hy, &ent.ly);
+          split_rel(S[2], a.u_inv, &ent.hz, &ent.lz);
+          ent.m = m;
+          ent.h = h;
+          ent.mask = imask;
+          ent.node = item;
+          ent.kind = kind;
+          ent.pad = 0;
+        }
+      }
+    }
+    // ---- append terminal entries to the list
+    const uint32_t em = __ballot_sync(0xffffffffu, emit);
+    if (emit) {
+      const int slot = nl + __popc(em & ((1u << lane) - 1u));
+      float4* dst = reinterpret_cast<float4*>(&L[slot]);
+      dst[0] = make_float4(ent.hx, ent.hy, ent.hz, ent.m);
+      dst[1] = make_float4(ent.lx, ent.ly, ent.lz, ent.h);
+      *reinterpret_cast<uint4*>(&dst[2]) = make_uint4(ent.mask, ent.node, ent.kind, 0u);
+    }
+    nl += __popc(em);
+    // ---- push open nodes
+    const uint32_t pm = __ballot_sync(0xffffffffu, push);
+    if (sp + __popc(pm) > a.stack_cap) {
+      if (lane == 0) atomicOr(a.err, DEV_ERR_STACK);
+      break;
+    }
+    if (push) {
+      const int slot = sp + __popc(pm & ((1u << lane) - 1u));
+      stk_node[slot] = item | (ambig ? AMB_FLAG : 0u);
+      stk_mask[slot] = imask;
+    }
+    sp += __popc(pm);
+    __syncwarp();
+    if (nl > CHUNK - 32) {
+      neval += (uint32_t)nl;
+      flush(a, L, nl, lane, has, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact);
+      __syncwarp();
+      nl = 0;
+    }
+    if (sp == 0) break;
+    // ---- pop a batch whose children fill at most one warp
+    const int avail = sp < 32 ? sp : 32;
+    uint32_t enode = 0, emask = 0, nc = 0;
+    if (lane < avail) {
+      enode = stk_node[sp - 1 - lane];
+      emask = stk_mask[sp - 1 - lane];
+      nc = a.nchild[enode & NODE_MASK];
+    }
+    const uint32_t incl = warp_incl_scan(nc, lane);
+    const uint32_t take = __ballot_sync(0xffffffffu, lane < avail && incl <= 32u);
+    const int k = __popc(take);
+    sp -= k;
+    // per-target refinement of undecided open nodes
+    uint32_t amb = __ballot_sync(0xffffffffu, lane < k && (enode & AMB_FLAG));
+    while (amb) {
+      const int e = __ffs(amb) - 1;
+      amb &= amb - 1;
+      const uint32_t node = __shfl_sync(0xffffffffu, enode, e) & NODE_MASK;
+      const uint32_t me = __shfl_sync(0xffffffffu, emask, e);
+      bool pass = false;
+      if (has && ((me >> lane) & 1u)) {
+        const uint4 w = a.walk[node];
+        const int dep = a.depth[node];
+        const float h = ldexpf(a.h0_u, -dep);
+        float s = 0.f;
+        const uint32_t wq[3] = {w.x, w.y, w.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          float dd = (float)rel32(wq[d], tq[d], a.periodic) * a.u_inv;
+          float ee = fmaxf(fabsf(dd) - h, 0.f);
+          s = fmaf(ee, ee, s);
+        }
+        if (s <= a.rc2_lo) pass = true;
+        else if (s <= a.rc2_hi) {
+          pass = exact_open_pass(a, p, node);
+          ++nexact;
+        }
+      }
+      const uint32_t nm = __ballot_sync(0xffffffffu, pass);
+      if (lane == e) emask = nm;
+    }
+    // distribute the children of the popped entries over the lanes
+    const uint32_t excl = incl - nc;
+    if (lane < k)
+      for (uint32_t c = 0; c < nc; ++c) owner[excl + c] = (uint8_t)lane;
+    __syncwarp();
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, k - 1);
+    have = (uint32_t)lane < total;
+    const int o = have ? owner[lane] : 0;
+    const uint32_t onode = __shfl_sync(0xffffffffu, enode, o) & NODE_MASK;
+    const uint32_t omask = __shfl_sync(0xffffffffu, emask, o);
+    const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, o);
+    __syncwarp();
+    if (have) {
+      item = a.child_ids[a.child_first[onode] + ((uint32_t)lane - oexcl)];
+      imask = omask;
+    }
+  }
+  if (nl > 0) {
+    neval += (uint32_t)nl;
+    flush(a, L, nl, lane, has, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact);
+  }
+  __syncwarp();
+  if (has) {
+    a.ax[p] = (acc.sx) * a.out_scale;
+    a.ay[p] = (acc.sy) * a.out_scale;
+    a.az[p] = (acc.sz) * a.out_scale;
+  }
+  // statistics
+  unsigned long long l = nleaf, m = nmono, x = nexact;
+  for (int off = 16; off > 0; off >>= 1) {
+    l += __shfl_down_sync(0xffffffffu, l, off);
+    m += __shfl_down_sync(0xffffffffu, m, off);
+    x += __shfl_down_sync(0xffffffffu, x, off);
+  }
+  if (lane == 0) {
+    atomicAdd(&a.stats[0], l);
+    atomicAdd(&a.stats[1], m);
+    atomicAdd(&a.stats[2], (unsigned long long)neval * 32ull);
+    atomicAdd(&a.stats[3], x);
+  }
+}
+
+__global__ void __launch_bounds__(WALK_THREADS, 4) k_walk(WalkArgs a) {
+  __shared__ Entry s_list[WALK_WARPS][CHUNK];
+  __shared__ uint8_t s_owner[WALK_WARPS][32];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t gw = (int64_t)blockIdx.x * WALK_WARPS + wid;
+  uint32_t* stk_node = a.stack + gw * 2 * (int64_t)a.stack_cap;
+  uint32_t* stk_mask = stk_node + a.stack_cap;
+  for (;;) {
+    uint32_t g = 0;
+    if (lane == 0) g = atomicAdd(a.work, 1u);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if ((int64_t)g >= a.ngroups) break;
+    const uint32_t first = a.gfirst[g], count = a.gsize[g];
+    // a group wider than 1/8 of the box would break the shared-origin minimum
+    // image: walk its targets one at a time instead
+    const bool has = (uint32_t)lane < count;
+    const uint32_t p = first + (has ? lane : 0);
+    const uint32_t t0[3] = {a.qx[first], a.qy[first], a.qz[first]};
+    const uint32_t tq[3] = {a.qx[p], a.qy[p], a.qz[p]};
+    bool wide = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int32_t r = rel32(tq[d], t0[d], a.periodic);
+      int32_t mn = __reduce_min_sync(0xffffffffu, has ? r : 0x7FFFFFFF);
+      int32_t mx = __reduce_max_sync(0xffffffffu, has ? r : -0x7FFFFFFF);
+      wide = wide || ((int64_t)mx - (int64_t)mn > WIDE_GROUP);
+    }
+    if (!wide) {
+      walk_targets(a, first, count, s_list[wid], s_owner[wid], stk_node, stk_mask);
+    } else {
+      for (uint32_t t = 0; t < count; ++t)
+        walk_targets(a, first + t, 1u, s_list[wid], s_owner[wid], stk_node, stk_mask);
+    }
+  }
+}
+
+// ---- per-target exact walk below a node whose centre of mass coincides with
+// the target (the reference opens such a monopole, short_range.rs:316-330)
+__global__ void k_deferred(WalkArgs a, uint32_t n_items) {
+  uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= n_items || it >= a.cap_deferred) return;
+  const uint2 job = a.deferred[it];
+  const uint32_t p = job.x;
+  double xi[3];
+  target_pos(a, p, xi);
+  const uint32_t tq[3] = {a.qx[p], a.qy[p], a.qz[p]};
+  uint32_t stack[8 * 48];
+  int sp = 0;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  // open `job.y`: push its children
+  {
+    const uint32_t nd = job.y;
+    const uint32_t f = a.child_first[nd], c = a.nchild[nd];
+    for (uint32_t k = 0; k < c; ++k) stack[sp++] = a.child_ids[f + k];
+  }
+  int64_t guard = 0;
+  while (sp > 0) {
+    if (++guard > a.n_int + a.n + 2) {
+      atomicOr(a.err, DEV_ERR_STACK);
+      break;
+    }
+    const uint32_t node = stack[--sp];
+    double c[3];
+    node_com(a, node, c);
+    float m;
+    uint32_t cq[3];
+    if (node & LEAF_BIT) {
+      const uint32_t j = node & ~LEAF_BIT;
+      m = a.massf[j];
+      cq[0] = a.qx[j]; cq[1] = a.qy[j]; cq[2] = a.qz[j];
+    } else {
+      const uint4 w = a.walk[node];
+      m = __uint_as_float(w.w);
+      cq[0] = w.x; cq[1] = w.y; cq[2] = w.z;
+    }
+    const int dep = (node & LEAF_BIT) ? a.leaf_depth[node & ~LEAF_BIT] : a.depth[node];
+    const double h = ldexp(a.h0, -dep);
+    if (d2_aabb(xi, c, h, a.box, a.periodic) > a.rc2) continue;
+    bool interact = false;
+    if (node & LEAF_BIT) {
+      if ((node & ~LEAF_BIT) == p) continue;
+      interact = exact_terminal(a, p, node) == 1;
+    } else if (h < a.thr) {
+      const int d = exact_terminal(a, p, node);
+      if (d == 1) interact = true;
+      else if (d == 2) {
+        const uint32_t f = a.child_first[node], cc = a.nchild[node];
+        if (sp + (int)cc > 8 * 48) { atomicOr(a.err, DEV_ERR_STACK); break; }
+        for (uint32_t k = 0; k < cc; ++k) stack[sp++] = a.child_ids[f + k];
+      }
+    } else {
+      const uint32_t f = a.child_first[node], cc = a.nchild[node];
+      if (sp + (int)cc > 8 * 48) { atomicOr(a.err, DEV_ERR_STACK); break; }
+      for (uint32_t k = 0; k < cc; ++k) stack[sp++] = a.child_ids[f + k];
+    }
+    if (interact) {
+      const float dx = (float)rel32(cq[0], tq[0], a.periodic) * a.u_inv;
+      const float dy = (float)rel32(cq[1], tq[1], a.periodic) * a.u_inv;
+      const float dz = (float)rel32(cq[2], tq[2], a.periodic) * a.u_inv;
+      const float f = pair_factor(a, fmaf(dx, dx, fmaf(dy, dy, dz * dz)), m);
+      fx = fmaf(dx, f, fx);
+      fy = fmaf(dy, f, fy);
+      fz = fmaf(dz, f, fz);
+    }
+  }
+  atomicAdd(&a.ax[p], fx * a.out_scale);
+  atomicAdd(&a.ay[p], fy * a.out_scale);
+  atomicAdd(&a.az[p], fz * a.out_scale);
+  atomicAdd(&a.stats[4], 1ull);
+}
+
+}  // namespace
+
+int walk_blocks_per_sm() {
+  int nb = 0;
+  TPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk, WALK_THREADS, 0));
+  return nb < 1 ? 1 : nb;
+}
+int walk_threads() { return WALK_THREADS; }
+size_t walk_stack_words(int grid, int stack_cap) { return (size_t)grid * WALK_WARPS * 2 * (size_t)stack_cap; }
+
+void launch_walk(const WalkArgs& a, int grid, cudaStream_t s) {
+  k_walk<<<grid, WALK_THREADS, 0, s>>>(a);
+  TPM_LAUNCH_CHECK();
+}
+
+void launch_deferred(const WalkArgs& a, uint32_t n_items, cudaStream_t s) {
+  if (n_items == 0) return;
+  k_deferred<<<grid_for(n_items, 64, 1ll << 20), 64, 0, s>>>(a, n_items);
+  TPM_LAUNCH_CHECK();
+}
+
+}  // namespace tpm

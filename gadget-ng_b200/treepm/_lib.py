@@ -1,0 +1,136 @@
+"""ctypes binding of libtreepm_b200.so (the C ABI declared in include/treepm_b200.h).
+
+The library is the product: there is no fallback.  If it is missing or no
+sm_100 device is present, calls fail with an exception naming the cause.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtreepm_b200.so")
+
+TPM_OK = 0
+ERRORS = {
+    1: "TPM_ERR_INVALID_ARGUMENT",
+    2: "TPM_ERR_CUDA",
+    3: "TPM_ERR_OUT_OF_MEMORY",
+    4: "TPM_ERR_COINCIDENT",
+    5: "TPM_ERR_WALK_STACK",
+    6: "TPM_ERR_DEFERRED",
+    7: "TPM_ERR_NOT_READY",
+    8: "TPM_ERR_NO_DEVICE",
+    9: "TPM_ERR_NONFINITE",
+}
+
+FLAG_APERIODIC_WALK = 1 << 0
+FLAG_DECONVOLVE_CIC = 1 << 1
+FLAG_FOUR_POINT_GRADIENT = 1 << 2
+FLAG_PM_ONLY = 1 << 3
+FLAG_HILBERT_TARGETS = 1 << 4
+
+
+class TpmConfig(C.Structure):
+    _fields_ = [
+        ("grid_size", C.c_int32),
+        ("box_size", C.c_double),
+        ("r_split", C.c_double),
+        ("r_cut_factor", C.c_double),
+        ("theta", C.c_double),
+        ("opening_criterion", C.c_int32),
+        ("err_tol_force_acc", C.c_double),
+        ("flags", C.c_uint32),
+        ("device", C.c_int32),
+        ("memory_cap_bytes", C.c_int64),
+    ]
+
+
+class TpmStats(C.Structure):
+    _fields_ = [
+        ("n_particles", C.c_int64),
+        ("n_tree_nodes", C.c_int64),
+        ("n_groups", C.c_int64),
+        ("leaf_pairs", C.c_int64),
+        ("monopoles", C.c_int64),
+        ("evaluated_pairs", C.c_int64),
+        ("exact_fallbacks", C.c_int64),
+        ("deferred_opens", C.c_int64),
+        ("max_tree_depth", C.c_int32),
+        ("terminal_depth", C.c_int32),
+        ("ms_bbox_keys", C.c_float),
+        ("ms_sort", C.c_float),
+        ("ms_build", C.c_float),
+        ("ms_walk", C.c_float),
+        ("ms_pm", C.c_float),
+        ("ms_gather_kick", C.c_float),
+        ("ms_total", C.c_float),
+        ("last_error", C.c_int32),
+        ("kernel_launches", C.c_int64),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+# every exported entry point and its signature (kept in step with the header)
+_P = C.c_void_p
+_D = C.c_double
+_I64 = C.c_int64
+_I = C.c_int
+SIGNATURES = {
+    "tpm_version": ([], _I),
+    "tpm_create": ([C.POINTER(TpmConfig), C.POINTER(_P)], _I),
+    "tpm_destroy": ([_P], None),
+    "tpm_last_error": ([_P], C.c_char_p),
+    "tpm_accelerations_for_indices": ([_P, _P, _P, _I64, _D, _D, _P, _I64, _P], _I),
+    "tpm_set_particles": ([_P, _P, _P, _P, _I64], _I),
+    "tpm_set_particles_fixed": ([_P, _P, _P, _P, _I64], _I),
+    "tpm_compute_forces": ([_P, _D, _D], _I),
+    "tpm_kdk_step": ([_P, _D, _D, _D, _D, _D], _I),
+    "tpm_kdk_step_host": ([_P, _P, _P, _P, _I64, _D, _D, _D, _D, _D], _I),
+    "tpm_get_state": ([_P, _P, _P, _P], _I),
+    "tpm_get_force_parts": ([_P, _P, _P], _I),
+    "tpm_get_stats": ([_P, C.POINTER(TpmStats)], _I),
+    "tpm_set_stream": ([_P, _P], _I),
+    "tpm_get_stream": ([_P], _P),
+    "tpm_drift_kick_factors": ([_D, _D, _D, _D, _D, _P], _I),
+    "tpm_advance_a": ([_D, _D, _D, _D, _D], _D),
+    "tpm_hilbert_keys": ([_P, _P, _P], _I),
+    "tpm_cic_cells": ([_P, _P], _I),
+    "tpm_tree_node_count": ([_P], _I64),
+    "tpm_export_tree": ([_P, _I64, _P, _P, _P, _P, _P, _P, _P], _I64),
+    "tpm_get_mesh": ([_P, _P, _P, _P, _P], _I),
+    "tpm_fp32_peak": ([_I, C.POINTER(_D)], _I),
+}
+
+_lib = None
+
+
+class TreePmError(RuntimeError):
+    """A non-zero status from the C ABI (the reference panics in these cases)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+def load():
+    """Load the shared library (no fallback: raises if it is absent)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise TreePmError(2, f"{LIB_PATH} is not built; run gadget-ng_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def check(handle, rc: int) -> None:
+    if rc != TPM_OK:
+        msg = load().tpm_last_error(handle) if handle else b""
+        raise TreePmError(rc, (msg or b"").decode(errors="replace"))

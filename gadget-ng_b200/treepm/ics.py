@@ -91,7 +91,7 @@ def _displacement_field(n: int, rms_cells: float, seed: int) -> np.ndarray:
     disp = np.empty((n, n, n, 3), dtype=np.float64)
     for a, ka in enumerate((kx[:, None, None], kx[None, :, None], kz[None, None, :])):
         psi_k = 1j * ka * inv_k2 * dk
-        disp[..., a] = np.fft.irfftn(psi_k, s=(n, n, n))
+        disp[..., a] = np.fft.irfftn(psi_k, s=(n, n, n), axes=(0, 1, 2))
     rms = math.sqrt(float(np.mean(np.sum(disp * disp, axis=-1))))
     disp *= rms_cells / rms
     return disp.reshape(-1, 3)

@@ -1,0 +1,191 @@
+/*
+ * treepm_b200 — C ABI of the B200 (sm_100a) TreePM gravity solver.
+ *
+ * Drop-in boundary: gadget-ng's `GravitySolver` trait
+ * (crates/gadget-ng-core/src/gravity.rs:14-56), implemented by
+ * `TreePmSolver` (crates/gadget-ng-treepm/src/solver.rs:44-108) and
+ * `PmSolver` (crates/gadget-ng-pm/src/solver.rs:23-140), constructed by
+ * `make_solver` (crates/gadget-ng-cli/src/engine/gravity.rs:352-556).  The
+ * integrator-side fused step replaces `leapfrog_cosmo_kdk_step`
+ * (crates/gadget-ng-integrators/src/leapfrog.rs:72-91).  The existing CUDA PM
+ * FFI of the reference (crates/gadget-ng-cuda/cuda/pm_gravity.h:11-66) is the
+ * pattern: an opaque handle, plain pointers and sizes, an int status.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (TPM_OK == 0) and never aborts;
+ *    tpm_last_error() gives a message for the last failure on a handle.
+ *  - Host buffers are caller-owned and copied synchronously inside the call.
+ *    Device state is handle-owned and persists between calls.
+ *  - A handle is not thread-safe: one host thread per handle, as the
+ *    reference calls its solver from one thread at a time
+ *    (crates/gadget-ng-cuda/src/pm_solver.rs:29-34).
+ *  - Positions are stored on the device as 32-bit fixed point per axis in
+ *    the periodic box (x = q * L / 2^32); inputs on that lattice round-trip
+ *    exactly.
+ */
+#ifndef TREEPM_B200_H
+#define TREEPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+  TPM_OK = 0,
+  TPM_ERR_INVALID_ARGUMENT = 1,
+  TPM_ERR_CUDA = 2,            /* a CUDA runtime call failed */
+  TPM_ERR_OUT_OF_MEMORY = 3,   /* device allocation refused (or over the handle's memory cap) */
+  TPM_ERR_COINCIDENT = 4,      /* two particles at the same position: the reference's
+                                  insertion octree recurses without bound on these
+                                  (crates/gadget-ng-tree/src/octree.rs:501-540) */
+  TPM_ERR_WALK_STACK = 5,      /* tree-walk stack capacity exceeded */
+  TPM_ERR_DEFERRED = 6,        /* exact-fallback work list overflowed */
+  TPM_ERR_NOT_READY = 7,       /* call needs particles / forces that are not set */
+  TPM_ERR_NO_DEVICE = 8,       /* no CUDA device, or the device is not sm_100 */
+  TPM_ERR_NONFINITE = 9        /* non-finite input position or mass */
+};
+
+/* ---- configuration flags -------------------------------------------------- */
+/* Short range with the aperiodic walk of short_range.rs:120-208 (the
+ * trait-level TreePmSolver).  Default: the periodic walk of
+ * short_range.rs:234-333 (treepm_slab at P=1). */
+#define TPM_FLAG_APERIODIC_WALK     (1u << 0)
+/* Divide the Green's function by the CIC window squared (extension; the
+ * reference force path has no deconvolution). */
+#define TPM_FLAG_DECONVOLVE_CIC     (1u << 1)
+/* 4-point finite-difference gradient in k-space instead of the exact i·k of
+ * fft_poisson.rs:542-548 (extension). */
+#define TPM_FLAG_FOUR_POINT_GRADIENT (1u << 2)
+/* Plain PM (PmSolver): no Gaussian filter, no short range. */
+#define TPM_FLAG_PM_ONLY            (1u << 3)
+/* Group walk targets along the Hilbert curve of sfc.rs:95-204 instead of the
+ * octree's own order. */
+#define TPM_FLAG_HILBERT_TARGETS    (1u << 4)
+
+typedef struct tpm_config {
+  int32_t grid_size;          /* [gravity] pm_grid_size (power of two, 8..1024) */
+  double box_size;            /* [simulation] box_size */
+  double r_split;             /* [gravity] r_split; <= 0 selects 2.5 cells (solver.rs:56-62) */
+  double r_cut_factor;        /* extension key gravity.r_cut_factor; <= 0 selects 5.0 (solver.rs:80) */
+  double theta;               /* [gravity] theta (kept for the TOML contract; unused by the TreePM walk) */
+  int32_t opening_criterion;  /* [gravity] opening_criterion: 0 geometric, 1 relative (unused by TreePM) */
+  double err_tol_force_acc;   /* [gravity] err_tol_force_acc (unused by TreePM) */
+  uint32_t flags;             /* TPM_FLAG_* */
+  int32_t device;             /* CUDA device ordinal */
+  int64_t memory_cap_bytes;   /* 0 = no cap; otherwise refuse allocations beyond it */
+} tpm_config;
+
+typedef struct tpm_stats {
+  int64_t n_particles;
+  int64_t n_tree_nodes;         /* internal octree nodes (non-empty) */
+  int64_t n_groups;             /* walk target groups */
+  int64_t leaf_pairs;           /* particle-particle interactions of the last walk */
+  int64_t monopoles;            /* particle-node interactions of the last walk */
+  int64_t evaluated_pairs;      /* pair evaluations issued, including masked ones */
+  int64_t exact_fallbacks;      /* borderline decisions resolved in FP64 */
+  int64_t deferred_opens;       /* nodes opened per target (COM on the target) */
+  int32_t max_tree_depth;
+  int32_t terminal_depth;       /* first depth whose half size is < 0.1 r_cut */
+  /* device milliseconds of the last force evaluation, per stage */
+  float ms_bbox_keys;
+  float ms_sort;
+  float ms_build;
+  float ms_walk;
+  float ms_pm;
+  float ms_gather_kick;
+  float ms_total;
+  int32_t last_error;
+  int64_t kernel_launches;      /* kernels launched by the last call that computed forces */
+} tpm_stats;
+
+typedef struct tpm_handle tpm_handle;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+/* make_solver (crates/gadget-ng-cli/src/engine/gravity.rs:511-517) +
+ * TreePmSolver { grid_size, box_size, r_split } (solver.rs:44-52). */
+int tpm_create(const tpm_config* cfg, tpm_handle** out);
+void tpm_destroy(tpm_handle* h);
+const char* tpm_last_error(const tpm_handle* h);
+int tpm_version(void);
+
+/* ---- the GravitySolver call ----------------------------------------------
+ * accelerations_for_indices(global_positions, global_masses, eps2, g,
+ * global_indices, out) — crates/gadget-ng-core/src/gravity.rs:16-24.
+ * positions: n x 3 float64 (AoS, like &[Vec3]); masses: n float64;
+ * indices: n_idx uint64 (usize); out: n_idx x 3 float64.
+ * out.len() == global_indices.len() is the reference's assertion
+ * (solver.rs:75); here n_idx sizes both. */
+int tpm_accelerations_for_indices(tpm_handle* h, const double* global_positions, const double* global_masses,
+                                  int64_t n, double eps2, double g, const uint64_t* global_indices,
+                                  int64_t n_idx, double* out);
+
+/* ---- device-resident state (the fused integrator path) ----------------- */
+/* Upload particles: positions n x 3 float64 (wrapped into the box), velocities
+ * n x 3 float64 (canonical momentum p = a^2 dx/dt, may be NULL = zero),
+ * masses n float64. */
+int tpm_set_particles(tpm_handle* h, const double* pos, const double* vel, const double* mass, int64_t n);
+/* Same, with positions already in 32-bit fixed point (n x 3). */
+int tpm_set_particles_fixed(tpm_handle* h, const uint32_t* q, const float* vel, const double* mass, int64_t n);
+/* One force evaluation of all resident particles (results stay on the device). */
+int tpm_compute_forces(tpm_handle* h, double eps2, double g);
+/* leapfrog_cosmo_kdk_step (leapfrog.rs:72-91) + wrap_position
+ * (crates/gadget-ng-core/src/cosmology.rs:772-778) fused on the device.
+ * The opening half kick reuses the previous step's closing acceleration,
+ * rescaled by g / g_prev when only the coupling G*a^3 changed; it recomputes
+ * when eps2 changed or no acceleration is cached. */
+int tpm_kdk_step(tpm_handle* h, double kick_half, double drift, double kick_half2, double eps2, double g);
+/* Host KDK step: state in host buffers (n x 3 float64 pos / vel), copied to
+ * the device, advanced by tpm_kdk_step, copied back (original order). */
+int tpm_kdk_step_host(tpm_handle* h, double* pos, double* vel, const double* mass, int64_t n, double kick_half,
+                      double drift, double kick_half2, double eps2, double g);
+/* Read back state in the original particle order (any pointer may be NULL). */
+int tpm_get_state(tpm_handle* h, double* pos, double* vel, double* acc);
+/* Long-range and short-range parts of the last force evaluation (original
+ * order, n x 3 float64 each; either may be NULL). */
+int tpm_get_force_parts(tpm_handle* h, double* acc_lr, double* acc_sr);
+int tpm_get_stats(const tpm_handle* h, tpm_stats* out);
+
+/* ---- the stream the handle launches on ----------------------------------- */
+int tpm_set_stream(tpm_handle* h, void* cuda_stream);
+void* tpm_get_stream(const tpm_handle* h);
+
+/* ---- cosmology (FP64 host) ------------------------------------------------
+ * CosmologyParams::drift_kick_factors (crates/gadget-ng-core/src/cosmology.rs:188-233)
+ * for LambdaCDM: out3 = {drift, kick_half, kick_half2}. */
+int tpm_drift_kick_factors(double omega_m, double omega_lambda, double h0, double a0, double dt, double* out3);
+/* CosmologyParams::advance_a (cosmology.rs:172-178). */
+double tpm_advance_a(double omega_m, double omega_lambda, double h0, double a, double dt);
+
+/* ---- inspection of the hot-path stages (parity tests) ------------------- */
+/* Hilbert keys of the resident particles (particle_hilbert, sfc.rs:187-204,
+ * bounding box from the positions) and their (key, original index) order. */
+int tpm_hilbert_keys(tpm_handle* h, uint64_t* keys, int64_t* order);
+/* CIC base cell (ix0, iy0, iz0) of each resident particle, original order
+ * (cic.rs:49-55). */
+int tpm_cic_cells(tpm_handle* h, int32_t* cells);
+/* Number of non-empty octree nodes of the last force evaluation. */
+int64_t tpm_tree_node_count(const tpm_handle* h);
+/* Export the non-empty octree nodes: per node depth, mass, COM (float64),
+ * quadrupole (6), the original index of the particle for leaves (-1 for
+ * internal nodes) and the octant path key (3 bits per level, root = 1).  cap
+ * is the array capacity; returns the count written (or a negative status). */
+int64_t tpm_export_tree(tpm_handle* h, int64_t cap, int32_t* depth, double* mass, double* com, double* quad,
+                        int64_t* particle, uint64_t* path_hi, uint64_t* path_lo);
+/* The PM mesh of the last force evaluation: density (mass per cell, nm^3)
+ * and the three force grids (nm^3 each), float32; any may be NULL. */
+int tpm_get_mesh(tpm_handle* h, float* density, float* fx, float* fy, float* fz);
+
+/* ---- measurement -----------------------------------------------------------
+ * No counterpart in the reference: FFMA throughput of `device` in TFLOP/s, the
+ * FP32 roofline denominator of the short-range walk. */
+int tpm_fp32_peak(int device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TREEPM_B200_H */

@@ -51,6 +51,7 @@ def lib():
             "orc_treepm": ([_p, _p, _i64, _d, _d, _i32, _d, _d, _d, _i32, _i32, _p, _i64, _p, _p, _p, _p, _p],
                            _i32),
             "orc_pm": ([_p, _p, _i64, _d, _i32, _d, _i32, _p, _i64, _p], None),
+            "orc_cic_cells": ([_p, _i64, _d, _i32, _p], None),
             "orc_hilbert3": ([_d, _d, _d], C.c_uint64),
             "orc_morton3": ([_d, _d, _d], C.c_uint64),
             "orc_coords_to_hilbert": ([C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32], C.c_uint64),
@@ -202,6 +203,40 @@ def pm(pos, mass, g, nm, box, targets=None, pm_flags=0):
     lib().orc_pm(_ptr(pos), _ptr(mass), n, float(g), int(nm), float(box), int(pm_flags), _ptr(t), t.shape[0],
                  _ptr(out))
     return out
+
+
+def cic_cells(pos, box, nm):
+    pos = _f64(pos)
+    out = np.zeros((pos.shape[0], 3), dtype=np.int32)
+    lib().orc_cic_cells(_ptr(pos), pos.shape[0], float(box), int(nm), _ptr(out))
+    return out
+
+
+def octree_paths(tree):
+    """(depth, path_hi, path_lo) of every non-empty node, paths packed like the
+    device export: 3 bits per level from bit 62 down, levels 22.. in path_lo."""
+    ch = tree["children"]
+    n = ch.shape[0]
+    hi = np.zeros(n, dtype=np.uint64)
+    lo = np.zeros(n, dtype=np.uint64)
+    depth = tree["depth"]
+    stack = [0]
+    while stack:
+        i = stack.pop()
+        for o in range(8):
+            c = int(ch[i, o])
+            if c == 0xFFFFFFFF:
+                continue
+            d = int(depth[c])
+            h, l = int(hi[i]), int(lo[i])
+            if d <= 21:
+                h |= o << (63 - 3 * d)
+            else:
+                l |= o << (63 - 3 * (d - 21))
+            hi[c], lo[c] = h, l
+            stack.append(c)
+    keep = tree["mass"] > 0
+    return keep, hi, lo
 
 
 def hilbert3(x, y, z) -> int:

@@ -900,6 +900,14 @@ void orc_pm(const double* pos, const double* mass, int64_t n, double g, int nm, 
   cic_interpolate(fx.data(), fy.data(), fz.data(), tpos.data(), nt, box, nm, out);
 }
 
+// CIC base cells (ix0, iy0, iz0) of each particle: cic.rs:49-55.
+void orc_cic_cells(const double* pos, int64_t n, double box, int nm, int32_t* cells) {
+  const double inv_cell = (double)nm / box;
+  const double nmf = (double)nm;
+  for (int64_t i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) cells[3 * i + c] = (int32_t)std::floor(rem_euclid(pos[3 * i + c] * inv_cell, nmf));
+}
+
 uint64_t orc_hilbert3(double x, double y, double z) { return hilbert3(x, y, z); }
 uint64_t orc_morton3(double x, double y, double z) { return morton3(x, y, z); }
 uint64_t orc_coords_to_hilbert(uint32_t ix, uint32_t iy, uint32_t iz, uint32_t p) {

@@ -1,0 +1,131 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports every
+entry point the header declares, fails loudly without a device, and the
+host-side logic (cosmology factors, FFT indexing, workload generators)
+matches the oracle."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import REPO, oracle
+
+HEADER = os.path.join(REPO, "include", "treepm_b200.h")
+
+
+def header_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tpm_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    import treepm._lib as L
+    lib = ctypes.CDLL(L.LIB_PATH)
+    names = header_functions()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), name
+    # the Python binding declares exactly the header's functions
+    assert sorted(L.SIGNATURES) == names
+
+
+def test_library_is_sm100a_only():
+    import treepm._lib as L
+    out = os.popen(f"/usr/local/cuda/bin/cuobjdump --list-elf {L.LIB_PATH} 2>/dev/null").read()
+    if not out:
+        pytest.skip("cuobjdump unavailable")
+    archs = set(re.findall(r"sm_(\d+a?)", out))
+    assert archs == {"100a"}, archs
+
+
+def test_create_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import treepm
+    with pytest.raises(treepm.TreePmError) as e:
+        treepm.TreePmSolver(32, 100.0)
+    assert e.value.code == 8  # TPM_ERR_NO_DEVICE
+
+
+def test_drift_kick_factors_bitwise_equal_to_oracle():
+    import treepm
+    for args in ((0.31, 0.69, 1.0, 0.02, 0.001), (0.31, 0.69, 1.0, 0.1, 0.004), (1.0, 0.0, 1.0, 1.0, 0.05)):
+        assert treepm.drift_kick_factors(*args) == oracle().drift_kick_factors(*args)
+        assert treepm.advance_a(*args) == oracle().advance_a(*args)
+
+
+def test_gravity_coupling():
+    import treepm
+    assert treepm.gravity_coupling_qksl(2.0, 0.5) == 2.0 * 0.5 * 0.5 * 0.5
+
+
+def _stockham_mirror(x, inverse=False):
+    """The radix-2 Stockham indexing of the device FFT (pm.cu fft_smem)."""
+    n = len(x)
+    logn = n.bit_length() - 1
+    a = x.astype(complex).copy()
+    b = np.empty_like(a)
+    tw = np.exp(-2j * np.pi * np.arange(n // 2) / n)
+    Ns = 1
+    for s in range(logn):
+        for j in range(n // 2):
+            k = j & (Ns - 1)
+            w = tw[k << (logn - 1 - s)]
+            if inverse:
+                w = np.conj(w)
+            x0, x1 = a[j], a[j + n // 2] * w
+            o = ((j - k) << 1) + k
+            b[o], b[o + Ns] = x0 + x1, x0 - x1
+        a, b = b, a
+        Ns *= 2
+    return a
+
+
+@pytest.mark.parametrize("n", [2, 4, 8, 32, 128])
+def test_stockham_indexing_is_a_dft(n):
+    x = np.random.default_rng(n).standard_normal(n) + 1j * np.random.default_rng(n + 1).standard_normal(n)
+    assert np.max(np.abs(_stockham_mirror(x) - np.fft.fft(x))) < 1e-12 * n
+    assert np.max(np.abs(_stockham_mirror(x, True) - n * np.fft.ifft(x))) < 1e-12 * n
+
+
+def test_half_spectrum_gradient_equals_real_part_of_full():
+    """Zeroing the derivative's Nyquist plane reproduces Re(ifft(-i k phi)) of the
+    reference's full complex transform (fft_poisson.rs:542-548, :466-473)."""
+    nm = 8
+    rng = np.random.default_rng(3)
+    rho = rng.standard_normal((nm, nm, nm))
+    k = 2 * np.pi * np.array([j if j <= nm // 2 else j - nm for j in range(nm)])
+    K = np.meshgrid(k, k, k, indexing="ij")  # axes (z, y, x)
+    k2 = K[0] ** 2 + K[1] ** 2 + K[2] ** 2
+    rk = np.fft.fftn(rho)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        phi = np.where(k2 > 0, -rk / k2, 0)
+    for axis in range(3):
+        full = np.real(np.fft.ifftn(-1j * K[axis] * phi))
+        d = K[axis].copy()
+        d[np.isclose(np.abs(d), np.pi * nm)] = 0.0
+        half = np.fft.irfftn((-1j * d * phi)[:, :, : nm // 2 + 1], s=(nm, nm, nm))
+        assert np.max(np.abs(full - half)) < 1e-12
+
+
+def test_workloads_are_seeded_and_distinct():
+    from treepm import ics
+    a = ics.lattice_box(16, 100.0, 1.0, seed=3)
+    b = ics.lattice_box(16, 100.0, 1.0, seed=3)
+    assert np.array_equal(a.q, b.q)
+    c = ics.clustered_box(16, 200.0, 0.3, 5, min_halo=10, max_halo=100, seed=4)
+    for box in (a, c):
+        u = np.unique(box.q.view([("x", np.uint32), ("y", np.uint32), ("z", np.uint32)]))
+        assert len(u) == box.n
+    x = a.positions()
+    assert np.all(x >= 0) and np.all(x < 100.0)
+    assert np.array_equal(ics.encode(x, 100.0), a.q)  # exact round trip
+
+
+def test_rms_displacement_scaling():
+    from treepm import ics
+    disp = ics._displacement_field(16, 0.2, 1)
+    assert abs(np.sqrt(np.mean(np.sum(disp ** 2, axis=1))) - 0.2) < 1e-12
