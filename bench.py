@@ -242,7 +242,7 @@ def run_b200(args):
     value = world * n * args.steps / (dev_ms * 1e-3)
 
     # ---- end to end through the host-buffer API (e2e) -------------------
-    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
     pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     vel = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     mass = torch.empty((n,), dtype=torch.float64, pin_memory=True).numpy()
@@ -250,7 +250,8 @@ def run_b200(args):
     vel[:] = 0.0
     mass[:] = box.mass
     d, k1, k2, g = factors[0]
-    solver.kdk_step_host(pos, vel, mass, k1, d, k2, phys["eps2"], g)  # warm
+    if e2e_steps:
+        solver.kdk_step_host(pos, vel, mass, k1, d, k2, phys["eps2"], g)  # warm
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -266,7 +267,7 @@ def run_b200(args):
     te = torch.tensor([e2e_wall], device="cuda")
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * e2e_steps / float(te.item())
+    e2e_value = world * n * e2e_steps / float(te.item()) if e2e_steps else None
     h2d = n * (24 + 24 + 8)
     d2h = n * (24 + 24)
 
@@ -275,7 +276,7 @@ def run_b200(args):
     evaluated = float(np.mean([s["evaluated_pairs"] for s in stats]))
     wms = float(np.mean(walk_ms))
     achieved = inter * FLOP_PER_INTERACTION / (wms * 1e-3) / 1e12
-    peak = fp32_peak_tflops(solver)
+    peak = None if args.no_peak else fp32_peak_tflops(solver)
     st = stats[-1]
     line = {
         "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s", "n_gpus": world,
@@ -332,6 +333,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-targets", type=int, default=65536)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak measurement (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

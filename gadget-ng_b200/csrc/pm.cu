@@ -141,7 +141,7 @@ __global__ void k_cells(const uint32_t* __restrict__ qx, const uint32_t* __restr
 
 // ---- x pass: real rows -> half spectrum ----------------------------------------
 __global__ void k_fft_x_r2c(const float* __restrict__ rho, float2* __restrict__ spec, int nm, int logn, int nh,
-                            int rows, const float2* __restrict__ tw) {
+                            int rows, int64_t nrows, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
   float2* s_tw = sm;
   float2* a = sm + (nm >> 1);
@@ -150,13 +150,13 @@ __global__ void k_fft_x_r2c(const float* __restrict__ rho, float2* __restrict__ 
   const int64_t row0 = (int64_t)blockIdx.x * rows;
   for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
     const int r = idx / nm, j = idx % nm;
-    a[idx] = make_float2(rho[(row0 + r) * nm + j], 0.f);
+    a[idx] = make_float2(row0 + r < nrows ? rho[(row0 + r) * nm + j] : 0.f, 0.f);
   }
   __syncthreads();
   const float2* res = fft_smem<true>(a, b, nm, logn, rows, s_tw, false);
   for (int idx = threadIdx.x; idx < rows * nh; idx += blockDim.x) {
     const int r = idx / nh, k = idx % nh;
-    spec[(row0 + r) * nh + k] = res[r * nm + k];
+    if (row0 + r < nrows) spec[(row0 + r) * nh + k] = res[r * nm + k];
   }
 }
 
@@ -242,24 +242,25 @@ __global__ void k_fft_z_poisson(const float2* __restrict__ spec, float2* __restr
 
 // ---- inverse x pass: half spectrum rows -> real rows -------------------------------
 __global__ void k_fft_x_c2r(const float2* __restrict__ spec3, float* __restrict__ force, int nm, int logn, int nh,
-                            int rows, const float2* __restrict__ tw) {
+                            int rows, int64_t nrows, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
   float2* s_tw = sm;
   float2* a = sm + (nm >> 1);
   float2* b = a + rows * nm;
   load_twiddles(s_tw, tw, nm);
   const int comp = blockIdx.y;
-  const int64_t nrows = (int64_t)nm * nm;
   const float2* in = spec3 + comp * nrows * nh;
   float* out = force + comp * nrows * nm;
   const int64_t row0 = (int64_t)blockIdx.x * rows;
   for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
     const int r = idx / nm, k = idx % nm;
-    float2 v;
-    if (k < nh) v = in[(row0 + r) * nh + k];
-    else {
-      v = in[(row0 + r) * nh + (nm - k)];
-      v.y = -v.y;
+    float2 v = make_float2(0.f, 0.f);
+    if (row0 + r < nrows) {
+      if (k < nh) v = in[(row0 + r) * nh + k];
+      else {
+        v = in[(row0 + r) * nh + (nm - k)];
+        v.y = -v.y;
+      }
     }
     a[idx] = v;
   }
@@ -267,7 +268,7 @@ __global__ void k_fft_x_c2r(const float2* __restrict__ spec3, float* __restrict_
   const float2* res = fft_smem<true>(a, b, nm, logn, rows, s_tw, true);
   for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
     const int r = idx / nm, j = idx % nm;
-    out[(row0 + r) * nm + j] = res[idx].x;
+    if (row0 + r < nrows) out[(row0 + r) * nm + j] = res[idx].x;
   }
 }
 
@@ -320,7 +321,11 @@ inline int ilog2(int n) {
   while ((1 << l) < n) ++l;
   return l;
 }
-inline int rows_for(int nm) { return nm >= 4096 ? 1 : 4096 / nm; }
+// rows of one x-pass block: 4096 complex values, never more than the mesh has
+inline int rows_for(int nm) {
+  int r = nm >= 4096 ? 1 : 4096 / nm;
+  return r > nm * nm ? nm * nm : r;
+}
 inline int tx_for(int nm) {
   int t = 4096 / nm;
   return t < 4 ? 4 : (t > 16 ? 16 : t);
@@ -414,7 +419,7 @@ void pm_solve(const PmPlan& p, cudaStream_t s) {
   const size_t sm_z = sizeof(float2) * ((size_t)(nm / 2) + 3 * (size_t)nm * tx);
   const int nblk_x = (int)((nrows + rows - 1) / rows);
   const int ntx = (nh + tx - 1) / tx;
-  k_fft_x_r2c<<<nblk_x, 256, sm_x, s>>>(p.rho, p.spec, nm, logn, nh, rows, p.twiddle);
+  k_fft_x_r2c<<<nblk_x, 256, sm_x, s>>>(p.rho, p.spec, nm, logn, nh, rows, nrows, p.twiddle);
   TPM_LAUNCH_CHECK();
   k_fft_y<<<dim3(ntx, nm, 1), 256, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
   TPM_LAUNCH_CHECK();
@@ -423,7 +428,7 @@ void pm_solve(const PmPlan& p, cudaStream_t s) {
   TPM_LAUNCH_CHECK();
   k_fft_y<<<dim3(ntx, nm, 3), 256, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
   TPM_LAUNCH_CHECK();
-  k_fft_x_c2r<<<dim3(nblk_x, 3), 256, sm_x, s>>>(p.spec3, p.force, nm, logn, nh, rows, p.twiddle);
+  k_fft_x_c2r<<<dim3(nblk_x, 3), 256, sm_x, s>>>(p.spec3, p.force, nm, logn, nh, rows, nrows, p.twiddle);
   TPM_LAUNCH_CHECK();
 }
 

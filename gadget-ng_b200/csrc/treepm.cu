@@ -183,6 +183,7 @@ struct tpm_handle {
   float *ax = nullptr, *ay = nullptr, *az = nullptr;
   float *srx = nullptr, *sry = nullptr, *srz = nullptr;
   float *lrx = nullptr, *lry = nullptr, *lrz = nullptr;
+  uint32_t* pcounts = nullptr;
   TreeBuffers T{};
   PmPlan pm;
   void* sort_scratch = nullptr;
@@ -291,6 +292,7 @@ void ensure_capacity(tpm_handle* h, int64_t n) {
   h->lrx = h->alloc<float>(c, 1);
   h->lry = h->alloc<float>(c, 1);
   h->lrz = h->alloc<float>(c, 1);
+  h->pcounts = h->alloc<uint32_t>(2 * c, 1);
   T.key_hi = h->alloc<uint64_t>(c, 1);
   T.key_lo = h->alloc<uint64_t>(c, 1);
   T.key_lo_tmp = h->alloc<uint64_t>(c, 1);
@@ -414,6 +416,7 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       a.scale = scale; a.box = box; a.rc2 = h->rc2; a.thr = h->thr; a.h0 = h0;
       a.periodic = h->periodic ? 1 : 0;
       a.u_inv = (float)std::ldexp(1.0, -U);
+      a.box_u = (float)std::ldexp(1.0, 32 - U);
       a.h0_u = (float)(h0 / u);
       const double rc2_u = h->rc2 / (u * u);
       a.rc2_lo = (float)(rc2_u * (1.0 - 1e-4));
@@ -431,6 +434,8 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       a.stats = h->stats_dev; a.err = T.err;
       a.deferred = h->deferred; a.ndeferred = h->ndeferred; a.cap_deferred = DEFERRED_CAP;
       a.stack = h->stack; a.stack_cap = STACK_CAP;
+      a.single_target = h->r_cut > 0.2 * box ? 1 : 0;
+      a.pcounts = h->pcounts;
       TPM_CUDA(cudaMemsetAsync(h->work, 0, sizeof(uint32_t), s));
       TPM_CUDA(cudaMemsetAsync(h->ndeferred, 0, sizeof(uint32_t), s));
       launch_walk(a, h->walk_grid, s);
@@ -561,8 +566,7 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
     h->thr = 0.1 * std::sqrt(h->rc2);  // short_range.rs:320
     h->periodic = !(cfg->flags & TPM_FLAG_APERIODIC_WALK);
     h->pm_only = (cfg->flags & TPM_FLAG_PM_ONLY) != 0;
-    if (!h->pm_only && h->r_cut >= 0.5 * cfg->box_size)
-      throw Error(TPM_ERR_INVALID_ARGUMENT, "r_cut must be below half the box");
+    if (!(h->r_cut > 0.0) || !std::isfinite(h->r_cut)) throw Error(TPM_ERR_INVALID_ARGUMENT, "r_cut must be positive");
     TPM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
     for (auto& e : h->ev) TPM_CUDA(cudaEventCreate(&e));
@@ -796,6 +800,26 @@ int tpm_get_force_parts(tpm_handle* h, double* acc_lr, double* acc_sr) {
         TPM_CUDA(cudaMemcpyAsync(acc_sr, h->staging, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
         TPM_CUDA(cudaStreamSynchronize(s));
       }
+    }
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_get_interaction_counts(tpm_handle* h, int64_t* counts) {
+  if (!h || !counts) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (!h->forces_valid || h->pm_only || h->n < 2) throw Error(TPM_ERR_NOT_READY, "no short-range walk computed");
+    const int64_t n = h->n;
+    std::vector<uint32_t> c((size_t)2 * n), id((size_t)n);
+    TPM_CUDA(cudaMemcpyAsync(c.data(), h->pcounts, sizeof(uint32_t) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
+    TPM_CUDA(cudaMemcpyAsync(id.data(), h->P[h->cur].id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, h->stream));
+    TPM_CUDA(cudaStreamSynchronize(h->stream));
+    for (int64_t i = 0; i < n; ++i) {
+      counts[2 * (int64_t)id[i]] = c[2 * i];
+      counts[2 * (int64_t)id[i] + 1] = c[2 * i + 1];
     }
   } catch (const Error& e) {
     return fail(h, e);

@@ -37,7 +37,7 @@ constexpr int WALK_THREADS = WALK_WARPS * 32;
 constexpr int CHUNK = 96;
 constexpr uint32_t AMB_FLAG = 0x40000000u;
 constexpr uint32_t NODE_MASK = 0x3FFFFFFFu;
-constexpr int32_t WIDE_GROUP = 1 << 29;  // quanta: 1/8 of the box
+constexpr int32_t WIDE_GROUP = 1 << 28;  // quanta: 1/16 of the box
 
 enum : uint32_t { KIND_LEAF = 0, KIND_MONO = 1 };
 
@@ -277,15 +277,27 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
         open = !(ldexp(a.h0, -dep) < a.thr);
         kind = KIND_MONO;
       }
+      // Per axis, the targets see the node at the minimum image of S - t for t
+      // in [bmin, bmax]: bound min / max of |wrap(S - t)| over that interval
+      // (images at 0 and +-L), then the AABB gap.
       float emin2 = 0.f, emax2 = 0.f;
       int32_t S[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         S[d] = rel32(cq[d], oq[d], a.periodic);
         const float sf = (float)S[d] * a.u_inv;
-        float lo_gap = fmaxf(fmaxf(bmin[d] - (sf + h), (sf - h) - bmax[d]), 0.f);
-        float far = fmaxf(fmaxf(fabsf(sf - bmin[d]), fabsf(sf - bmax[d])) - h, 0.f);
-        emin2 = fmaf(lo_gap, lo_gap, emin2);
+        const float lo = sf - bmax[d], hi = sf - bmin[d];
+        float dmin = lo > 0.f ? lo : (hi < 0.f ? -hi : 0.f);
+        float dmax = fmaxf(fabsf(lo), fabsf(hi));
+        if (a.periodic) {
+          dmin = fminf(dmin, fminf(a.box_u - hi, lo + a.box_u));
+          const float half = 0.5f * a.box_u;
+          if (lo <= -half || hi >= half) dmax = half;
+          else dmax = fminf(dmax, half);
+        }
+        const float gap = fmaxf(dmin - h, 0.f);
+        const float far = fmaxf(dmax - h, 0.f);
+        emin2 = fmaf(gap, gap, emin2);
         emax2 = fmaf(far, far, emax2);
       }
       if (!(emin2 > a.grc2_hi)) {
@@ -403,6 +415,8 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     a.ax[p] = (acc.sx) * a.out_scale;
     a.ay[p] = (acc.sy) * a.out_scale;
     a.az[p] = (acc.sz) * a.out_scale;
+    a.pcounts[2 * (int64_t)p] = nleaf;
+    a.pcounts[2 * (int64_t)p + 1] = nmono;
   }
   // statistics
   unsigned long long l = nleaf, m = nmono, x = nexact;
@@ -446,6 +460,7 @@ __global__ void __launch_bounds__(WALK_THREADS, 4) k_walk(WalkArgs a) {
       int32_t mx = __reduce_max_sync(0xffffffffu, has ? r : -0x7FFFFFFF);
       wide = wide || ((int64_t)mx - (int64_t)mn > WIDE_GROUP);
     }
+    wide = wide || a.single_target;
     if (!wide) {
       walk_targets(a, first, count, s_list[wid], s_owner[wid], stk_node, stk_mask);
     } else {
@@ -515,6 +530,7 @@ __global__ void k_deferred(WalkArgs a, uint32_t n_items) {
       for (uint32_t k = 0; k < cc; ++k) stack[sp++] = a.child_ids[f + k];
     }
     if (interact) {
+      atomicAdd(&a.pcounts[2 * (int64_t)p + ((node & LEAF_BIT) ? 0 : 1)], 1u);
       const float dx = (float)rel32(cq[0], tq[0], a.periodic) * a.u_inv;
       const float dy = (float)rel32(cq[1], tq[1], a.periodic) * a.u_inv;
       const float dz = (float)rel32(cq[2], tq[2], a.periodic) * a.u_inv;

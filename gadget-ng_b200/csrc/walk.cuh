@@ -29,6 +29,7 @@ struct WalkArgs {
   double scale, box, rc2, thr, h0;
   int periodic;
   float u_inv;    // 2^-U: quanta -> walk units u = scale * 2^U
+  float box_u;    // box side in walk units (2^32 quanta)
   float h0_u;     // root half side in u
   float rc2_lo, rc2_hi;    // per-target ambiguity band around r_cut^2 (u^2)
   float grc2_lo, grc2_hi;  // group-level band
@@ -48,6 +49,8 @@ struct WalkArgs {
   uint32_t cap_deferred;
   uint32_t* stack;
   int stack_cap;
+  int single_target;     // walk every target alone (r_cut above a quarter box)
+  uint32_t* pcounts;     // per target (sorted order): leaf pairs, monopoles
 };
 
 int walk_blocks_per_sm();

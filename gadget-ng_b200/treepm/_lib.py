@@ -92,6 +92,7 @@ SIGNATURES = {
     "tpm_get_state": ([_P, _P, _P, _P], _I),
     "tpm_get_force_parts": ([_P, _P, _P], _I),
     "tpm_get_stats": ([_P, C.POINTER(TpmStats)], _I),
+    "tpm_get_interaction_counts": ([_P, _P], _I),
     "tpm_set_stream": ([_P, _P], _I),
     "tpm_get_stream": ([_P], _P),
     "tpm_drift_kick_factors": ([_D, _D, _D, _D, _D, _P], _I),

@@ -134,6 +134,12 @@ class TreePmSolver:
         check(self._h.h, self._h._lib.tpm_get_force_parts(self._h.h, _ptr(lr), _ptr(sr)))
         return lr, sr
 
+    def interaction_counts(self, n: int):
+        """(n, 2) leaf pairs and monopoles of the last walk, per particle."""
+        c = np.empty((n, 2), dtype=np.int64)
+        check(self._h.h, self._h._lib.tpm_get_interaction_counts(self._h.h, _ptr(c)))
+        return c
+
     def stats(self) -> dict:
         s = TpmStats()
         check(self._h.h, self._h._lib.tpm_get_stats(self._h.h, C.byref(s)))

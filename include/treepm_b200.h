@@ -148,6 +148,10 @@ int tpm_get_state(tpm_handle* h, double* pos, double* vel, double* acc);
  * order, n x 3 float64 each; either may be NULL). */
 int tpm_get_force_parts(tpm_handle* h, double* acc_lr, double* acc_sr);
 int tpm_get_stats(const tpm_handle* h, tpm_stats* out);
+/* Interactions of the last short-range walk per particle (original order,
+ * n x 2: leaf pairs, monopoles) — the per-target work counters the reference
+ * keeps for its walks (crates/gadget-ng-tree/src/octree.rs:77-151). */
+int tpm_get_interaction_counts(tpm_handle* h, int64_t* counts);
 
 /* ---- the stream the handle launches on ----------------------------------- */
 int tpm_set_stream(tpm_handle* h, void* cuda_stream);

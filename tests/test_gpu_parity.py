@@ -122,6 +122,9 @@ def _sr_parity(b, nm, periodic=True, r_cut_factor=4.5, eps_frac=30.0):
 def test_short_range_parity_and_interaction_set(kind):
     b = small_box(24, 100.0, 1.0, 12) if kind == "lattice" else clustered_small(24, 100.0, 13)
     s, sr, ref, cnt, st = _sr_parity(b, 32)
+    per = s.interaction_counts(b.n)
+    bad = np.nonzero(np.any(per != cnt, axis=1))[0]
+    assert len(bad) == 0, (len(bad), bad[:8], per[bad[:8]], cnt[bad[:8]])
     assert st["leaf_pairs"] == int(cnt[:, 0].sum())
     assert st["monopoles"] == int(cnt[:, 1].sum())
     assert global_rel(sr, ref) < RMS_TOL
@@ -202,7 +205,9 @@ def test_index_subset_and_order():
     full = s.accelerations_for_indices(pos, b.mass, 1e-3, 1.0, np.arange(b.n))
     idx = np.array([5, 0, 4095, 17, 5])
     sub = s.accelerations_for_indices(pos, b.mass, 1e-3, 1.0, idx)
-    np.testing.assert_array_equal(sub, full[idx])
+    # float atomics in the mass deposit make repeated calls agree to rounding only
+    np.testing.assert_allclose(sub, full[idx], rtol=1e-5, atol=0)
+    assert np.array_equal(sub[0], sub[4])
 
 
 def test_known_answer_pair_across_boundary():
