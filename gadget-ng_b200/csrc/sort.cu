@@ -209,4 +209,40 @@ void radix_sort_u64(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, voi
   }
 }
 
+void radix_sort_u64_all_passes(uint64_t* keys, uint32_t* vals, int64_t n, void* scratch, size_t scratch_bytes,
+                               cudaStream_t s) {
+  if (n <= 1) return;
+  if (scratch_bytes < radix_sort_scratch_bytes(n)) throw Error(1, "radix sort scratch too small");
+  int64_t ntiles = (n + SORT_TILE - 1) / SORT_TILE;
+  char* p = (char*)scratch;
+  auto carve = [&](size_t bytes) {
+    char* r = p;
+    p += (bytes + 255) & ~(size_t)255;
+    return (void*)r;
+  };
+  uint64_t* keys_alt = (uint64_t*)carve((size_t)n * sizeof(uint64_t));
+  uint32_t* vals_alt = (uint32_t*)carve((size_t)n * sizeof(uint32_t));
+  uint32_t* tile_counts = (uint32_t*)carve((size_t)ntiles * 256 * sizeof(uint32_t));
+  uint32_t* offsets = (uint32_t*)carve((size_t)ntiles * 256 * sizeof(uint32_t));
+  uint32_t* hist = (uint32_t*)carve(8 * 256 * sizeof(uint32_t));
+  TPM_CUDA(cudaMemsetAsync(hist, 0, 8 * 256 * sizeof(uint32_t), s));
+  k_hist8<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(keys, n, hist);
+  TPM_LAUNCH_CHECK();
+  uint64_t* kin = keys;
+  uint32_t* vin = vals;
+  uint64_t* kout = keys_alt;
+  uint32_t* vout = vals_alt;
+  for (int pass = 0; pass < 8; ++pass) {  // eight passes: the result ends in keys / vals
+    const int shift = 8 * pass;
+    k_upsweep<<<(unsigned)ntiles, SORT_BLOCK, 0, s>>>(kin, n, shift, ntiles, tile_counts);
+    TPM_LAUNCH_CHECK();
+    k_scan_tiles<<<256, 1024, 0, s>>>(tile_counts, hist + pass * 256, ntiles, offsets);
+    TPM_LAUNCH_CHECK();
+    k_downsweep<<<(unsigned)ntiles, SORT_BLOCK, 0, s>>>(kin, vin, kout, vout, n, shift, ntiles, offsets);
+    TPM_LAUNCH_CHECK();
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+}
+
 }  // namespace tpm

@@ -22,6 +22,7 @@ ERRORS = {
     7: "TPM_ERR_NOT_READY",
     8: "TPM_ERR_NO_DEVICE",
     9: "TPM_ERR_NONFINITE",
+    10: "TPM_ERR_TOO_LARGE",
 }
 
 FLAG_APERIODIC_WALK = 1 << 0
@@ -103,7 +104,9 @@ SIGNATURES = {
     "tpm_export_tree": ([_P, _I64, _P, _P, _P, _P, _P, _P, _P], _I64),
     "tpm_get_mesh": ([_P, _P, _P, _P, _P], _I),
     "tpm_fp32_peak": ([_I, C.POINTER(_D)], _I),
+    "tpm_hilbert_sort_noalloc": ([_P, _P, _P, _I64, _D, _P, _P, _P], _I),
 }
+NOALLOC_MAX_PARTICLES = 1 << 18
 
 _lib = None
 

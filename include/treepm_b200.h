@@ -46,7 +46,8 @@ enum {
   TPM_ERR_DEFERRED = 6,        /* exact-fallback work list overflowed */
   TPM_ERR_NOT_READY = 7,       /* call needs particles / forces that are not set */
   TPM_ERR_NO_DEVICE = 8,       /* no CUDA device, or the device is not sm_100 */
-  TPM_ERR_NONFINITE = 9        /* non-finite input position or mass */
+  TPM_ERR_NONFINITE = 9,       /* non-finite input position or mass */
+  TPM_ERR_TOO_LARGE = 10       /* more particles than tpm_hilbert_sort_noalloc's fixed scratch holds */
 };
 
 /* ---- configuration flags -------------------------------------------------- */
@@ -182,6 +183,28 @@ int64_t tpm_export_tree(tpm_handle* h, int64_t cap, int32_t* depth, double* mass
 /* The PM mesh of the last force evaluation: density (mass per cell, nm^3)
  * and the three force grids (nm^3 each), float32; any may be NULL. */
 int tpm_get_mesh(tpm_handle* h, float* density, float* fx, float* fy, float* fz);
+
+/* ---- allocation-free variant ---------------------------------------------------
+ * No counterpart in the reference.  The Hilbert keys and (key, index) order of
+ * tpm_hilbert_keys, for callers that cannot call cudaMalloc — a simulation that
+ * owns all device memory through its own pool and forbids other allocations,
+ * or code running where an allocation would stall or break it.  It allocates
+ * nothing: the radix sort's intermediate buffers live in a fixed file-scope
+ * device array of about 3.3 MB, held on every GPU that loads this library
+ * until the process exits.
+ *  - qx, qy, qz: device arrays of n 32-bit fixed-point positions
+ *    (x = q * box_size / 2^32); keys_out (n uint64) and order_out (n uint32):
+ *    device arrays owned by the caller.  On return keys_out holds the keys
+ *    sorted ascending and order_out the input index of each, ties by
+ *    ascending index.  Work is queued on `stream` (NULL = legacy default);
+ *    the caller synchronises before reading the outputs.
+ *  - n above TPM_NOALLOC_MAX_PARTICLES returns TPM_ERR_TOO_LARGE, nothing runs.
+ *  - The first call on a device looks up the array's device address with that
+ *    device current; make that first call before any stream capture.
+ *  - Every call shares the one array: calls that overlap on the GPU race. */
+#define TPM_NOALLOC_MAX_PARTICLES (1 << 18)
+int tpm_hilbert_sort_noalloc(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, int64_t n,
+                             double box_size, uint64_t* keys_out, uint32_t* order_out, void* stream);
 
 /* ---- measurement -----------------------------------------------------------
  * No counterpart in the reference: FFMA throughput of `device` in TFLOP/s, the
