@@ -35,6 +35,7 @@ WORKLOADS = {
     # name: (generator, mesh, a_start, a_end over 10 steps)
     "clustered256": ("clustered_box_256", 256, 0.1, 0.12),
     "treepm128": ("treepm_box_128", 128, 0.1, 0.12),
+    "treepm64": ("treepm_box_64", 64, 0.1, 0.12),
     "clustered512": ("clustered_box_512", 512, 0.1, 0.12),
     "pm64": ("pm_box_64", 64, 0.02, 0.0202),
 }

@@ -400,6 +400,57 @@ __global__ void k_walk_nodes(int64_t n_int, double inv_scale, const double* __re
 }
 
 // ---------------------------------------------------------------------------
+// walk records: children of each internal node contiguous
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ WalkNode make_record(uint32_t c, const uint32_t* __restrict__ qx,
+                                                const uint32_t* __restrict__ qy, const uint32_t* __restrict__ qz,
+                                                const float* __restrict__ massf, const uint8_t* __restrict__ leaf_depth,
+                                                const uint4* __restrict__ walk, const uint8_t* __restrict__ o_depth,
+                                                const uint32_t* __restrict__ nchild,
+                                                const uint32_t* __restrict__ child_first, double h0, double thr) {
+  WalkNode r;
+  r.pad = 0;
+  if (c & LEAF_BIT) {
+    const uint32_t j = c & ~LEAF_BIT;
+    r.cq[0] = qx[j];
+    r.cq[1] = qy[j];
+    r.cq[2] = qz[j];
+    r.mass = massf[j];
+    r.first = 0;
+    r.info = ((uint32_t)leaf_depth[j] << 4) | WN_LEAF;
+    r.ref = j;
+  } else {
+    const uint4 w = walk[c];
+    r.cq[0] = w.x;
+    r.cq[1] = w.y;
+    r.cq[2] = w.z;
+    r.mass = __uint_as_float(w.w);
+    r.first = 1u + child_first[c];
+    const int dep = o_depth[c];
+    r.info = nchild[c] | ((uint32_t)dep << 4) | (ldexp(h0, -dep) < thr ? WN_TERMINAL : 0u);
+    r.ref = c;
+  }
+  return r;
+}
+
+__global__ void k_walk_records(int64_t n_int, const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                               const uint32_t* __restrict__ qz, const float* __restrict__ massf,
+                               const uint8_t* __restrict__ leaf_depth, const uint4* __restrict__ walk,
+                               const uint8_t* __restrict__ o_depth, const uint32_t* __restrict__ nchild,
+                               const uint32_t* __restrict__ child_first, const uint32_t* __restrict__ child_ids,
+                               const TreeParams* __restrict__ prm, double thr, WalkNode* __restrict__ recs) {
+  int64_t P = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (P >= n_int) return;
+  const double h0 = prm->half;
+  if (P == 0)
+    recs[0] = make_record(0u, qx, qy, qz, massf, leaf_depth, walk, o_depth, nchild, child_first, h0, thr);
+  const uint32_t f = child_first[P], nc = nchild[P];
+  for (uint32_t r = 0; r < nc; ++r)
+    recs[1 + (int64_t)f + r] =
+        make_record(child_ids[f + r], qx, qy, qz, massf, leaf_depth, walk, o_depth, nchild, child_first, h0, thr);
+}
+
+// ---------------------------------------------------------------------------
 // walk groups: maximal subtrees of <= group_max particles, consecutive small
 // siblings packed together
 // ---------------------------------------------------------------------------
@@ -607,6 +658,14 @@ void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, 
                                                           t.o_com, t.o_quad);
   TPM_LAUNCH_CHECK();
   k_walk_nodes<<<grid_for(n_int, 256, 1ll << 30), 256, 0, s>>>(n_int, TWO32 / box, t.o_mass, t.o_com, t.o_walk);
+  TPM_LAUNCH_CHECK();
+}
+
+void launch_walk_records(const Particles& p, int64_t n, int64_t n_int, double thr, TreeBuffers& t, cudaStream_t s) {
+  (void)n;
+  k_walk_records<<<grid_for(n_int, 128, 1ll << 30), 128, 0, s>>>(n_int, p.qx, p.qy, p.qz, p.massf, t.leaf_depth,
+                                                                 t.o_walk, t.o_depth, t.o_nchild, t.o_child_first,
+                                                                 t.child_ids, t.params, thr, t.recs);
   TPM_LAUNCH_CHECK();
 }
 

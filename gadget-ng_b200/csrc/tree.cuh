@@ -10,6 +10,23 @@ constexpr uint32_t LEAF_BIT = 0x80000000u;
 constexpr uint32_t EMPTY_SLOT = 0xFFFFFFFFu;
 constexpr int KEY_LEVELS = 42;  // 21 octant digits in each of two 64-bit words
 
+// One node of the walk, 32 bytes.  Records are laid out so that the children
+// of every internal node are contiguous (root at 0, the children of internal
+// node P at 1 + child_first[P] ...), so the walk reads a node's children with
+// one coalesced load.
+struct __align__(16) WalkNode {
+  uint32_t cq[3];    // fixed-point centre of mass (leaf: the particle)
+  float mass;
+  uint32_t first;    // record index of the first child (internal nodes)
+  uint32_t info;     // nchild [0,4) | depth [4,10) | leaf bit 10 | terminal bit 11
+  uint32_t ref;      // leaf: sorted particle index; internal: octree node id
+  uint32_t pad;
+};
+constexpr uint32_t WN_LEAF = 1u << 10;
+constexpr uint32_t WN_TERMINAL = 1u << 11;
+__host__ __device__ inline uint32_t wn_nchild(uint32_t info) { return info & 15u; }
+__host__ __device__ inline int wn_depth(uint32_t info) { return (int)((info >> 4) & 63u); }
+
 // Geometry of one force evaluation, computed on the device.
 struct TreeParams {
   double center[3];  // bounding_cube centre (octree.rs:1306-1332)
@@ -63,6 +80,7 @@ struct TreeBuffers {
   double* o_com;   // 3 per node
   double* o_quad;  // 6 per node
   uint4* o_walk;   // fixed-point COM (x, y, z) and float mass bits
+  WalkNode* recs;  // n_int + n walk records
   // leaves
   int32_t* leaf_oparent;
   uint8_t* leaf_depth;
@@ -87,6 +105,7 @@ void launch_karras(int64_t n, TreeBuffers& t, cudaStream_t s);
 void launch_octree_nodes(int64_t n, TreeBuffers& t, cudaStream_t s);
 void launch_octree_links(int64_t n, int64_t n_int, TreeBuffers& t, void* scan_scratch, cudaStream_t s);
 void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, TreeBuffers& t, cudaStream_t s);
+void launch_walk_records(const Particles& p, int64_t n, int64_t n_int, double thr, TreeBuffers& t, cudaStream_t s);
 void launch_groups(int64_t n, int64_t n_int, int group_max, TreeBuffers& t, void* scan_scratch, cudaStream_t s);
 void launch_hilbert_keys(const Particles& p, int64_t n, double box, const TreeParams* prm, uint64_t* keys,
                          uint32_t* vals, cudaStream_t s);

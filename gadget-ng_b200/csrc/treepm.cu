@@ -335,6 +335,7 @@ void ensure_tree_capacity(tpm_handle* h, int64_t n_int) {
   T.o_com = h->alloc<double>(3 * c, 2);
   T.o_quad = h->alloc<double>(6 * c, 2);
   T.o_walk = h->alloc<uint4>(c, 2);
+  T.recs = h->alloc<WalkNode>(c + h->cap + 8, 2);
   T.grp_count_per_node = h->alloc<uint32_t>(c, 2);
   T.grp_base = h->alloc<uint32_t>(c, 2);
   T.grp_first = h->alloc<uint32_t>(h->cap + 1, 2);
@@ -387,6 +388,7 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       launch_octree_nodes(n, T, s);
       launch_octree_links(n, h->n_int, T, h->scan_scratch, s);
       launch_aggregate(h->P[h->cur], n, h->n_int, box, T, s);
+      launch_walk_records(h->P[h->cur], n, h->n_int, h->thr, T, s);
       launch_groups(n, h->n_int, GROUP_MAX, T, h->scan_scratch, s);
       TPM_CUDA(cudaMemcpyAsync(sc, T.scalars, sizeof(sc), cudaMemcpyDeviceToHost, s));
       TPM_CUDA(cudaStreamSynchronize(s));
@@ -410,6 +412,7 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       a.n_int = h->n_int;
       const Particles& P = h->P[h->cur];
       a.qx = P.qx; a.qy = P.qy; a.qz = P.qz; a.massf = P.massf;
+      a.recs = T.recs;
       a.walk = T.o_walk; a.depth = T.o_depth; a.nchild = T.o_nchild; a.child_first = T.o_child_first;
       a.child_ids = T.child_ids; a.o_com = T.o_com; a.leaf_depth = T.leaf_depth;
       a.gfirst = T.grp_first; a.gsize = T.grp_size; a.ngroups = h->n_groups; a.work = h->work;

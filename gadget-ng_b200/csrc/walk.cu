@@ -25,6 +25,8 @@
 // reference's.  Pair arithmetic is FP32: exact fixed-point differences split
 // into two floats, rsqrt / rcp / ex2 hardware approximations, the A&S 7.1.26
 // erfc, and Kahan-compensated per-target accumulators.
+#include <cstdlib>
+
 #include "common.cuh"
 #include "tree.cuh"
 #include "walk.cuh"
@@ -34,7 +36,8 @@ namespace {
 
 constexpr int WALK_WARPS = 4;
 constexpr int WALK_THREADS = WALK_WARPS * 32;
-constexpr int CHUNK = 96;
+constexpr int CHUNK_L = 96;  // leaf-list capacity
+constexpr int CHUNK_M = 64;  // monopole-list capacity
 constexpr uint32_t AMB_FLAG = 0x40000000u;
 constexpr uint32_t NODE_MASK = 0x3FFFFFFFu;
 constexpr int32_t WIDE_GROUP = 1 << 28;  // quanta: 1/16 of the box
@@ -173,49 +176,113 @@ struct Acc {
   }
 };
 
-// Evaluate the interaction list against this lane's target.
-__device__ __forceinline__ void flush(const WalkArgs& a, const Entry* L, int nl, int lane, bool has, uint32_t p,
-                                      float thx, float thy, float thz, float tlx, float tly, float tlz, Acc& acc,
-                                      uint32_t& nleaf, uint32_t& nmono, uint32_t& nexact) {
-  float fx = 0.f, fy = 0.f, fz = 0.f;
-  const uint32_t self = p | LEAF_BIT;
+// Evaluate one interaction list against this lane's target.  MONO selects the
+// monopole list (AABB-gap test) or the leaf list (bare-distance test; the
+// aperiodic walk's leaves carry their half side and take the AABB test too).
+// Borderline pairs are left out here and flagged; resolve_list settles them.
+template <bool MONO>
+__device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, int nl, int lane, float thx, float thy,
+                                           float thz, float tlx, float tly, float tlz, float& fx, float& fy,
+                                           float& fz, uint32_t& nok, bool& amb_any) {
 #pragma unroll 2
   for (int e = 0; e < nl; ++e) {
     const float4 A = *reinterpret_cast<const float4*>(&L[e].hx);
     const float4 B = *reinterpret_cast<const float4*>(&L[e].lx);
-    const uint4 C = *reinterpret_cast<const uint4*>(&L[e].mask);
+    const uint32_t mask = L[e].mask;
     const float dx = (A.x - thx) + (B.x - tlx);
     const float dy = (A.y - thy) + (B.y - tly);
     const float dz = (A.z - thz) + (B.z - tlz);
     const float r2b = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const float ex = fmaxf(fabsf(dx) - B.w, 0.f), ey = fmaxf(fabsf(dy) - B.w, 0.f), ez = fmaxf(fabsf(dz) - B.w, 0.f);
-    const float s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-    const bool in = (C.x >> lane) & 1u;
-    bool ok = in && s <= a.rc2_lo;
-    bool amb = in && s > a.rc2_lo && s <= a.rc2_hi;
-    if (C.z == KIND_MONO) amb = amb || (in && r2b < a.tiny_u);
-    if (amb) {
-      int d = exact_terminal(a, p, C.y);
-      ++nexact;
-      if (d == 2) defer(a, p, C.y);
-      ok = d == 1;
+    float s = r2b;
+    if (MONO || !a.periodic) {
+      const float ex = fmaxf(fabsf(dx) - B.w, 0.f), ey = fmaxf(fabsf(dy) - B.w, 0.f);
+      const float ez = fmaxf(fabsf(dz) - B.w, 0.f);
+      s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     }
+    const bool in = (mask >> lane) & 1u;
+    const bool ok = in && s <= a.rc2_lo;
+    bool amb = in && s > a.rc2_lo && s <= a.rc2_hi;
+    if (MONO) amb = amb || (in && r2b < a.tiny_u);
+    amb_any = amb_any || amb;
     float f = pair_factor(a, r2b, A.w);
     f = ok ? f : 0.f;
     fx = fmaf(dx, f, fx);
     fy = fmaf(dy, f, fy);
     fz = fmaf(dz, f, fz);
-    if (ok && C.y != self) {
-      if (C.z == KIND_LEAF) ++nleaf; else ++nmono;
-    }
+    nok += (ok && r2b > 0.f) ? 1u : 0u;  // r2b == 0 only for the target's own leaf
   }
-  acc.add(fx, fy, fz);
-  (void)has;
 }
 
+// Float64 decisions for this lane's borderline pairs of one list (rare).
+template <bool MONO>
+__device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float thx,
+                                          float thy, float thz, float tlx, float tly, float tlz, float* f3,
+                                          uint32_t* nok, uint32_t* nexact) {
+  for (int e = 0; e < nl; ++e) {
+    const float4 A = *reinterpret_cast<const float4*>(&L[e].hx);
+    const float4 B = *reinterpret_cast<const float4*>(&L[e].lx);
+    const uint32_t mask = L[e].mask, node = L[e].node;
+    const float dx = (A.x - thx) + (B.x - tlx);
+    const float dy = (A.y - thy) + (B.y - tly);
+    const float dz = (A.z - thz) + (B.z - tlz);
+    const float r2b = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float s = r2b;
+    if (MONO || !a.periodic) {
+      const float ex = fmaxf(fabsf(dx) - B.w, 0.f), ey = fmaxf(fabsf(dy) - B.w, 0.f);
+      const float ez = fmaxf(fabsf(dz) - B.w, 0.f);
+      s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+    }
+    const bool in = (mask >> lane) & 1u;
+    bool amb = in && s > a.rc2_lo && s <= a.rc2_hi;
+    if (MONO) amb = amb || (in && r2b < a.tiny_u);
+    if (!amb) continue;
+    ++*nexact;
+    const int d = exact_terminal(a, p, node);
+    if (d == 2) defer(a, p, node);
+    if (d != 1) continue;
+    const float f = pair_factor(a, r2b, A.w);
+    f3[0] = fmaf(dx, f, f3[0]);
+    f3[1] = fmaf(dy, f, f3[1]);
+    f3[2] = fmaf(dz, f, f3[2]);
+    if (r2b > 0.f) ++*nok;
+  }
+}
+
+// Evaluate both interaction lists against this lane's target.
+__device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nll, const Entry* Lm, int nlm, int lane,
+                                      uint32_t p, float thx, float thy, float thz, float tlx, float tly, float tlz,
+                                      Acc& acc, uint32_t& nleaf, uint32_t& nmono, uint32_t& nexact, uint32_t& neval) {
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  bool amb_any = false;
+  neval += (uint32_t)(nll + nlm);
+  flush_list<false>(a, Ll, nll, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nleaf, amb_any);
+  flush_list<true>(a, Lm, nlm, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nmono, amb_any);
+  if (amb_any) {
+    float f3[3] = {fx, fy, fz};
+    resolve_list<false>(a, Ll, nll, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nleaf, &nexact);
+    resolve_list<true>(a, Lm, nlm, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nmono, &nexact);
+    fx = f3[0];
+    fy = f3[1];
+    fz = f3[2];
+  }
+  __syncwarp();
+  acc.add(fx, fy, fz);
+}
+
+// Stack entry of an open node: its children's record range, mask of the
+// targets that still see it, and the octree id for the per-target test.
+struct __align__(16) StackEntry {
+  uint32_t first;  // record index of the first child
+  uint32_t info;   // the node's record info | AMB_FLAG when undecided for the group
+  uint32_t mask;
+  uint32_t ref;    // octree node id
+};
+constexpr int STACK_ENTRIES = 1024;  // global, per warp
+constexpr uint32_t INFO_AMB = 0x80000000u;
+
 // Walk the tree for targets [first, first + count) (count <= 32) with one warp.
-__device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, Entry* L, uint8_t* owner,
-                             uint32_t* stk_node, uint32_t* stk_mask) {
+__device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, Entry* Ll, Entry* Lm, uint8_t* owner,
+                             StackEntry* stk) {
   const int lane = threadIdx.x & 31;
   const bool has = (uint32_t)lane < count;
   const uint32_t p = first + (has ? (uint32_t)lane : 0u);
@@ -237,11 +304,11 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
   const uint32_t mask0 = count >= 32 ? 0xFFFFFFFFu : ((1u << count) - 1u);
   Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   uint32_t nleaf = 0, nmono = 0, nexact = 0, neval = 0;
-  int nl = 0, sp = 0;
+  int nll = 0, nlm = 0, sp = 0;
 
-  // the first item is the root (node 0, or the single leaf when n == 1)
+  // the first item is the root record
   bool have = lane == 0;
-  uint32_t item = a.n_int > 0 ? 0u : LEAF_BIT;
+  uint32_t item = 0;
   uint32_t imask = mask0;
   // each iteration pops at least one node, so a walk over a well-formed tree
   // ends within (internal nodes + 1) iterations; the cap turns a malformed
@@ -255,28 +322,18 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       break;
     }
     // ---- classify this lane's item against the group box
-    bool emit = false, push = false, ambig = false;
+    bool emit = false, push = false, ambig = false, is_leaf = false;
     Entry ent;
+    StackEntry se;
     if (have && imask != 0u) {
-      uint32_t cq[3];
-      float m, h;
-      uint32_t kind;
-      bool open = false;
-      if (item & LEAF_BIT) {
-        const uint32_t j = item & ~LEAF_BIT;
-        cq[0] = a.qx[j]; cq[1] = a.qy[j]; cq[2] = a.qz[j];
-        m = a.massf[j];
-        h = a.periodic ? 0.f : ldexpf(a.h0_u, -(int)a.leaf_depth[j]);
-        kind = KIND_LEAF;
-      } else {
-        const uint4 w = a.walk[item];
-        cq[0] = w.x; cq[1] = w.y; cq[2] = w.z;
-        m = __uint_as_float(w.w);
-        const int dep = a.depth[item];
-        h = ldexpf(a.h0_u, -dep);
-        open = !(ldexp(a.h0, -dep) < a.thr);
-        kind = KIND_MONO;
-      }
+      const uint4 r0 = __ldg(reinterpret_cast<const uint4*>(&a.recs[item]));
+      const uint4 r1 = __ldg(reinterpret_cast<const uint4*>(&a.recs[item]) + 1);
+      const uint32_t info = r1.y;
+      const bool leaf = (info & WN_LEAF) != 0;
+      const int dep = wn_depth(info);
+      const float h = (leaf && a.periodic) ? 0.f : ldexpf(a.h0_u, -dep);
+      const bool open = !leaf && !(info & WN_TERMINAL);
+      const uint32_t cq[3] = {r0.x, r0.y, r0.z};
       // Per axis, the targets see the node at the minimum image of S - t for t
       // in [bmin, bmax]: bound min / max of |wrap(S - t)| over that interval
       // (images at 0 and +-L), then the AABB gap.
@@ -304,73 +361,80 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
         if (open) {
           push = true;
           ambig = !(emax2 < a.grc2_lo);
+          se.first = r1.x;
+          se.info = info | (ambig ? INFO_AMB : 0u);
+          se.mask = imask;
+          se.ref = r1.z;
         } else {
           emit = true;
           split_rel(S[0], a.u_inv, &ent.hx, &ent.lx);
           split_rel(S[1], a.u_inv, &ent.hy, &ent.ly);
           split_rel(S[2], a.u_inv, &ent.hz, &ent.lz);
-          ent.m = m;
+          ent.m = __uint_as_float(r0.w);
           ent.h = h;
           ent.mask = imask;
-          ent.node = item;
-          ent.kind = kind;
+          ent.node = leaf ? (r1.z | LEAF_BIT) : r1.z;
+          ent.kind = leaf ? KIND_LEAF : KIND_MONO;
+          is_leaf = leaf;
           ent.pad = 0;
         }
       }
     }
-    // ---- append terminal entries to the list
-    const uint32_t em = __ballot_sync(0xffffffffu, emit);
+    // ---- append terminal entries to the leaf and monopole lists
+    const uint32_t eml = __ballot_sync(0xffffffffu, emit && is_leaf);
+    const uint32_t emm = __ballot_sync(0xffffffffu, emit && !is_leaf);
     if (emit) {
-      const int slot = nl + __popc(em & ((1u << lane) - 1u));
-      float4* dst = reinterpret_cast<float4*>(&L[slot]);
+      const unsigned lt = (1u << lane) - 1u;
+      Entry* dstE = is_leaf ? &Ll[nll + __popc(eml & lt)] : &Lm[nlm + __popc(emm & lt)];
+      float4* dst = reinterpret_cast<float4*>(dstE);
       dst[0] = make_float4(ent.hx, ent.hy, ent.hz, ent.m);
       dst[1] = make_float4(ent.lx, ent.ly, ent.lz, ent.h);
       *reinterpret_cast<uint4*>(&dst[2]) = make_uint4(ent.mask, ent.node, ent.kind, 0u);
     }
-    nl += __popc(em);
+    nll += __popc(eml);
+    nlm += __popc(emm);
     // ---- push open nodes
     const uint32_t pm = __ballot_sync(0xffffffffu, push);
-    if (sp + __popc(pm) > a.stack_cap) {
+    if (sp + __popc(pm) > STACK_ENTRIES) {
       if (lane == 0) atomicOr(a.err, DEV_ERR_STACK);
       break;
     }
     if (push) {
       const int slot = sp + __popc(pm & ((1u << lane) - 1u));
-      stk_node[slot] = item | (ambig ? AMB_FLAG : 0u);
-      stk_mask[slot] = imask;
+      *reinterpret_cast<uint4*>(&stk[slot]) = make_uint4(se.first, se.info, se.mask, se.ref);
     }
     sp += __popc(pm);
     __syncwarp();
-    if (nl > CHUNK - 32) {
-      neval += (uint32_t)nl;
-      flush(a, L, nl, lane, has, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact);
+    if (nll > CHUNK_L - 32 || nlm > CHUNK_M - 32) {
+      flush(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
       __syncwarp();
-      nl = 0;
+      nll = 0;
+      nlm = 0;
     }
     if (sp == 0) break;
     // ---- pop a batch whose children fill at most one warp
     const int avail = sp < 32 ? sp : 32;
-    uint32_t enode = 0, emask = 0, nc = 0;
+    uint4 e = make_uint4(0u, 0u, 0u, 0u);
+    uint32_t nc = 0;
     if (lane < avail) {
-      enode = stk_node[sp - 1 - lane];
-      emask = stk_mask[sp - 1 - lane];
-      nc = a.nchild[enode & NODE_MASK];
+      e = *reinterpret_cast<const uint4*>(&stk[sp - 1 - lane]);
+      nc = wn_nchild(e.y);
     }
     const uint32_t incl = warp_incl_scan(nc, lane);
     const uint32_t take = __ballot_sync(0xffffffffu, lane < avail && incl <= 32u);
     const int k = __popc(take);
     sp -= k;
     // per-target refinement of undecided open nodes
-    uint32_t amb = __ballot_sync(0xffffffffu, lane < k && (enode & AMB_FLAG));
+    uint32_t amb = __ballot_sync(0xffffffffu, lane < k && (e.y & INFO_AMB));
     while (amb) {
-      const int e = __ffs(amb) - 1;
+      const int src = __ffs(amb) - 1;
       amb &= amb - 1;
-      const uint32_t node = __shfl_sync(0xffffffffu, enode, e) & NODE_MASK;
-      const uint32_t me = __shfl_sync(0xffffffffu, emask, e);
+      const uint32_t node = __shfl_sync(0xffffffffu, e.w, src);
+      const uint32_t me = __shfl_sync(0xffffffffu, e.z, src);
+      const int dep = wn_depth(__shfl_sync(0xffffffffu, e.y, src));
       bool pass = false;
       if (has && ((me >> lane) & 1u)) {
-        const uint4 w = a.walk[node];
-        const int dep = a.depth[node];
+        const uint4 w = __ldg(&a.walk[node]);
         const float h = ldexpf(a.h0_u, -dep);
         float s = 0.f;
         const uint32_t wq[3] = {w.x, w.y, w.z};
@@ -387,7 +451,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
         }
       }
       const uint32_t nm = __ballot_sync(0xffffffffu, pass);
-      if (lane == e) emask = nm;
+      if (lane == src) e.z = nm;
     }
     // distribute the children of the popped entries over the lanes
     const uint32_t excl = incl - nc;
@@ -397,18 +461,17 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     const uint32_t total = __shfl_sync(0xffffffffu, incl, k - 1);
     have = (uint32_t)lane < total;
     const int o = have ? owner[lane] : 0;
-    const uint32_t onode = __shfl_sync(0xffffffffu, enode, o) & NODE_MASK;
-    const uint32_t omask = __shfl_sync(0xffffffffu, emask, o);
+    const uint32_t ofirst = __shfl_sync(0xffffffffu, e.x, o);
+    const uint32_t omask = __shfl_sync(0xffffffffu, e.z, o);
     const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, o);
     __syncwarp();
     if (have) {
-      item = a.child_ids[a.child_first[onode] + ((uint32_t)lane - oexcl)];
+      item = ofirst + ((uint32_t)lane - oexcl);
       imask = omask;
     }
   }
-  if (nl > 0) {
-    neval += (uint32_t)nl;
-    flush(a, L, nl, lane, has, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact);
+  if (nll + nlm > 0) {
+    flush(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
   }
   __syncwarp();
   if (has) {
@@ -433,20 +496,25 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
   }
 }
 
-__global__ void __launch_bounds__(WALK_THREADS, 4) k_walk(WalkArgs a) {
-  __shared__ Entry s_list[WALK_WARPS][CHUNK];
-  __shared__ uint8_t s_owner[WALK_WARPS][32];
+constexpr size_t WALK_SMEM_PER_WARP = sizeof(Entry) * (CHUNK_L + CHUNK_M) + 32;
+
+template <int MIN_BLOCKS>
+__global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
+  extern __shared__ __align__(16) unsigned char s_walk[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char* mine = s_walk + wid * WALK_SMEM_PER_WARP;
+  Entry* list_l = reinterpret_cast<Entry*>(mine);
+  Entry* list_m = list_l + CHUNK_L;
+  uint8_t* owner = reinterpret_cast<uint8_t*>(list_m + CHUNK_M);
   const int64_t gw = (int64_t)blockIdx.x * WALK_WARPS + wid;
-  uint32_t* stk_node = a.stack + gw * 2 * (int64_t)a.stack_cap;
-  uint32_t* stk_mask = stk_node + a.stack_cap;
+  StackEntry* stk = reinterpret_cast<StackEntry*>(a.stack) + gw * STACK_ENTRIES;
   for (;;) {
     uint32_t g = 0;
     if (lane == 0) g = atomicAdd(a.work, 1u);
     g = __shfl_sync(0xffffffffu, g, 0);
     if ((int64_t)g >= a.ngroups) break;
     const uint32_t first = a.gfirst[g], count = a.gsize[g];
-    // a group wider than 1/8 of the box would break the shared-origin minimum
+    // a group wider than 1/16 of the box would break the shared-origin minimum
     // image: walk its targets one at a time instead
     const bool has = (uint32_t)lane < count;
     const uint32_t p = first + (has ? lane : 0);
@@ -462,10 +530,9 @@ __global__ void __launch_bounds__(WALK_THREADS, 4) k_walk(WalkArgs a) {
     }
     wide = wide || a.single_target;
     if (!wide) {
-      walk_targets(a, first, count, s_list[wid], s_owner[wid], stk_node, stk_mask);
+      walk_targets(a, first, count, list_l, list_m, owner, stk);
     } else {
-      for (uint32_t t = 0; t < count; ++t)
-        walk_targets(a, first + t, 1u, s_list[wid], s_owner[wid], stk_node, stk_mask);
+      for (uint32_t t = 0; t < count; ++t) walk_targets(a, first + t, 1u, list_l, list_m, owner, stk);
     }
   }
 }
@@ -548,16 +615,46 @@ __global__ void k_deferred(WalkArgs a, uint32_t n_items) {
 
 }  // namespace
 
-int walk_blocks_per_sm() {
+// Occupancy variant of the walk: register budget for 4, 5 or 6 resident
+// blocks of 4 warps per SM (TPM_WALK_BLOCKS overrides the default).
+static int walk_variant() {
+  static int v = [] {
+    const char* e = getenv("TPM_WALK_BLOCKS");
+    int b = e ? atoi(e) : 5;
+    return (b == 4 || b == 5 || b == 6) ? b : 5;
+  }();
+  return v;
+}
+
+template <int B>
+static int blocks_for() {
+  const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
+  TPM_CUDA(cudaFuncSetAttribute(k_walk<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int nb = 0;
-  TPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk, WALK_THREADS, 0));
+  TPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<B>, WALK_THREADS, smem));
   return nb < 1 ? 1 : nb;
 }
+
+int walk_blocks_per_sm() {
+  switch (walk_variant()) {
+    case 4: return blocks_for<4>();
+    case 6: return blocks_for<6>();
+    default: return blocks_for<5>();
+  }
+}
 int walk_threads() { return WALK_THREADS; }
-size_t walk_stack_words(int grid, int stack_cap) { return (size_t)grid * WALK_WARPS * 2 * (size_t)stack_cap; }
+size_t walk_stack_words(int grid, int stack_cap) {
+  (void)stack_cap;
+  return (size_t)grid * WALK_WARPS * STACK_ENTRIES * 4;  // one 16-byte entry = 4 words
+}
 
 void launch_walk(const WalkArgs& a, int grid, cudaStream_t s) {
-  k_walk<<<grid, WALK_THREADS, 0, s>>>(a);
+  const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
+  switch (walk_variant()) {
+    case 4: k_walk<4><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    case 6: k_walk<6><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    default: k_walk<5><<<grid, WALK_THREADS, smem, s>>>(a); break;
+  }
   TPM_LAUNCH_CHECK();
 }
 

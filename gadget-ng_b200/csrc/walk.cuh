@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "tree.cuh"
+
 namespace tpm {
 
 struct WalkArgs {
@@ -13,6 +15,7 @@ struct WalkArgs {
   const uint32_t* qz;
   const float* massf;
   // octree
+  const WalkNode* recs;  // walk records, children contiguous
   const uint4* walk;  // internal nodes: fixed-point COM + float mass bits
   const uint8_t* depth;
   const uint32_t* nchild;

@@ -152,6 +152,11 @@ def pm_box_64(seed: int = 1) -> Box:
     return lattice_box(64, 100.0, 0.2, seed, name="pm64_L100")
 
 
+def treepm_box_64(seed: int = 1) -> Box:
+    """64³ particles, L = 50 Mpc/h (the 128³ box's density), 1.0-cell rms displacement."""
+    return lattice_box(64, 50.0, 1.0, seed, name="treepm64_L50")
+
+
 def treepm_box_128(seed: int = 1) -> Box:
     """128³ particles, L = 100 Mpc/h, 1.0-cell rms displacement (TreePM case)."""
     return lattice_box(128, 100.0, 1.0, seed, name="treepm128_L100")
