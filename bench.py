@@ -242,6 +242,20 @@ def run_b200(args):
     ms_per_step = dev_ms / args.steps
     value = world * n * args.steps / (dev_ms * 1e-3)
 
+    # ---- force error of the last evaluation against FP64 Ewald ------------
+    ewald = None
+    if rank == 0 and not args.no_ewald:
+        from treepm import accuracy
+        p_now, _, a_now = solver.get_state(n, pos=True, vel=False, acc=True)
+        tg = accuracy.seeded_targets(n, args.ewald_targets)
+        g_last = factors[args.warmup + args.steps - 1][3]
+        t_e = time.perf_counter()
+        ref = accuracy.ewald_accelerations(p_now, box.mass, box.box_size, g_last, phys["eps2"],
+                                           phys["r_cut_factor"] * phys["r_split"], tg, device=local)
+        rms, p99 = accuracy.relative_errors(a_now[tg], ref)
+        ewald = {"rms": rms, "p99": p99, "targets": int(len(tg)), "seconds": time.perf_counter() - t_e,
+                 "reference": "FP64 Ewald, Plummer-softened nearest images within r_cut"}
+
     # ---- end to end through the host-buffer API (e2e) -------------------
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
     pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -305,6 +319,7 @@ def run_b200(args):
                 "path": "tpm_kdk_step_host: float64 positions, velocities and masses from pinned host memory, "
                         "two force evaluations (no cached acceleration across calls), state back to host"},
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+        "force_error_vs_ewald": ewald,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -336,6 +351,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak measurement (profiling runs)")
+    ap.add_argument("--no-ewald", action="store_true", help="skip the FP64 Ewald error report")
+    ap.add_argument("--ewald-targets", type=int, default=4096)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

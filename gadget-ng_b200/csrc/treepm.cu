@@ -389,7 +389,7 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       launch_octree_links(n, h->n_int, T, h->scan_scratch, s);
       launch_aggregate(h->P[h->cur], n, h->n_int, box, T, s);
       launch_walk_records(h->P[h->cur], n, h->n_int, h->thr, T, s);
-      launch_groups(n, h->n_int, GROUP_MAX, T, h->scan_scratch, s);
+      launch_groups(n, h->n_int, walk_targets_per_warp(), T, h->scan_scratch, s);
       TPM_CUDA(cudaMemcpyAsync(sc, T.scalars, sizeof(sc), cudaMemcpyDeviceToHost, s));
       TPM_CUDA(cudaStreamSynchronize(s));
       h->n_groups = sc[1];
@@ -424,6 +424,13 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       const double rc2_u = h->rc2 / (u * u);
       a.rc2_lo = (float)(rc2_u * (1.0 - 1e-4));
       a.rc2_hi = (float)(rc2_u * (1.0 + 1e-4));
+      {
+        uint32_t lo_bits, hi_bits;
+        std::memcpy(&lo_bits, &a.rc2_lo, 4);
+        std::memcpy(&hi_bits, &a.rc2_hi, 4);
+        a.rc2_lo_bits = lo_bits;
+        a.band_bits = hi_bits - lo_bits;
+      }
       a.grc2_lo = (float)(rc2_u * (1.0 - 4e-4));
       a.grc2_hi = (float)(rc2_u * (1.0 + 4e-4));
       a.eps2_u = (float)(eps2 / (u * u));

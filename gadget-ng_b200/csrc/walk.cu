@@ -180,12 +180,16 @@ struct Acc {
 // monopole list (AABB-gap test) or the leaf list (bare-distance test; the
 // aperiodic walk's leaves carry their half side and take the AABB test too).
 // Borderline pairs are left out here and flagged; resolve_list settles them.
-template <bool MONO>
+template <bool MONO, int TPW>
 __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, int nl, int lane, float thx, float thy,
                                            float thz, float tlx, float tly, float tlz, float& fx, float& fy,
                                            float& fz, uint32_t& nok, bool& amb_any) {
+  // TPW targets per warp; with 16, lanes t and t + 16 share target t and
+  // take alternate entries
+  constexpr int STRIDE = 32 / TPW;
+  const int t = lane & (TPW - 1);
 #pragma unroll 2
-  for (int e = 0; e < nl; ++e) {
+  for (int e = lane / TPW; e < nl; e += STRIDE) {
     const float4 A = *reinterpret_cast<const float4*>(&L[e].hx);
     const float4 B = *reinterpret_cast<const float4*>(&L[e].lx);
     const uint32_t mask = L[e].mask;
@@ -199,9 +203,10 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
       const float ez = fmaxf(fabsf(dz) - B.w, 0.f);
       s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     }
-    const bool in = (mask >> lane) & 1u;
+    const bool in = (mask >> t) & 1u;
     const bool ok = in && s <= a.rc2_lo;
-    bool amb = in && s > a.rc2_lo && s <= a.rc2_hi;
+    // s in (rc2_lo, rc2_hi]: positive floats order like their bit patterns
+    bool amb = in && (__float_as_uint(s) - a.rc2_lo_bits - 1u) < a.band_bits;
     if (MONO) amb = amb || (in && r2b < a.tiny_u);
     amb_any = amb_any || amb;
     float f = pair_factor(a, r2b, A.w);
@@ -209,16 +214,18 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
     fx = fmaf(dx, f, fx);
     fy = fmaf(dy, f, fy);
     fz = fmaf(dz, f, fz);
-    nok += (ok && r2b > 0.f) ? 1u : 0u;  // r2b == 0 only for the target's own leaf
+    nok += ok ? 1u : 0u;  // the target's own leaf is masked out at emission
   }
 }
 
 // Float64 decisions for this lane's borderline pairs of one list (rare).
-template <bool MONO>
+template <bool MONO, int TPW>
 __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float thx,
                                           float thy, float thz, float tlx, float tly, float tlz, float* f3,
                                           uint32_t* nok, uint32_t* nexact) {
-  for (int e = 0; e < nl; ++e) {
+  constexpr int STRIDE = 32 / TPW;
+  const int t = lane & (TPW - 1);
+  for (int e = lane / TPW; e < nl; e += STRIDE) {
     const float4 A = *reinterpret_cast<const float4*>(&L[e].hx);
     const float4 B = *reinterpret_cast<const float4*>(&L[e].lx);
     const uint32_t mask = L[e].mask, node = L[e].node;
@@ -232,7 +239,7 @@ __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int
       const float ez = fmaxf(fabsf(dz) - B.w, 0.f);
       s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     }
-    const bool in = (mask >> lane) & 1u;
+    const bool in = (mask >> t) & 1u;
     bool amb = in && s > a.rc2_lo && s <= a.rc2_hi;
     if (MONO) amb = amb || (in && r2b < a.tiny_u);
     if (!amb) continue;
@@ -244,23 +251,24 @@ __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int
     f3[0] = fmaf(dx, f, f3[0]);
     f3[1] = fmaf(dy, f, f3[1]);
     f3[2] = fmaf(dz, f, f3[2]);
-    if (r2b > 0.f) ++*nok;
+    ++*nok;
   }
 }
 
 // Evaluate both interaction lists against this lane's target.
+template <int TPW>
 __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nll, const Entry* Lm, int nlm, int lane,
                                       uint32_t p, float thx, float thy, float thz, float tlx, float tly, float tlz,
                                       Acc& acc, uint32_t& nleaf, uint32_t& nmono, uint32_t& nexact, uint32_t& neval) {
   float fx = 0.f, fy = 0.f, fz = 0.f;
   bool amb_any = false;
   neval += (uint32_t)(nll + nlm);
-  flush_list<false>(a, Ll, nll, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nleaf, amb_any);
-  flush_list<true>(a, Lm, nlm, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nmono, amb_any);
+  flush_list<false, TPW>(a, Ll, nll, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nleaf, amb_any);
+  flush_list<true, TPW>(a, Lm, nlm, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nmono, amb_any);
   if (amb_any) {
     float f3[3] = {fx, fy, fz};
-    resolve_list<false>(a, Ll, nll, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nleaf, &nexact);
-    resolve_list<true>(a, Lm, nlm, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nmono, &nexact);
+    resolve_list<false, TPW>(a, Ll, nll, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nleaf, &nexact);
+    resolve_list<true, TPW>(a, Lm, nlm, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nmono, &nexact);
     fx = f3[0];
     fy = f3[1];
     fz = f3[2];
@@ -280,12 +288,14 @@ struct __align__(16) StackEntry {
 constexpr int STACK_ENTRIES = 1024;  // global, per warp
 constexpr uint32_t INFO_AMB = 0x80000000u;
 
-// Walk the tree for targets [first, first + count) (count <= 32) with one warp.
+// Walk the tree for targets [first, first + count) (count <= TPW) with one warp.
+template <int TPW>
 __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, Entry* Ll, Entry* Lm, uint8_t* owner,
                              StackEntry* stk) {
   const int lane = threadIdx.x & 31;
-  const bool has = (uint32_t)lane < count;
-  const uint32_t p = first + (has ? (uint32_t)lane : 0u);
+  const int tgt = lane & (TPW - 1);  // this lane's target within the group
+  const bool has = (uint32_t)tgt < count;
+  const uint32_t p = first + (has ? (uint32_t)tgt : 0u);
   const uint32_t tq[3] = {a.qx[p], a.qy[p], a.qz[p]};
   uint32_t oq[3];
 #pragma unroll
@@ -301,7 +311,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     bmin[d] = (float)mn * a.u_inv;
     bmax[d] = (float)mx * a.u_inv;
   }
-  const uint32_t mask0 = count >= 32 ? 0xFFFFFFFFu : ((1u << count) - 1u);
+  const uint32_t mask0 = count >= 32 ? 0xFFFFFFFFu : ((1u << count) - 1u);  // bit t: target t
   Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   uint32_t nleaf = 0, nmono = 0, nexact = 0, neval = 0;
   int nll = 0, nlm = 0, sp = 0;
@@ -372,7 +382,9 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
           split_rel(S[2], a.u_inv, &ent.hz, &ent.lz);
           ent.m = __uint_as_float(r0.w);
           ent.h = h;
-          ent.mask = imask;
+          // the reference skips the target's own leaf (j != skip)
+          const uint32_t own = leaf ? r1.z - first : 32u;
+          ent.mask = own < count ? (imask & ~(1u << own)) : imask;
           ent.node = leaf ? (r1.z | LEAF_BIT) : r1.z;
           ent.kind = leaf ? KIND_LEAF : KIND_MONO;
           is_leaf = leaf;
@@ -406,7 +418,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     sp += __popc(pm);
     __syncwarp();
     if (nll > CHUNK_L - 32 || nlm > CHUNK_M - 32) {
-      flush(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
+      flush<TPW>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
       __syncwarp();
       nll = 0;
       nlm = 0;
@@ -433,7 +445,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const uint32_t me = __shfl_sync(0xffffffffu, e.z, src);
       const int dep = wn_depth(__shfl_sync(0xffffffffu, e.y, src));
       bool pass = false;
-      if (has && ((me >> lane) & 1u)) {
+      if (has && lane < TPW && ((me >> tgt) & 1u)) {
         const uint4 w = __ldg(&a.walk[node]);
         const float h = ldexpf(a.h0_u, -dep);
         float s = 0.f;
@@ -450,7 +462,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
           ++nexact;
         }
       }
-      const uint32_t nm = __ballot_sync(0xffffffffu, pass);
+      const uint32_t nm = __ballot_sync(0xffffffffu, pass);  // lanes < TPW hold the targets
       if (lane == src) e.z = nm;
     }
     // distribute the children of the popped entries over the lanes
@@ -471,16 +483,26 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     }
   }
   if (nll + nlm > 0) {
-    flush(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
+    flush<TPW>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
   }
   __syncwarp();
-  if (has) {
-    a.ax[p] = (acc.sx) * a.out_scale;
-    a.ay[p] = (acc.sy) * a.out_scale;
-    a.az[p] = (acc.sz) * a.out_scale;
+  if (TPW < 32) {  // fold the two lanes of each target
+    float ox = __shfl_xor_sync(0xffffffffu, acc.sx, 16), oy = __shfl_xor_sync(0xffffffffu, acc.sy, 16);
+    float oz = __shfl_xor_sync(0xffffffffu, acc.sz, 16);
+    float cx = __shfl_xor_sync(0xffffffffu, acc.cx, 16), cy = __shfl_xor_sync(0xffffffffu, acc.cy, 16);
+    float cz = __shfl_xor_sync(0xffffffffu, acc.cz, 16);
+    acc.add(ox - cx, oy - cy, oz - cz);
+    nleaf += __shfl_xor_sync(0xffffffffu, nleaf, 16);
+    nmono += __shfl_xor_sync(0xffffffffu, nmono, 16);
+  }
+  if (has && lane < TPW) {
+    a.ax[p] = (acc.sx - acc.cx) * a.out_scale;
+    a.ay[p] = (acc.sy - acc.cy) * a.out_scale;
+    a.az[p] = (acc.sz - acc.cz) * a.out_scale;
     a.pcounts[2 * (int64_t)p] = nleaf;
     a.pcounts[2 * (int64_t)p + 1] = nmono;
   }
+  if (lane >= TPW) nleaf = nmono = 0;  // counted once per target
   // statistics
   unsigned long long l = nleaf, m = nmono, x = nexact;
   for (int off = 16; off > 0; off >>= 1) {
@@ -491,14 +513,14 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
   if (lane == 0) {
     atomicAdd(&a.stats[0], l);
     atomicAdd(&a.stats[1], m);
-    atomicAdd(&a.stats[2], (unsigned long long)neval * 32ull);
+    atomicAdd(&a.stats[2], (unsigned long long)neval * (unsigned long long)TPW);
     atomicAdd(&a.stats[3], x);
   }
 }
 
 constexpr size_t WALK_SMEM_PER_WARP = sizeof(Entry) * (CHUNK_L + CHUNK_M) + 32;
 
-template <int MIN_BLOCKS>
+template <int MIN_BLOCKS, int TPW>
 __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char s_walk[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -516,8 +538,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
     const uint32_t first = a.gfirst[g], count = a.gsize[g];
     // a group wider than 1/16 of the box would break the shared-origin minimum
     // image: walk its targets one at a time instead
-    const bool has = (uint32_t)lane < count;
-    const uint32_t p = first + (has ? lane : 0);
+    const bool has = (uint32_t)(lane & (TPW - 1)) < count;
+    const uint32_t p = first + (has ? (lane & (TPW - 1)) : 0);
     const uint32_t t0[3] = {a.qx[first], a.qy[first], a.qz[first]};
     const uint32_t tq[3] = {a.qx[p], a.qy[p], a.qz[p]};
     bool wide = false;
@@ -530,9 +552,9 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
     }
     wide = wide || a.single_target;
     if (!wide) {
-      walk_targets(a, first, count, list_l, list_m, owner, stk);
+      walk_targets<TPW>(a, first, count, list_l, list_m, owner, stk);
     } else {
-      for (uint32_t t = 0; t < count; ++t) walk_targets(a, first + t, 1u, list_l, list_m, owner, stk);
+      for (uint32_t t = 0; t < count; ++t) walk_targets<TPW>(a, first + t, 1u, list_l, list_m, owner, stk);
     }
   }
 }
@@ -615,33 +637,53 @@ __global__ void k_deferred(WalkArgs a, uint32_t n_items) {
 
 }  // namespace
 
-// Occupancy variant of the walk: register budget for 4, 5 or 6 resident
-// blocks of 4 warps per SM (TPM_WALK_BLOCKS overrides the default).
-static int walk_variant() {
-  static int v = [] {
-    const char* e = getenv("TPM_WALK_BLOCKS");
-    int b = e ? atoi(e) : 5;
-    return (b == 4 || b == 5 || b == 6) ? b : 5;
-  }();
+// Variants of the walk: the register budget for 4, 5 or 6 resident blocks of
+// 4 warps per SM (TPM_WALK_BLOCKS) and 32 or 16 targets per warp
+// (TPM_WALK_TARGETS; with 16, two lanes share each target).
+static int env_choice(const char* name, int dflt, int a, int b, int c) {
+  const char* e = getenv(name);
+  const int v = e ? atoi(e) : dflt;
+  return (v == a || v == b || v == c) ? v : dflt;
+}
+static int walk_blocks_variant() {
+  static int v = env_choice("TPM_WALK_BLOCKS", 5, 4, 5, 6);
+  return v;
+}
+int walk_targets_per_warp() {
+  static int v = env_choice("TPM_WALK_TARGETS", 32, 32, 16, 32);
   return v;
 }
 
-template <int B>
+template <int B, int T>
 static int blocks_for() {
   const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
-  TPM_CUDA(cudaFuncSetAttribute(k_walk<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TPM_CUDA(cudaFuncSetAttribute(k_walk<B, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int nb = 0;
-  TPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<B>, WALK_THREADS, smem));
+  TPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<B, T>, WALK_THREADS, smem));
   return nb < 1 ? 1 : nb;
 }
 
-int walk_blocks_per_sm() {
-  switch (walk_variant()) {
-    case 4: return blocks_for<4>();
-    case 6: return blocks_for<6>();
-    default: return blocks_for<5>();
+template <int T>
+static int blocks_t() {
+  switch (walk_blocks_variant()) {
+    case 4: return blocks_for<4, T>();
+    case 6: return blocks_for<6, T>();
+    default: return blocks_for<5, T>();
   }
 }
+
+int walk_blocks_per_sm() { return walk_targets_per_warp() == 16 ? blocks_t<16>() : blocks_t<32>(); }
+
+template <int T>
+static void launch_t(const WalkArgs& a, int grid, cudaStream_t s) {
+  const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
+  switch (walk_blocks_variant()) {
+    case 4: k_walk<4, T><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    case 6: k_walk<6, T><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    default: k_walk<5, T><<<grid, WALK_THREADS, smem, s>>>(a); break;
+  }
+}
+
 int walk_threads() { return WALK_THREADS; }
 size_t walk_stack_words(int grid, int stack_cap) {
   (void)stack_cap;
@@ -649,12 +691,8 @@ size_t walk_stack_words(int grid, int stack_cap) {
 }
 
 void launch_walk(const WalkArgs& a, int grid, cudaStream_t s) {
-  const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
-  switch (walk_variant()) {
-    case 4: k_walk<4><<<grid, WALK_THREADS, smem, s>>>(a); break;
-    case 6: k_walk<6><<<grid, WALK_THREADS, smem, s>>>(a); break;
-    default: k_walk<5><<<grid, WALK_THREADS, smem, s>>>(a); break;
-  }
+  if (walk_targets_per_warp() == 16) launch_t<16>(a, grid, s);
+  else launch_t<32>(a, grid, s);
   TPM_LAUNCH_CHECK();
 }
 

@@ -35,6 +35,7 @@ struct WalkArgs {
   float box_u;    // box side in walk units (2^32 quanta)
   float h0_u;     // root half side in u
   float rc2_lo, rc2_hi;    // per-target ambiguity band around r_cut^2 (u^2)
+  uint32_t rc2_lo_bits, band_bits;  // the band as float bit patterns: (lo, lo + band]
   float grc2_lo, grc2_hi;  // group-level band
   float eps2_u;
   float pcx;      // 0.3275911 * scale*2^U / (sqrt(2) r_s)
@@ -57,6 +58,7 @@ struct WalkArgs {
 };
 
 int walk_blocks_per_sm();
+int walk_targets_per_warp();
 int walk_threads();
 size_t walk_stack_words(int grid, int stack_cap);
 void launch_walk(const WalkArgs& a, int grid, cudaStream_t s);

@@ -104,6 +104,7 @@ SIGNATURES = {
     "tpm_export_tree": ([_P, _I64, _P, _P, _P, _P, _P, _P, _P], _I64),
     "tpm_get_mesh": ([_P, _P, _P, _P, _P], _I),
     "tpm_fp32_peak": ([_I, C.POINTER(_D)], _I),
+    "tpm_ewald": ([_P, _P, _I64, _D, _D, _D, _D, _P, _I64, _D, _D, _I, _I, _P], _I),
     "tpm_hilbert_sort_noalloc": ([_P, _P, _P, _I64, _D, _P, _P, _P], _I),
 }
 NOALLOC_MAX_PARTICLES = 1 << 18

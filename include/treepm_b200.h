@@ -207,7 +207,16 @@ int tpm_hilbert_sort_noalloc(const uint32_t* qx, const uint32_t* qy, const uint3
                              double box_size, uint64_t* keys_out, uint32_t* order_out, void* stream);
 
 /* ---- measurement -----------------------------------------------------------
- * No counterpart in the reference: FFMA throughput of `device` in TFLOP/s, the
+ * No counterpart in the reference: FP64 Ewald accelerations of the targets
+ * (periodic box `box`, coupling g), the accuracy reference of the TreePM
+ * force.  Real space over minimum images within r_c (Ewald parameter alpha),
+ * k space over integer modes 0 < |n| <= n_max; nearest images closer than
+ * r_soft are Plummer softened with eps2.  Host arrays in and out (n x 3
+ * positions, n masses, nt target indices, nt x 3 out); allocates and frees its
+ * own device buffers.  A checker: run outside timed regions. */
+int tpm_ewald(const double* pos, const double* mass, int64_t n, double box, double g, double eps2, double r_soft,
+              const int64_t* targets, int64_t nt, double alpha, double r_c, int n_max, int device, double* out);
+/* No counterpart in the reference: FFMA throughput of `device` in TFLOP/s, the
  * FP32 roofline denominator of the short-range walk. */
 int tpm_fp32_peak(int device, double* tflops);
 

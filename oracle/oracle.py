@@ -60,6 +60,7 @@ def lib():
             "orc_advance_a": ([_d, _d, _d, _d, _d], _d),
             "orc_kdk_step_treepm": ([_p, _p, _p, _i64, _d, _d, _d, _d, _d, _i32, _d, _d, _d, _p], _i32),
             "orc_direct_min_image": ([_p, _p, _i64, _d, _d, _d, _p, _i64, _p], None),
+            "orc_ewald": ([_p, _p, _i64, _d, _d, _d, _d, _p, _i64, _d, _d, _i32, _p], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -288,4 +289,14 @@ def direct_min_image(pos, mass, eps2, g, box, targets=None):
     out = np.zeros((t.shape[0], 3))
     lib().orc_direct_min_image(_ptr(pos), _ptr(mass), n, float(eps2), float(g), float(box), _ptr(t), t.shape[0],
                                _ptr(out))
+    return out
+
+
+def ewald(pos, mass, box, g, eps2, r_soft, targets, alpha, r_c, n_max):
+    """FP64 Ewald accelerations at `targets` (nearest images within r_soft Plummer-softened)."""
+    pos, mass = _f64(pos), _f64(mass)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    out = np.zeros((t.shape[0], 3))
+    lib().orc_ewald(_ptr(pos), _ptr(mass), pos.shape[0], float(box), float(g), float(eps2), float(r_soft), _ptr(t),
+                    t.shape[0], float(alpha), float(r_c), int(n_max), _ptr(out))
     return out
