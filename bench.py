@@ -186,6 +186,32 @@ def fp32_peak_tflops(lib_solver):
     return out.value
 
 
+def accurate_mode_report(box, mesh, phys, pos, g, targets, ref, device, reps=3):
+    """Speed and Ewald error of the extension mode (complete split kernel,
+    opening angle 0.5, CIC deconvolution) on the bench's final state."""
+    import treepm
+    from treepm import accuracy
+    s = treepm.TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"], accurate=True,
+                            theta=0.5, deconvolve_cic=True, device=device)
+    s.set_particles(pos, box.mass)
+    for _ in range(2):
+        s.compute_forces(phys["eps2"], g)
+    ms, inter = [], []
+    for _ in range(reps):
+        s.compute_forces(phys["eps2"], g)
+        st = s.stats()
+        ms.append(st["ms_total"])
+        inter.append(st["leaf_pairs"] + st["monopoles"])
+    _, _, acc = s.get_state(box.n, pos=False, vel=False)
+    rms, p99 = accuracy.relative_errors(acc[targets], ref)
+    s.close()
+    m = float(np.mean(ms))
+    return {"flags": "accurate | deconvolve_cic", "theta": 0.5, "ms_per_force_evaluation": m,
+            "particle_updates_per_s": box.n / (m * 1e-3),
+            "interactions_per_particle": float(np.mean(inter)) / box.n,
+            "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -243,7 +269,7 @@ def run_b200(args):
     value = world * n * args.steps / (dev_ms * 1e-3)
 
     # ---- force error of the last evaluation against FP64 Ewald ------------
-    ewald = None
+    ewald = accurate = None
     if rank == 0 and not args.no_ewald:
         from treepm import accuracy
         p_now, _, a_now = solver.get_state(n, pos=True, vel=False, acc=True)
@@ -255,6 +281,8 @@ def run_b200(args):
         rms, p99 = accuracy.relative_errors(a_now[tg], ref)
         ewald = {"rms": rms, "p99": p99, "targets": int(len(tg)), "seconds": time.perf_counter() - t_e,
                  "reference": "FP64 Ewald, Plummer-softened nearest images within r_cut"}
+        if not args.no_accurate:
+            accurate = accurate_mode_report(box, mesh, phys, p_now, g_last, tg, ref, local)
 
     # ---- end to end through the host-buffer API (e2e) -------------------
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
@@ -320,6 +348,7 @@ def run_b200(args):
                         "two force evaluations (no cached acceleration across calls), state back to host"},
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "force_error_vs_ewald": ewald,
+        "accurate_mode": accurate,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -352,6 +381,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak measurement (profiling runs)")
     ap.add_argument("--no-ewald", action="store_true", help="skip the FP64 Ewald error report")
+    ap.add_argument("--no-accurate", action="store_true", help="skip the accurate-mode report")
     ap.add_argument("--ewald-targets", type=int, default=4096)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -440,6 +440,18 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       const double tq = std::ldexp(4.0, -U);
       a.tiny_u = (float)(tq * tq);
       a.out_scale = (float)(1.0 / (u * u));
+      a.accurate = (h->cfg.flags & TPM_FLAG_ACCURATE) ? 1 : 0;
+      a.gkc = a.accurate ? (float)(2.0 / std::sqrt(M_PI) * cx) : 0.f;
+      {
+        const double th = h->cfg.theta > 0.0 ? h->cfg.theta : 0.5;
+        a.theta2 = (float)(th * th);
+      }
+      if (a.accurate) {  // no reference decisions to reproduce: no float64 band, no COM-on-target opening
+        a.rc2_lo = a.rc2_hi = (float)rc2_u;
+        std::memcpy(&a.rc2_lo_bits, &a.rc2_lo, 4);
+        a.band_bits = 0u;
+        a.tiny_u = -1.f;
+      }
       a.ax = h->srx; a.ay = h->sry; a.az = h->srz;
       a.stats = h->stats_dev; a.err = T.err;
       a.deferred = h->deferred; a.ndeferred = h->ndeferred; a.cap_deferred = DEFERRED_CAP;
@@ -558,6 +570,10 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
       throw Error(TPM_ERR_INVALID_ARGUMENT, "pm_grid_size must be a power of two in [4, 1024]");
     if (!(cfg->box_size > 0.0) || !std::isfinite(cfg->box_size))
       throw Error(TPM_ERR_INVALID_ARGUMENT, "box_size must be positive");
+    // accurate mode: a cell holding the target has s/d >= 1/sqrt(3) for any
+    // centre of mass inside it, so theta below that never accepts one
+    if ((cfg->flags & TPM_FLAG_ACCURATE) && !(cfg->theta == 0.0 || (cfg->theta > 0.0 && cfg->theta < 0.577)))
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "accurate mode needs theta in (0, 0.577)");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
       cudaGetLastError();
@@ -589,7 +605,7 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
     h->ndeferred = h->alloc<uint32_t>(1, 0);
     h->deferred = h->alloc<uint2>(DEFERRED_CAP, 0);
     int sms = prop.multiProcessorCount;
-    h->walk_grid = sms * walk_blocks_per_sm();
+    h->walk_grid = sms * walk_blocks_per_sm((cfg->flags & TPM_FLAG_ACCURATE) != 0);
     h->stack = h->alloc<uint32_t>(walk_stack_words(h->walk_grid, STACK_CAP), 0);
     TPM_CUDA(cudaMemset(h->T.err, 0, sizeof(uint32_t)));
     pm_plan_init(h->pm, nm, cfg->box_size, h->pm_only ? 0.0 : h->r_s, cfg->flags, cfg->device);

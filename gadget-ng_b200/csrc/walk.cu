@@ -37,9 +37,7 @@ namespace {
 constexpr int WALK_WARPS = 4;
 constexpr int WALK_THREADS = WALK_WARPS * 32;
 constexpr int CHUNK_L = 96;  // leaf-list capacity
-constexpr int CHUNK_M = 64;  // monopole-list capacity
-constexpr uint32_t AMB_FLAG = 0x40000000u;
-constexpr uint32_t NODE_MASK = 0x3FFFFFFFu;
+constexpr int CHUNK_M = 96;  // monopole-list capacity
 constexpr int32_t WIDE_GROUP = 1 << 28;  // quanta: 1/16 of the box
 
 enum : uint32_t { KIND_LEAF = 0, KIND_MONO = 1 };
@@ -154,7 +152,9 @@ __device__ __forceinline__ void defer(const WalkArgs& a, uint32_t p, uint32_t no
   else atomicOr(a.err, DEV_ERR_DEFERRED);
 }
 
-// FP32 pair term: returns m * erfc(r/(sqrt2 r_s)) / r^3 (walk units).
+// FP32 pair term: returns m * erfc(x) / r^3 (walk units), x = r/(sqrt2 r_s);
+// ACC (accurate mode) adds the Gaussian term (2x/sqrt(pi)) exp(-x^2).
+template <bool ACC = false>
 __device__ __forceinline__ float pair_factor(const WalkArgs& a, float r2b, float m) {
   float r2 = fmaxf(r2b + a.eps2_u, 1e-30f);
   float ri = rsqrt_approx(r2);
@@ -162,7 +162,8 @@ __device__ __forceinline__ float pair_factor(const WalkArgs& a, float r2b, float
   float tt = rcp_approx(fmaf(a.pcx, r, 1.0f));
   float poly = tt * fmaf(tt, fmaf(tt, fmaf(tt, fmaf(tt, ErfcConst::A5, ErfcConst::A4), ErfcConst::A3), ErfcConst::A2),
                          ErfcConst::A1);
-  float w = poly * ex2_approx(r2 * a.ex2k);
+  if (ACC) poly = fmaf(a.gkc, r, poly);
+  const float w = poly * ex2_approx(r2 * a.ex2k);
   return m * w * (ri * ri * ri);
 }
 
@@ -180,7 +181,7 @@ struct Acc {
 // monopole list (AABB-gap test) or the leaf list (bare-distance test; the
 // aperiodic walk's leaves carry their half side and take the AABB test too).
 // Borderline pairs are left out here and flagged; resolve_list settles them.
-template <bool MONO, int TPW>
+template <bool MONO, int TPW, bool ACC>
 __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, int nl, int lane, float thx, float thy,
                                            float thz, float tlx, float tly, float tlz, float& fx, float& fy,
                                            float& fz, uint32_t& nok, bool& amb_any) {
@@ -205,11 +206,13 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
     }
     const bool in = (mask >> t) & 1u;
     const bool ok = in && s <= a.rc2_lo;
-    // s in (rc2_lo, rc2_hi]: positive floats order like their bit patterns
-    bool amb = in && (__float_as_uint(s) - a.rc2_lo_bits - 1u) < a.band_bits;
-    if (MONO) amb = amb || (in && r2b < a.tiny_u);
-    amb_any = amb_any || amb;
-    float f = pair_factor(a, r2b, A.w);
+    if (!ACC) {  // accurate mode reproduces no float64 decisions
+      // s in (rc2_lo, rc2_hi]: positive floats order like their bit patterns
+      bool amb = in && (__float_as_uint(s) - a.rc2_lo_bits - 1u) < a.band_bits;
+      if (MONO) amb = amb || (in && r2b < a.tiny_u);
+      amb_any = amb_any || amb;
+    }
+    float f = pair_factor<ACC>(a, r2b, A.w);
     f = ok ? f : 0.f;
     fx = fmaf(dx, f, fx);
     fy = fmaf(dy, f, fy);
@@ -256,16 +259,16 @@ __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int
 }
 
 // Evaluate both interaction lists against this lane's target.
-template <int TPW>
+template <int TPW, bool ACC>
 __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nll, const Entry* Lm, int nlm, int lane,
                                       uint32_t p, float thx, float thy, float thz, float tlx, float tly, float tlz,
                                       Acc& acc, uint32_t& nleaf, uint32_t& nmono, uint32_t& nexact, uint32_t& neval) {
   float fx = 0.f, fy = 0.f, fz = 0.f;
   bool amb_any = false;
   neval += (uint32_t)(nll + nlm);
-  flush_list<false, TPW>(a, Ll, nll, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nleaf, amb_any);
-  flush_list<true, TPW>(a, Lm, nlm, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nmono, amb_any);
-  if (amb_any) {
+  flush_list<false, TPW, ACC>(a, Ll, nll, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nleaf, amb_any);
+  flush_list<true, TPW, ACC>(a, Lm, nlm, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nmono, amb_any);
+  if (!ACC && amb_any) {
     float f3[3] = {fx, fy, fz};
     resolve_list<false, TPW>(a, Ll, nll, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nleaf, &nexact);
     resolve_list<true, TPW>(a, Lm, nlm, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nmono, &nexact);
@@ -281,15 +284,16 @@ __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nl
 // targets that still see it, and the octree id for the per-target test.
 struct __align__(16) StackEntry {
   uint32_t first;  // record index of the first child
-  uint32_t info;   // the node's record info | AMB_FLAG when undecided for the group
+  uint32_t info;   // the node's record info | INFO_AMB / INFO_MAC when undecided for the group
   uint32_t mask;
   uint32_t ref;    // octree node id
 };
 constexpr int STACK_ENTRIES = 1024;  // global, per warp
 constexpr uint32_t INFO_AMB = 0x80000000u;
+constexpr uint32_t INFO_MAC = 0x40000000u;  // opening angle undecided for the group
 
 // Walk the tree for targets [first, first + count) (count <= TPW) with one warp.
-template <int TPW>
+template <int TPW, bool ACC>
 __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, Entry* Ll, Entry* Lm, uint8_t* owner,
                              StackEntry* stk) {
   const int lane = threadIdx.x & 31;
@@ -341,13 +345,15 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const uint32_t info = r1.y;
       const bool leaf = (info & WN_LEAF) != 0;
       const int dep = wn_depth(info);
-      const float h = (leaf && a.periodic) ? 0.f : ldexpf(a.h0_u, -dep);
-      const bool open = !leaf && !(info & WN_TERMINAL);
+      const float hnode = ldexpf(a.h0_u, -dep);
+      // cull half side: the COM-centred AABB of the reference, or (accurate
+      // mode) twice that, which holds the whole cell
+      const float h = (leaf && a.periodic) ? 0.f : (ACC && !leaf ? 2.f * hnode : hnode);
       const uint32_t cq[3] = {r0.x, r0.y, r0.z};
       // Per axis, the targets see the node at the minimum image of S - t for t
       // in [bmin, bmax]: bound min / max of |wrap(S - t)| over that interval
       // (images at 0 and +-L), then the AABB gap.
-      float emin2 = 0.f, emax2 = 0.f;
+      float emin2 = 0.f, emax2 = 0.f, dmin2 = 0.f, dmax2 = 0.f;
       int32_t S[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -366,13 +372,28 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
         const float far = fmaxf(dmax - h, 0.f);
         emin2 = fmaf(gap, gap, emin2);
         emax2 = fmaf(far, far, emax2);
+        dmin2 = fmaf(dmin, dmin, dmin2);
+        dmax2 = fmaf(dmax, dmax, dmax2);
+      }
+      bool open, macmix = false;
+      if (ACC && !leaf) {
+        // opening angle s/d < theta, s = 2 * half side (octree.rs:763-809);
+        // a margin on both sides leaves the float-rounding cases to the
+        // per-target test at pop time
+        const float s2 = 4.f * hnode * hnode;
+        const bool accept_all = s2 < a.theta2 * dmin2 * 0.999f;
+        const bool open_all = s2 >= a.theta2 * dmax2 * 1.001f;
+        open = !accept_all;
+        macmix = !accept_all && !open_all;
+      } else {
+        open = !leaf && !(info & WN_TERMINAL);
       }
       if (!(emin2 > a.grc2_hi)) {
         if (open) {
           push = true;
           ambig = !(emax2 < a.grc2_lo);
           se.first = r1.x;
-          se.info = info | (ambig ? INFO_AMB : 0u);
+          se.info = info | (ambig ? INFO_AMB : 0u) | (macmix ? INFO_MAC : 0u);
           se.mask = imask;
           se.ref = r1.z;
         } else {
@@ -388,7 +409,6 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
           ent.node = leaf ? (r1.z | LEAF_BIT) : r1.z;
           ent.kind = leaf ? KIND_LEAF : KIND_MONO;
           is_leaf = leaf;
-          ent.pad = 0;
         }
       }
     }
@@ -417,8 +437,10 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     }
     sp += __popc(pm);
     __syncwarp();
-    if (nll > CHUNK_L - 32 || nlm > CHUNK_M - 32) {
-      flush<TPW>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
+    // before the next check the pop adds up to 32 monopole entries (accurate
+    // mode) and the next classification up to 32 to either list
+    if (nll > CHUNK_L - 32 || nlm > CHUNK_M - (ACC ? 64 : 32)) {
+      flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
       __syncwarp();
       nll = 0;
       nlm = 0;
@@ -447,7 +469,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       bool pass = false;
       if (has && lane < TPW && ((me >> tgt) & 1u)) {
         const uint4 w = __ldg(&a.walk[node]);
-        const float h = ldexpf(a.h0_u, -dep);
+        const float h = ldexpf(a.h0_u, (ACC ? 1 : 0) - dep);
         float s = 0.f;
         const uint32_t wq[3] = {w.x, w.y, w.z};
 #pragma unroll
@@ -457,7 +479,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
           s = fmaf(ee, ee, s);
         }
         if (s <= a.rc2_lo) pass = true;
-        else if (s <= a.rc2_hi) {
+        else if (!ACC && s <= a.rc2_hi) {
           pass = exact_open_pass(a, p, node);
           ++nexact;
         }
@@ -465,6 +487,46 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const uint32_t nm = __ballot_sync(0xffffffffu, pass);  // lanes < TPW hold the targets
       if (lane == src) e.z = nm;
     }
+    // accurate mode: per-target opening angle for nodes undecided for the
+    // group; targets that accept take the node as a monopole now, the rest
+    // open it
+    uint32_t macm = ACC ? __ballot_sync(0xffffffffu, lane < k && (e.y & INFO_MAC)) : 0u;
+    while (macm) {
+      const int src = __ffs(macm) - 1;
+      macm &= macm - 1;
+      const uint32_t node = __shfl_sync(0xffffffffu, e.w, src);
+      const uint32_t me = __shfl_sync(0xffffffffu, e.z, src);
+      const int dep = wn_depth(__shfl_sync(0xffffffffu, e.y, src));
+      const uint4 w = __ldg(&a.walk[node]);
+      const float hnode = ldexpf(a.h0_u, -dep);
+      bool accept = false;
+      if (has && lane < TPW && ((me >> tgt) & 1u)) {
+        float d2 = 0.f;
+        const uint32_t wq[3] = {w.x, w.y, w.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const float dd = (float)rel32(wq[d], tq[d], a.periodic) * a.u_inv;
+          d2 = fmaf(dd, dd, d2);
+        }
+        accept = 4.f * hnode * hnode < a.theta2 * d2;
+      }
+      const uint32_t am = __ballot_sync(0xffffffffu, accept);
+      if (am) {  // one monopole entry for the accepting targets (same slot on every lane)
+        if (lane == src) {
+          float hx, lx, hy, ly, hz, lz;
+          split_rel(rel32(w.x, oq[0], a.periodic), a.u_inv, &hx, &lx);
+          split_rel(rel32(w.y, oq[1], a.periodic), a.u_inv, &hy, &ly);
+          split_rel(rel32(w.z, oq[2], a.periodic), a.u_inv, &hz, &lz);
+          float4* dst = reinterpret_cast<float4*>(&Lm[nlm]);
+          dst[0] = make_float4(hx, hy, hz, __uint_as_float(w.w));
+          dst[1] = make_float4(lx, ly, lz, 2.f * hnode);
+          *reinterpret_cast<uint4*>(&dst[2]) = make_uint4(am, node, KIND_MONO, 0u);
+        }
+        ++nlm;
+      }
+      if (lane == src) e.z = me & ~am;
+    }
+    __syncwarp();
     // distribute the children of the popped entries over the lanes
     const uint32_t excl = incl - nc;
     if (lane < k)
@@ -483,7 +545,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     }
   }
   if (nll + nlm > 0) {
-    flush<TPW>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
+    flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
   }
   __syncwarp();
   if (TPW < 32) {  // fold the two lanes of each target
@@ -520,7 +582,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
 
 constexpr size_t WALK_SMEM_PER_WARP = sizeof(Entry) * (CHUNK_L + CHUNK_M) + 32;
 
-template <int MIN_BLOCKS, int TPW>
+template <int MIN_BLOCKS, int TPW, bool ACC>
 __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char s_walk[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -552,9 +614,9 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
     }
     wide = wide || a.single_target;
     if (!wide) {
-      walk_targets<TPW>(a, first, count, list_l, list_m, owner, stk);
+      walk_targets<TPW, ACC>(a, first, count, list_l, list_m, owner, stk);
     } else {
-      for (uint32_t t = 0; t < count; ++t) walk_targets<TPW>(a, first + t, 1u, list_l, list_m, owner, stk);
+      for (uint32_t t = 0; t < count; ++t) walk_targets<TPW, ACC>(a, first + t, 1u, list_l, list_m, owner, stk);
     }
   }
 }
@@ -654,33 +716,41 @@ int walk_targets_per_warp() {
   return v;
 }
 
-template <int B, int T>
+template <int B, int T, bool ACC>
 static int blocks_for() {
   const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
-  TPM_CUDA(cudaFuncSetAttribute(k_walk<B, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TPM_CUDA(cudaFuncSetAttribute(k_walk<B, T, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int nb = 0;
-  TPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<B, T>, WALK_THREADS, smem));
+  TPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<B, T, ACC>, WALK_THREADS, smem));
   return nb < 1 ? 1 : nb;
 }
 
+// the accurate mode has one variant (5 blocks per SM)
 template <int T>
-static int blocks_t() {
+static int blocks_t(bool accurate) {
+  if (accurate) return blocks_for<5, T, true>();
   switch (walk_blocks_variant()) {
-    case 4: return blocks_for<4, T>();
-    case 6: return blocks_for<6, T>();
-    default: return blocks_for<5, T>();
+    case 4: return blocks_for<4, T, false>();
+    case 6: return blocks_for<6, T, false>();
+    default: return blocks_for<5, T, false>();
   }
 }
 
-int walk_blocks_per_sm() { return walk_targets_per_warp() == 16 ? blocks_t<16>() : blocks_t<32>(); }
+int walk_blocks_per_sm(bool accurate) {
+  return walk_targets_per_warp() == 16 ? blocks_t<16>(accurate) : blocks_t<32>(accurate);
+}
 
 template <int T>
 static void launch_t(const WalkArgs& a, int grid, cudaStream_t s) {
   const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
+  if (a.accurate) {
+    k_walk<5, T, true><<<grid, WALK_THREADS, smem, s>>>(a);
+    return;
+  }
   switch (walk_blocks_variant()) {
-    case 4: k_walk<4, T><<<grid, WALK_THREADS, smem, s>>>(a); break;
-    case 6: k_walk<6, T><<<grid, WALK_THREADS, smem, s>>>(a); break;
-    default: k_walk<5, T><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    case 4: k_walk<4, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    case 6: k_walk<6, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    default: k_walk<5, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
   }
 }
 

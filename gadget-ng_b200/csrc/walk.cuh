@@ -42,6 +42,9 @@ struct WalkArgs {
   float ex2k;     // -(scale*2^U / (sqrt(2) r_s))^2 * log2(e)
   float tiny_u;   // (4 quanta)^2 in u^2
   float out_scale;  // 1/u^2 in physical units
+  int accurate;      // extension mode: complete split kernel + opening angle
+  float theta2;      // opening angle squared (accurate mode)
+  float gkc;         // (2/sqrt(pi)) * u/(sqrt(2) r_s): the Gaussian term of the split
   // outputs (physical, per unit G), sorted order
   float* ax;
   float* ay;
@@ -57,7 +60,7 @@ struct WalkArgs {
   uint32_t* pcounts;     // per target (sorted order): leaf pairs, monopoles
 };
 
-int walk_blocks_per_sm();
+int walk_blocks_per_sm(bool accurate);
 int walk_targets_per_warp();
 int walk_threads();
 size_t walk_stack_words(int grid, int stack_cap);

@@ -30,6 +30,7 @@ FLAG_DECONVOLVE_CIC = 1 << 1
 FLAG_FOUR_POINT_GRADIENT = 1 << 2
 FLAG_PM_ONLY = 1 << 3
 FLAG_HILBERT_TARGETS = 1 << 4
+FLAG_ACCURATE = 1 << 5
 
 
 class TpmConfig(C.Structure):

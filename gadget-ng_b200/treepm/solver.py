@@ -52,13 +52,17 @@ class TreePmSolver:
     <= 0 selects 2.5 cells.  `r_cut_factor` is the extension key for r_cut / r_s
     (the reference hard-codes 5).  `periodic_walk` selects the periodic walk of
     the P=1 slab path (default) or the aperiodic walk of the trait-level solver.
+    `accurate` selects the extension mode (complete split kernel, geometric
+    opening angle `theta`); it is validated against Ewald, not the reference.
     """
 
     def __init__(self, grid_size: int, box_size: float, r_split: float = 0.0, *, r_cut_factor: float = 5.0,
                  periodic_walk: bool = True, theta: float = 0.5, opening_criterion: int = 0,
                  err_tol_force_acc: float = 0.005, deconvolve_cic: bool = False, four_point_gradient: bool = False,
-                 device: int = 0, memory_cap_bytes: int = 0, _pm_only: bool = False):
+                 accurate: bool = False, device: int = 0, memory_cap_bytes: int = 0, _pm_only: bool = False):
         flags = 0
+        if accurate:
+            flags |= _lib.FLAG_ACCURATE
         if not periodic_walk:
             flags |= _lib.FLAG_APERIODIC_WALK
         if deconvolve_cic:
@@ -206,7 +210,8 @@ def make_solver(cfg: dict):
 
     `cfg` is the parsed TOML document: [simulation] box_size, [gravity]
     solver / pm_grid_size / r_split / theta / opening_criterion /
-    err_tol_force_acc and the extension r_cut_factor.
+    err_tol_force_acc and the extension keys r_cut_factor and
+    treepm_accurate (the complete split kernel with the opening angle).
     """
     sim = cfg.get("simulation", {})
     grav = cfg.get("gravity", {})
@@ -223,7 +228,8 @@ def make_solver(cfg: dict):
                         periodic_walk=bool(grav.get("treepm_slab", True)),
                         theta=float(grav.get("theta", 0.5)),
                         opening_criterion=1 if crit in ("relative", 1) else 0,
-                        err_tol_force_acc=float(grav.get("err_tol_force_acc", 0.005)))
+                        err_tol_force_acc=float(grav.get("err_tol_force_acc", 0.005)),
+                        accurate=bool(grav.get("treepm_accurate", False)))
 
 
 def drift_kick_factors(omega_m: float, omega_lambda: float, h0: float, a0: float, dt: float):

@@ -66,13 +66,22 @@ enum {
 /* Group walk targets along the Hilbert curve of sfc.rs:95-204 instead of the
  * octree's own order. */
 #define TPM_FLAG_HILBERT_TARGETS    (1u << 4)
+/* Accurate short range (extension, validated against Ewald only): the split
+ * kernel erfc(x) + (2x/sqrt(pi)) exp(-x^2) that complements the Gaussian
+ * long-range filter exactly (the reference's short_range.rs:108-111 keeps
+ * erfc(x) alone), and the geometric opening criterion s/d < theta of the
+ * reference's Barnes-Hut walk (crates/gadget-ng-tree/src/octree.rs:763-809)
+ * instead of the 0.1 r_cut node-size rule, so a node holding the target is
+ * never taken as a monopole (theta must lie in (0, 0.577)).  Culls use the
+ * node's whole cell. */
+#define TPM_FLAG_ACCURATE           (1u << 5)
 
 typedef struct tpm_config {
   int32_t grid_size;          /* [gravity] pm_grid_size (power of two, 8..1024) */
   double box_size;            /* [simulation] box_size */
   double r_split;             /* [gravity] r_split; <= 0 selects 2.5 cells (solver.rs:56-62) */
   double r_cut_factor;        /* extension key gravity.r_cut_factor; <= 0 selects 5.0 (solver.rs:80) */
-  double theta;               /* [gravity] theta (kept for the TOML contract; unused by the TreePM walk) */
+  double theta;               /* [gravity] theta: unused by the parity walk; the opening angle of TPM_FLAG_ACCURATE (0 = 0.5) */
   int32_t opening_criterion;  /* [gravity] opening_criterion: 0 geometric, 1 relative (unused by TreePM) */
   double err_tol_force_acc;   /* [gravity] err_tol_force_acc (unused by TreePM) */
   uint32_t flags;             /* TPM_FLAG_* */
