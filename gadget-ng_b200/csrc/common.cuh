@@ -42,6 +42,7 @@ enum : uint32_t {
   DEV_ERR_LIST = 1u << 3,
   DEV_ERR_TIE_RUN = 1u << 4,
   DEV_ERR_NONFINITE = 1u << 5,
+  DEV_ERR_MMA_TIMEOUT = 1u << 6,  // a tensor-core wait ran past its time limit
 };
 
 // ---- fixed point --------------------------------------------------------------

@@ -185,7 +185,8 @@ __global__ void k_fft_y(float2* __restrict__ spec, int64_t comp_stride, int nm, 
 // ---- z pass + Green's function x filter x gradient + inverse z pass ---------------
 __global__ void k_fft_z_poisson(const float2* __restrict__ spec, float2* __restrict__ spec3, int nm, int logn,
                                 int nh, int tx, const float2* __restrict__ tw, const float* __restrict__ kval,
-                                const float* __restrict__ kfilter, const float* __restrict__ kderiv, float kcoef) {
+                                const float* __restrict__ kfilter, const float* __restrict__ kderiv, float kcoef,
+                                int ncomp) {
   extern __shared__ float2 sm[];
   float2* s_tw = sm;
   float2* a = sm + (nm >> 1);
@@ -216,12 +217,16 @@ __global__ void k_fft_z_poisson(const float2* __restrict__ spec, float2* __restr
     rho_k[idx] = v;  // phi
   }
   __syncthreads();
-  for (int comp = 0; comp < 3; ++comp) {
+  for (int comp = 0; comp < ncomp; ++comp) {
     for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
       const int z = idx / tx, c = idx % tx;
       const int kx = kx0 + c < nh ? kx0 + c : 0;
-      const float d = comp == 0 ? kderiv[kx] : (comp == 1 ? kderiv[y] : kderiv[z]);
       const float2 ph = rho_k[idx];
+      if (comp == 3) {  // the potential itself
+        c3[idx] = ph;
+        continue;
+      }
+      const float d = comp == 0 ? kderiv[kx] : (comp == 1 ? kderiv[y] : kderiv[z]);
       c3[idx] = make_float2(d * ph.y, -d * ph.x);
     }
     __syncthreads();
@@ -374,8 +379,9 @@ void pm_plan_init(PmPlan& p, int nm, double box, double r_split, uint32_t flags,
   TPM_CUDA(cudaMalloc(&p.kderiv, sizeof(float) * nm));
   TPM_CUDA(cudaMalloc(&p.rho, sizeof(float) * nm3));
   TPM_CUDA(cudaMalloc(&p.spec, sizeof(float2) * nspec));
-  TPM_CUDA(cudaMalloc(&p.spec3, sizeof(float2) * nspec * 3));
-  TPM_CUDA(cudaMalloc(&p.force, sizeof(float) * nm3 * 3));
+  p.ncomp = (flags & (1u << 6)) ? 4 : 3;
+  TPM_CUDA(cudaMalloc(&p.spec3, sizeof(float2) * nspec * p.ncomp));
+  TPM_CUDA(cudaMalloc(&p.force, sizeof(float) * nm3 * p.ncomp));
   TPM_CUDA(cudaMemcpy(p.twiddle, tw.data(), sizeof(float2) * (nm / 2), cudaMemcpyHostToDevice));
   TPM_CUDA(cudaMemcpy(p.kval, kval.data(), sizeof(float) * nm, cudaMemcpyHostToDevice));
   TPM_CUDA(cudaMemcpy(p.kfilter, kfil.data(), sizeof(float) * nm, cudaMemcpyHostToDevice));
@@ -424,11 +430,11 @@ void pm_solve(const PmPlan& p, cudaStream_t s) {
   k_fft_y<<<dim3(ntx, nm, 1), 256, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
   TPM_LAUNCH_CHECK();
   k_fft_z_poisson<<<dim3(ntx, nm), 256, sm_z, s>>>(p.spec, p.spec3, nm, logn, nh, tx, p.twiddle, p.kval, p.kfilter,
-                                                   p.kderiv, p.kcoef);
+                                                   p.kderiv, p.kcoef, p.ncomp);
   TPM_LAUNCH_CHECK();
-  k_fft_y<<<dim3(ntx, nm, 3), 256, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
+  k_fft_y<<<dim3(ntx, nm, p.ncomp), 256, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
   TPM_LAUNCH_CHECK();
-  k_fft_x_c2r<<<dim3(nblk_x, 3), 256, sm_x, s>>>(p.spec3, p.force, nm, logn, nh, rows, nrows, p.twiddle);
+  k_fft_x_c2r<<<dim3(nblk_x, p.ncomp), 256, sm_x, s>>>(p.spec3, p.force, nm, logn, nh, rows, nrows, p.twiddle);
   TPM_LAUNCH_CHECK();
 }
 

@@ -15,12 +15,14 @@ struct PmPlan {
   float* kval = nullptr;      // per-axis wavenumber k (for k^2)
   float* rho = nullptr;       // nm^3 real, mass per cell
   float2* spec = nullptr;     // nm*nm*nh complex work array
-  float2* spec3 = nullptr;    // 3 x nm*nm*nh
-  float* force = nullptr;     // 3 x nm^3 real, per unit G
+  float2* spec3 = nullptr;    // ncomp x nm*nm*nh
+  float* force = nullptr;     // ncomp x nm^3 real, per unit G: -dphi/dx, -dphi/dy, -dphi/dz [, phi]
+  int ncomp = 3;              // 4 keeps the long-range potential itself (learned short range)
   float kcoef = 0.f;          // -4 pi / V_cell / N^3
 };
 
-// Build tables for mesh nm, box L, split r_s (<= 0: no filter), flags.
+// Build tables for mesh nm, box L, split r_s (<= 0: no filter), flags
+// (bit 1 CIC deconvolution, bit 2 four-point gradient, bit 6 keep phi).
 void pm_plan_init(PmPlan& p, int nm, double box, double r_split, uint32_t flags, int device);
 void pm_plan_free(PmPlan& p);
 

@@ -12,7 +12,9 @@
 #include <vector>
 
 #include "../../include/treepm_b200.h"
+#include "cnn_api.h"
 #include "common.cuh"
+#include "learned.cuh"
 #include "pm.cuh"
 #include "scan.cuh"
 #include "sort.cuh"
@@ -202,7 +204,19 @@ struct tpm_handle {
   int64_t n_int = 0, n_groups = 0;
   TreeParams params_host{};
   tpm_stats stats{};
-  cudaEvent_t ev[8]{};
+  cudaEvent_t ev[10]{};
+  // learned short range (TPM_FLAG_LEARNED)
+  bool learned = false;
+  bool net_attached = false;
+  LearnedNet net{};
+  double m_total = 0.0;
+  __nv_bfloat16* vol_a = nullptr;  // (nm + 6)^3 x 16
+  __nv_bfloat16* vol_b = nullptr;  // (nm + 4)^3 x 16
+  uint8_t* fallback = nullptr;     // per particle: 1 = the tree walk, 0 = the network
+  uint32_t* lgrp_first = nullptr;  // walk groups holding fallback particles
+  uint32_t* lgrp_size = nullptr;
+  uint32_t* lgrp_count = nullptr;
+  unsigned long long* learned_count = nullptr;
   size_t mem_used = 0;
   // every device allocation with its size; `group` 0 = persistent,
   // 1 = sized by the particle capacity, 2 = sized by the octree
@@ -312,6 +326,11 @@ void ensure_capacity(tpm_handle* h, int64_t n) {
   h->sort_bytes = radix_sort_scratch_bytes(c);
   h->sort_scratch = h->alloc<char>(h->sort_bytes, 1);
   h->scan_scratch = h->alloc<char>(scan_scratch_bytes(4 * c + 16), 1);
+  if (h->learned) {
+    h->fallback = h->alloc<uint8_t>(c, 1);
+    h->lgrp_first = h->alloc<uint32_t>(c + 1, 1);
+    h->lgrp_size = h->alloc<uint32_t>(c + 1, 1);
+  }
   h->staging_elems = (size_t)9 * c;  // positions, velocities, accelerations (n x 3 float64 each)
   h->staging = h->alloc<double>(h->staging_elems, 1);
   h->cap = n;
@@ -350,6 +369,18 @@ float ms_between(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+LearnedMesh learned_mesh_of(const tpm_handle* h) {
+  LearnedMesh m{};
+  m.nm = h->pm.nm;
+  m.box = h->cfg.box_size;
+  m.m_cell = h->m_total / ((double)m.nm * m.nm * m.nm);
+  m.rho = h->pm.rho;
+  m.phi = h->pm.force + 3 * (int64_t)m.nm * m.nm * m.nm;
+  m.vol_a = h->vol_a;
+  m.vol_b = h->vol_b;
+  return m;
+}
+
 // One force evaluation of all resident particles.  kick != 0 applies
 // v += a * kick in the gather.
 void force_eval(tpm_handle* h, double eps2, double g, double kick) {
@@ -362,6 +393,8 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
   TPM_CUDA(cudaEventRecord(h->ev[0], s));
   TPM_CUDA(cudaMemsetAsync(h->stats_dev, 0, 8 * sizeof(unsigned long long), s));
   const bool need_tree = !h->pm_only;
+  const bool use_net = need_tree && h->learned && h->net_attached;
+  int64_t walk_groups = 0;
   h->tree_valid = false;
   if (need_tree) {
     // ---- keys and sort
@@ -401,6 +434,25 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
     }
     h->tree_valid = true;
     TPM_CUDA(cudaEventRecord(h->ev[3], s));
+    walk_groups = h->n_groups;
+    if (use_net) {
+      // the network and the dense-cell mask read the mesh: long range first
+      const Particles& P = h->P[h->cur];
+      pm_deposit(h->pm, P.qx, P.qy, P.qz, P.massf, n, s);
+      pm_solve(h->pm, s);
+      TPM_CUDA(cudaEventRecord(h->ev[7], s));
+      const LearnedMesh lm = learned_mesh_of(h);
+      learned_mesh(h->net, lm, T.err, s);
+      TPM_CUDA(cudaMemsetAsync(h->learned_count, 0, sizeof(unsigned long long), s));
+      learned_mask(P.qx, P.qy, P.qz, n, h->net, lm, h->fallback, h->learned_count, s);
+      learned_groups(T.grp_first, T.grp_size, h->n_groups, h->fallback, h->lgrp_first, h->lgrp_size, h->lgrp_count,
+                     s);
+      uint32_t ng = 0;
+      TPM_CUDA(cudaMemcpyAsync(&ng, h->lgrp_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+      walk_groups = ng;
+      TPM_CUDA(cudaEventRecord(h->ev[8], s));
+    }
     // ---- short-range walk
     if (n >= 2) {
       const double scale = box / TWO32;
@@ -415,7 +467,10 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       a.recs = T.recs;
       a.walk = T.o_walk; a.depth = T.o_depth; a.nchild = T.o_nchild; a.child_first = T.o_child_first;
       a.child_ids = T.child_ids; a.o_com = T.o_com; a.leaf_depth = T.leaf_depth;
-      a.gfirst = T.grp_first; a.gsize = T.grp_size; a.ngroups = h->n_groups; a.work = h->work;
+      a.gfirst = use_net ? h->lgrp_first : T.grp_first;
+      a.gsize = use_net ? h->lgrp_size : T.grp_size;
+      a.ngroups = walk_groups;
+      a.work = h->work;
       a.scale = scale; a.box = box; a.rc2 = h->rc2; a.thr = h->thr; a.h0 = h0;
       a.periodic = h->periodic ? 1 : 0;
       a.u_inv = (float)std::ldexp(1.0, -U);
@@ -476,6 +531,10 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       TPM_CUDA(cudaMemsetAsync(h->sry, 0, sizeof(float) * n, s));
       TPM_CUDA(cudaMemsetAsync(h->srz, 0, sizeof(float) * n, s));
     }
+    if (use_net) {
+      const Particles& P = h->P[h->cur];
+      learned_apply(P.qx, P.qy, P.qz, n, h->net, learned_mesh_of(h), h->fallback, h->srx, h->sry, h->srz, s);
+    }
   } else {
     TPM_CUDA(cudaEventRecord(h->ev[1], s));
     TPM_CUDA(cudaEventRecord(h->ev[2], s));
@@ -484,8 +543,10 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
   TPM_CUDA(cudaEventRecord(h->ev[4], s));
   // ---- long range
   const Particles& P = h->P[h->cur];
-  pm_deposit(h->pm, P.qx, P.qy, P.qz, P.massf, n, s);
-  pm_solve(h->pm, s);
+  if (!use_net) {
+    pm_deposit(h->pm, P.qx, P.qy, P.qz, P.massf, n, s);
+    pm_solve(h->pm, s);
+  }
   TPM_CUDA(cudaEventRecord(h->ev[5], s));
   GatherArgs ga{};
   ga.n = n;
@@ -516,8 +577,21 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
   h->stats.ms_bbox_keys = ms_between(h->ev[0], h->ev[1]);
   h->stats.ms_sort = ms_between(h->ev[1], h->ev[2]);
   h->stats.ms_build = ms_between(h->ev[2], h->ev[3]);
-  h->stats.ms_walk = ms_between(h->ev[3], h->ev[4]);
-  h->stats.ms_pm = ms_between(h->ev[4], h->ev[5]);
+  if (use_net) {
+    unsigned long long nl = 0;
+    TPM_CUDA(cudaMemcpy(&nl, h->learned_count, sizeof(nl), cudaMemcpyDeviceToHost));
+    h->stats.learned_particles = (int64_t)nl;
+    h->stats.walk_groups = walk_groups;
+    h->stats.ms_pm = ms_between(h->ev[3], h->ev[7]);
+    h->stats.ms_learned = ms_between(h->ev[7], h->ev[8]);
+    h->stats.ms_walk = ms_between(h->ev[8], h->ev[4]);
+  } else {
+    h->stats.learned_particles = 0;
+    h->stats.walk_groups = walk_groups;
+    h->stats.ms_learned = 0.f;
+    h->stats.ms_walk = ms_between(h->ev[3], h->ev[4]);
+    h->stats.ms_pm = ms_between(h->ev[4], h->ev[5]);
+  }
   h->stats.ms_gather_kick = ms_between(h->ev[5], h->ev[6]);
   h->stats.ms_total = ms_between(h->ev[0], h->ev[6]);
   h->stats.kernel_launches = (int64_t)(g_kernel_launches - launches0);
@@ -533,6 +607,8 @@ void upload(tpm_handle* h, const double* pos, const double* vel, const double* m
   h->n = n;
   h->cur = 0;
   h->forces_valid = false;
+  h->m_total = 0.0;
+  for (int64_t i = 0; i < n; ++i) h->m_total += mass[i];
   if (n == 0) return;
   cudaStream_t s = h->stream;
   double* dpos = h->staging;
@@ -592,6 +668,8 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
     h->thr = 0.1 * std::sqrt(h->rc2);  // short_range.rs:320
     h->periodic = !(cfg->flags & TPM_FLAG_APERIODIC_WALK);
     h->pm_only = (cfg->flags & TPM_FLAG_PM_ONLY) != 0;
+    h->learned = (cfg->flags & TPM_FLAG_LEARNED) != 0;
+    if (h->learned && h->pm_only) throw Error(TPM_ERR_INVALID_ARGUMENT, "the learned short range needs the TreePM solver");
     if (!(h->r_cut > 0.0) || !std::isfinite(h->r_cut)) throw Error(TPM_ERR_INVALID_ARGUMENT, "r_cut must be positive");
     TPM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
@@ -602,6 +680,8 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
     h->T.err = h->alloc<uint32_t>(1, 0);
     h->stats_dev = h->alloc<unsigned long long>(8, 0);
     h->work = h->alloc<uint32_t>(1, 0);
+    h->lgrp_count = h->alloc<uint32_t>(1, 0);
+    h->learned_count = h->alloc<unsigned long long>(1, 0);
     h->ndeferred = h->alloc<uint32_t>(1, 0);
     h->deferred = h->alloc<uint2>(DEFERRED_CAP, 0);
     int sms = prop.multiProcessorCount;
@@ -701,6 +781,8 @@ int tpm_set_particles_fixed(tpm_handle* h, const uint32_t* q, const float* vel, 
     h->n = n;
     h->cur = 0;
     h->forces_valid = false;
+    h->m_total = 0.0;
+    for (int64_t i = 0; i < n; ++i) h->m_total += mass[i];
     cudaStream_t s = h->stream;
     std::vector<uint32_t> tmp((size_t)n);
     Particles& P = h->P[0];
@@ -800,6 +882,86 @@ int tpm_kdk_step_host(tpm_handle* h, double* pos, double* vel, const double* mas
   rc = tpm_kdk_step(h, kick_half, drift, kick_half2, eps2, g);
   if (rc) return rc;
   return tpm_get_state(h, pos, vel, nullptr);
+}
+
+int tpm_set_learned(tpm_handle* h, const tpm_cnn* c) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (!h->learned) throw Error(TPM_ERR_INVALID_ARGUMENT, "the handle was not created with TPM_FLAG_LEARNED");
+    TPM_CUDA(cudaStreamSynchronize(h->stream));
+    h->net_attached = false;
+    h->forces_valid = false;
+    h->release_group(3);
+    if (!c) return TPM_OK;
+    if (c->device != h->cfg.device) throw Error(TPM_ERR_INVALID_ARGUMENT, "network and solver are on different devices");
+    if (c->c_in > cnn::N_FEATURES) throw Error(TPM_ERR_INVALID_ARGUMENT, "the mesh provides 2 input features");
+    TPM_CUDA(cudaStreamSynchronize(c->stream));
+    LearnedNet& net = h->net;
+    net.L = c->L;
+    float* params = h->alloc<float>(c->L.total, 3);
+    TPM_CUDA(cudaMemcpyAsync(params, c->params, sizeof(float) * c->L.total, cudaMemcpyDeviceToDevice, h->stream));
+    uint4* pack = h->alloc<uint4>((size_t)cnn::WPACK_U4 * 5, 3);
+    cnn::Packed P{};
+    for (int l = 0; l < 3; ++l) P.fwd[l] = pack + (size_t)l * cnn::WPACK_U4;
+    P.bwd[1] = pack + (size_t)3 * cnn::WPACK_U4;
+    P.bwd[2] = pack + (size_t)4 * cnn::WPACK_U4;
+    cnn::pack_weights(params, c->L, P, h->stream);
+    net.params = params;
+    for (int l = 0; l < 3; ++l) net.fwd[l] = P.fwd[l];
+    for (int k = 0; k < cnn::MAX_CIN; ++k) {
+      net.shift[k] = c->shift[k];
+      net.scale[k] = c->scale[k];
+    }
+    net.out_scale = c->out_scale;
+    net.delta_max = c->delta_max;
+    const int64_t nm = h->pm.nm;
+    h->vol_a = h->alloc<__nv_bfloat16>((size_t)(nm + 6) * (nm + 6) * (nm + 6) * cnn::CH, 3);
+    h->vol_b = h->alloc<__nv_bfloat16>((size_t)(nm + 4) * (nm + 4) * (nm + 4) * cnn::CH, 3);
+    TPM_CUDA(cudaStreamSynchronize(h->stream));
+    h->net_attached = true;
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_cnn_add_box(tpm_cnn* c, tpm_handle* h, int32_t held_out) {
+  if (!c || !h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (!h->learned) throw Error(TPM_ERR_INVALID_ARGUMENT, "the handle was not created with TPM_FLAG_LEARNED");
+    if (h->net_attached)
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "training targets come from the walk: detach the network first");
+    if (!h->forces_valid) throw Error(TPM_ERR_NOT_READY, "no forces computed");
+    if (c->device != h->cfg.device) throw Error(TPM_ERR_INVALID_ARGUMENT, "network and solver are on different devices");
+    if (c->c_in > cnn::N_FEATURES) throw Error(TPM_ERR_INVALID_ARGUMENT, "the mesh provides 2 input features");
+    TPM_CUDA(cudaStreamSynchronize(h->stream));
+    const Particles& P = h->P[h->cur];
+    cnn::BoxSource b{};
+    b.nm = h->pm.nm;
+    b.box = h->cfg.box_size;
+    b.n = h->n;
+    b.qx = P.qx;
+    b.qy = P.qy;
+    b.qz = P.qz;
+    b.rho = h->pm.rho;
+    b.phi = h->pm.force + 3 * (int64_t)b.nm * b.nm * b.nm;
+    b.srx = h->srx;
+    b.sry = h->sry;
+    b.srz = h->srz;
+    b.lrx = h->lrx;
+    b.lry = h->lry;
+    b.lrz = h->lrz;
+    b.g = h->g_acc;
+    b.m_total = h->m_total;
+    if (!(b.g > 0.0)) throw Error(TPM_ERR_INVALID_ARGUMENT, "the last force evaluation had g <= 0");
+    cnn::add_box(c, b, held_out != 0);
+  } catch (const Error& e) {
+    c->err = e.what();
+    return e.code ? e.code : TPM_ERR_CUDA;
+  }
+  return TPM_OK;
 }
 
 int tpm_get_force_parts(tpm_handle* h, double* acc_lr, double* acc_sr) {

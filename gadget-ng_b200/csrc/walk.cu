@@ -37,7 +37,8 @@ namespace {
 constexpr int WALK_WARPS = 4;
 constexpr int WALK_THREADS = WALK_WARPS * 32;
 constexpr int CHUNK_L = 96;  // leaf-list capacity
-constexpr int CHUNK_M = 96;  // monopole-list capacity
+// monopole-list capacity: the accurate mode also emits monopoles at pop time
+template <bool ACC> constexpr int chunk_m() { return ACC ? 96 : 64; }
 constexpr int32_t WIDE_GROUP = 1 << 28;  // quanta: 1/16 of the box
 
 enum : uint32_t { KIND_LEAF = 0, KIND_MONO = 1 };
@@ -439,7 +440,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     __syncwarp();
     // before the next check the pop adds up to 32 monopole entries (accurate
     // mode) and the next classification up to 32 to either list
-    if (nll > CHUNK_L - 32 || nlm > CHUNK_M - (ACC ? 64 : 32)) {
+    if (nll > CHUNK_L - 32 || nlm > chunk_m<ACC>() - (ACC ? 64 : 32)) {
       flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
       __syncwarp();
       nll = 0;
@@ -580,16 +581,16 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
   }
 }
 
-constexpr size_t WALK_SMEM_PER_WARP = sizeof(Entry) * (CHUNK_L + CHUNK_M) + 32;
+template <bool ACC> constexpr size_t walk_smem_per_warp() { return sizeof(Entry) * (CHUNK_L + chunk_m<ACC>()) + 32; }
 
 template <int MIN_BLOCKS, int TPW, bool ACC>
 __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char s_walk[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned char* mine = s_walk + wid * WALK_SMEM_PER_WARP;
+  unsigned char* mine = s_walk + wid * walk_smem_per_warp<ACC>();
   Entry* list_l = reinterpret_cast<Entry*>(mine);
   Entry* list_m = list_l + CHUNK_L;
-  uint8_t* owner = reinterpret_cast<uint8_t*>(list_m + CHUNK_M);
+  uint8_t* owner = reinterpret_cast<uint8_t*>(list_m + chunk_m<ACC>());
   const int64_t gw = (int64_t)blockIdx.x * WALK_WARPS + wid;
   StackEntry* stk = reinterpret_cast<StackEntry*>(a.stack) + gw * STACK_ENTRIES;
   for (;;) {
@@ -718,7 +719,7 @@ int walk_targets_per_warp() {
 
 template <int B, int T, bool ACC>
 static int blocks_for() {
-  const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
+  const size_t smem = walk_smem_per_warp<ACC>() * WALK_WARPS;
   TPM_CUDA(cudaFuncSetAttribute(k_walk<B, T, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int nb = 0;
   TPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<B, T, ACC>, WALK_THREADS, smem));
@@ -742,11 +743,11 @@ int walk_blocks_per_sm(bool accurate) {
 
 template <int T>
 static void launch_t(const WalkArgs& a, int grid, cudaStream_t s) {
-  const size_t smem = WALK_SMEM_PER_WARP * WALK_WARPS;
   if (a.accurate) {
-    k_walk<5, T, true><<<grid, WALK_THREADS, smem, s>>>(a);
+    k_walk<5, T, true><<<grid, WALK_THREADS, walk_smem_per_warp<true>() * WALK_WARPS, s>>>(a);
     return;
   }
+  const size_t smem = walk_smem_per_warp<false>() * WALK_WARPS;
   switch (walk_blocks_variant()) {
     case 4: k_walk<4, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
     case 6: k_walk<6, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;

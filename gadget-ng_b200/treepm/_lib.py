@@ -31,6 +31,7 @@ FLAG_FOUR_POINT_GRADIENT = 1 << 2
 FLAG_PM_ONLY = 1 << 3
 FLAG_HILBERT_TARGETS = 1 << 4
 FLAG_ACCURATE = 1 << 5
+FLAG_LEARNED = 1 << 6
 
 
 class TpmConfig(C.Structure):
@@ -69,6 +70,9 @@ class TpmStats(C.Structure):
         ("ms_total", C.c_float),
         ("last_error", C.c_int32),
         ("kernel_launches", C.c_int64),
+        ("learned_particles", C.c_int64),
+        ("walk_groups", C.c_int64),
+        ("ms_learned", C.c_float),
     ]
 
     def as_dict(self):
@@ -107,6 +111,22 @@ SIGNATURES = {
     "tpm_fp32_peak": ([_I, C.POINTER(_D)], _I),
     "tpm_ewald": ([_P, _P, _I64, _D, _D, _D, _D, _P, _I64, _D, _D, _I, _I, _P], _I),
     "tpm_hilbert_sort_noalloc": ([_P, _P, _P, _I64, _D, _P, _P, _P], _I),
+    "tpm_cnn_param_count": ([C.c_int32], _I64),
+    "tpm_cnn_create": ([C.c_int32, C.c_int32, C.POINTER(_P)], _I),
+    "tpm_cnn_destroy": ([_P], _I),
+    "tpm_cnn_last_error": ([_P], C.c_char_p),
+    "tpm_cnn_set_params": ([_P, _P, _I64], _I),
+    "tpm_cnn_get_params": ([_P, _P, _I64], _I),
+    "tpm_cnn_set_scales": ([_P, _P, _P, C.c_float, C.c_float], _I),
+    "tpm_cnn_get_scales": ([_P, _P, _P, _P, _P], _I),
+    "tpm_cnn_forward": ([_P, _P, C.c_int32, C.c_int32, _P], _I),
+    "tpm_cnn_loss_grad": ([_P, _P, C.c_int32, C.c_int32, _I64, _P, _P, _P, _P, _P, _P], _I),
+    "tpm_cnn_adam_step": ([_P, _P, C.c_float, C.c_float, C.c_float, C.c_float], _I),
+    "tpm_cnn_add_box": ([_P, _P, C.c_int32], _I),
+    "tpm_cnn_box_count": ([_P, C.c_int32], _I),
+    "tpm_cnn_train": ([_P, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _P], _I),
+    "tpm_cnn_evaluate": ([_P, C.c_int32, C.c_int32, _P], _I),
+    "tpm_set_learned": ([_P, _P], _I),
 }
 NOALLOC_MAX_PARTICLES = 1 << 18
 

@@ -54,15 +54,21 @@ class TreePmSolver:
     the P=1 slab path (default) or the aperiodic walk of the trait-level solver.
     `accurate` selects the extension mode (complete split kernel, geometric
     opening angle `theta`); it is validated against Ewald, not the reference.
+    `learned` keeps the long-range potential on the mesh so that a trained
+    `treepm.learned.Network` can be attached (`set_learned`) to stand in for
+    the walk outside dense cells, or boxes can be captured to train one.
     """
 
     def __init__(self, grid_size: int, box_size: float, r_split: float = 0.0, *, r_cut_factor: float = 5.0,
                  periodic_walk: bool = True, theta: float = 0.5, opening_criterion: int = 0,
                  err_tol_force_acc: float = 0.005, deconvolve_cic: bool = False, four_point_gradient: bool = False,
-                 accurate: bool = False, device: int = 0, memory_cap_bytes: int = 0, _pm_only: bool = False):
+                 accurate: bool = False, learned: bool = False, device: int = 0, memory_cap_bytes: int = 0,
+                 _pm_only: bool = False):
         flags = 0
         if accurate:
             flags |= _lib.FLAG_ACCURATE
+        if learned:
+            flags |= _lib.FLAG_LEARNED
         if not periodic_walk:
             flags |= _lib.FLAG_APERIODIC_WALK
         if deconvolve_cic:
@@ -79,6 +85,10 @@ class TreePmSolver:
         self.box_size = float(box_size)
         self.r_split = float(r_split)
         self._h = _Handle(cfg)
+
+    def set_learned(self, network):
+        """Attach a trained network (a copy is taken); None detaches it."""
+        check(self._h.h, self._h._lib.tpm_set_learned(self._h.h, None if network is None else network.h))
 
     # ---- the GravitySolver call ------------------------------------------
     def accelerations_for_indices(self, global_positions, global_masses, eps2: float, g: float,

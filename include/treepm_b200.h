@@ -75,6 +75,10 @@ enum {
  * never taken as a monopole (theta must lie in (0, 0.577)).  Culls use the
  * node's whole cell. */
 #define TPM_FLAG_ACCURATE           (1u << 5)
+/* Learned short range (extension): keep the long-range potential on the mesh
+ * and, once a network is attached (tpm_set_learned), take the short-range
+ * acceleration from it outside dense cells (see tpm_cnn below). */
+#define TPM_FLAG_LEARNED            (1u << 6)
 
 typedef struct tpm_config {
   int32_t grid_size;          /* [gravity] pm_grid_size (power of two, 8..1024) */
@@ -110,6 +114,9 @@ typedef struct tpm_stats {
   float ms_total;
   int32_t last_error;
   int64_t kernel_launches;      /* kernels launched by the last call that computed forces */
+  int64_t learned_particles;    /* particles whose short range came from the network (TPM_FLAG_LEARNED) */
+  int64_t walk_groups;          /* walk groups walked (all groups, or those holding fallback particles) */
+  float ms_learned;             /* device milliseconds of the network and its mask */
 } tpm_stats;
 
 typedef struct tpm_handle tpm_handle;
@@ -228,6 +235,53 @@ int tpm_ewald(const double* pos, const double* mass, int64_t n, double box, doub
 /* No counterpart in the reference: FFMA throughput of `device` in TFLOP/s, the
  * FP32 roofline denominator of the short-range walk. */
 int tpm_fp32_peak(int device, double* tflops);
+
+/* ---- learned short-range network (extension) --------------------------------
+ * No counterpart in the reference.  A small 3D CNN reads the long-range mesh
+ * (density and potential) and predicts the short-range acceleration at each
+ * particle; a solver created with TPM_FLAG_LEARNED and given a trained network
+ * (tpm_set_learned) uses it instead of the tree walk for particles whose 8
+ * CIC nodes all have overdensity <= delta_max, and walks the tree for the
+ * rest.  Network: three valid 3x3x3 convolutions to 16 channels with GELU
+ * (BF16 on the tensor cores, FP32 accumulation), a linear head 16 -> 3 read
+ * by trilinear interpolation.  Parameters are a flat float32 vector
+ * [W1 (27,16,c_in), b1 (16), W2 (27,16,16), b2, W3 (27,16,16), b3,
+ * Wh (3,16), bh (3)]; tap t = (dz*3 + dy)*3 + dx reads node o + (dx,dy,dz).
+ * Host arrays are copied synchronously. */
+typedef struct tpm_cnn tpm_cnn;
+int64_t tpm_cnn_param_count(int32_t c_in);
+int tpm_cnn_create(int32_t c_in, int32_t device, tpm_cnn** out);
+int tpm_cnn_destroy(tpm_cnn* c);
+const char* tpm_cnn_last_error(const tpm_cnn* c);
+int tpm_cnn_set_params(tpm_cnn* c, const float* params, int64_t n);  /* also resets Adam */
+int tpm_cnn_get_params(tpm_cnn* c, float* params, int64_t n);
+/* Features x = (raw - shift) * scale; raw = (ln(1 + rho/m_cell), phi * cell / m_cell);
+ * the head predicts a / (out_scale * m_cell / cell^2).  Captured boxes set
+ * them from the first box unless set here. */
+int tpm_cnn_set_scales(tpm_cnn* c, const float* shift, const float* scale, float out_scale, float delta_max);
+int tpm_cnn_get_scales(const tpm_cnn* c, float* shift, float* scale, float* out_scale, float* delta_max);
+/* Forward of a batch of volumes x0 [batch][d][d][d][c_in] -> head output
+ * out [batch][d-6][d-6][d-6][3]. */
+int tpm_cnn_forward(tpm_cnn* c, const float* x0, int32_t batch, int32_t d, float* out);
+/* Loss sum_p w_p |pred_p - target_p|^2 / sum w and its gradient; particle p
+ * reads volume pb[p] at node coordinates ps[p] (within [0, d-7]). */
+int tpm_cnn_loss_grad(tpm_cnn* c, const float* x0, int32_t batch, int32_t d, int64_t n, const int32_t* pb,
+                      const float* ps, const float* target, const float* weight, float* loss, float* grad);
+/* One Adam step with `grad` (host; NULL = the last computed gradient). */
+int tpm_cnn_adam_step(tpm_cnn* c, const float* grad, float lr, float beta1, float beta2, float eps);
+/* Capture a training (or held-out) box from a solver handle created with
+ * TPM_FLAG_LEARNED after tpm_compute_forces without a network: the mesh
+ * features and, for particles in cells at or below delta_max, the
+ * short-range acceleration of the walk as the target. */
+int tpm_cnn_add_box(tpm_cnn* c, tpm_handle* solver, int32_t held_out);
+int tpm_cnn_box_count(const tpm_cnn* c, int32_t held_out);
+/* `steps` Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on batches of
+ * `batch` random 14^3 patches of the training boxes; loss per step out. */
+int tpm_cnn_train(tpm_cnn* c, int32_t steps, int32_t batch, float lr, uint64_t seed, float* loss_history);
+/* Weighted loss over a tiling of the held-out (or training) boxes. */
+int tpm_cnn_evaluate(tpm_cnn* c, int32_t held_out, int32_t batch, float* loss);
+/* Give a TPM_FLAG_LEARNED solver a copy of the network (NULL detaches it). */
+int tpm_set_learned(tpm_handle* h, const tpm_cnn* c);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,139 @@
+"""The learned short-range network on the GPU against its CPU restatement.
+
+Forward pass, gradients and Adam are compared with the float64 oracle on the
+same inputs, with the convolution weights and the input rounded to BF16 as the
+tensor cores see them (intermediate activations are BF16 on the device, so
+the tolerances are relative norms of a few 1e-3 per layer).  Then the network
+is trained on boxes the solver generates and must beat the method without it
+on a held-out box.
+"""
+import numpy as np
+import pytest
+
+import cnn_oracle as co
+
+pytestmark = pytest.mark.gpu
+
+
+def _quantised(params, c_in):
+    """Convolution weights rounded to BF16 (biases and head stay FP32)."""
+    parts = co.unflatten(params.astype(np.float64), c_in)
+    for k in (0, 2, 4):
+        parts[k] = co.to_bf16(parts[k])
+    return co.flatten(parts)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def _batch(seed, B=2, D=14, n=400, c_in=2):
+    rng = np.random.default_rng(seed)
+    x0 = rng.normal(size=(B, D, D, D, c_in)).astype(np.float32)
+    pb = rng.integers(0, B, n).astype(np.int32)
+    ps = rng.uniform(0.0, D - 7 - 1e-3, (n, 3)).astype(np.float32)
+    tg = rng.normal(size=(n, 3)).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    return x0, pb, ps, tg, w
+
+
+def _net(seed=0):
+    from treepm import learned
+    return learned.Network(2, params=learned.init_params(2, seed))
+
+
+@pytest.mark.parametrize("D", [7, 12, 21])
+def test_forward_matches_oracle(D):
+    net = _net(1)
+    p = net.params()
+    rng = np.random.default_rng(D)
+    x0 = rng.normal(size=(3, D, D, D, 2)).astype(np.float32)
+    got = net.forward(x0)
+    ref = co.forward(_quantised(p, 2), co.to_bf16(x0))["out"]
+    assert got.shape == ref.shape
+    assert _rel(got, ref) < 2e-2, _rel(got, ref)
+
+
+def test_gradients_match_oracle():
+    net = _net(2)
+    p = net.params()
+    x0, pb, ps, tg, w = _batch(3)
+    loss, grad = net.loss_grad(x0, pb, ps, tg, w)
+    ref_loss, ref_grad = co.loss_and_grads(_quantised(p, 2), co.to_bf16(x0), pb, ps.astype(np.float64), tg, w)
+    assert abs(loss - ref_loss) < 1e-2 * ref_loss
+    parts, refs = co.unflatten(grad, 2), co.unflatten(ref_grad, 2)
+    for k, (g, r) in enumerate(zip(parts, refs)):
+        cos = float(np.dot(g.ravel(), r.ravel()) / (np.linalg.norm(g) * np.linalg.norm(r) + 1e-30))
+        assert _rel(g, r) < 5e-2 and cos > 0.998, (k, _rel(g, r), cos)
+
+
+def test_adam_matches_oracle():
+    net = _net(4)
+    p = net.params().astype(np.float64)
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    rng = np.random.default_rng(5)
+    for step in range(1, 4):
+        g = rng.normal(size=p.shape).astype(np.float32)
+        net.adam_step(g, lr=1e-3)
+        p, m, v = co.adam(p, g.astype(np.float64), m, v, step, lr=1e-3)
+    assert np.max(np.abs(net.params() - p)) < 1e-6
+
+
+def test_invalid_particle_coordinates_are_rejected():
+    from treepm import TreePmError
+    net = _net(0)
+    x0, pb, ps, tg, w = _batch(6, n=10)
+    ps[0, 0] = 7.5  # beyond the last interpolation cell of an 8^3 output
+    with pytest.raises(TreePmError):
+        net.loss_grad(x0, pb, ps, tg, w)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    """A network trained on solver-generated 32^3 boxes (same cell size as the
+    benchmark), with one held-out box."""
+    from treepm import learned
+    net = learned.Network(2, params=learned.init_params(2, 7))
+    boxes = [learned.training_box(300 + k, side=32, box_size=25.0) for k in range(4)]
+    for k, b in enumerate(boxes):
+        learned.capture(net, b, 32, held_out=(k == 3))
+    before = net.evaluate(held_out=True, batch=32)
+    hist = net.train(600, batch=32, lr=2e-3, seed=11)
+    after = net.evaluate(held_out=True, batch=32)
+    return net, boxes[3], before, after, hist
+
+
+def test_training_reduces_held_out_loss(trained):
+    net, _, before, after, hist = trained
+    assert np.all(np.isfinite(hist))
+    assert after < 0.5 * before, (before, after)
+
+
+def test_learned_solver_beats_the_method_without_it(trained):
+    """PM + network (+ walk in dense cells) against the accurate TreePM on the
+    held-out box, next to the same solver whose network predicts zero."""
+    from treepm import learned, ics
+    net, box, _, _, _ = trained
+    phys = ics.physics(box, 32, 1.0)
+    ref_s = learned.solver_for(box, 32)
+    ref_s.set_particles(box.positions(), box.mass)
+    ref_s.compute_forces(phys["eps2"], phys["g"])
+    _, _, ref = ref_s.get_state(box.n, pos=False, vel=False)
+
+    def run(network):
+        s = learned.solver_for(box, 32)
+        s.set_learned(network)
+        s.set_particles(box.positions(), box.mass)
+        s.compute_forces(phys["eps2"], phys["g"])
+        _, _, a = s.get_state(box.n, pos=False, vel=False)
+        st = s.stats()
+        return a, st
+
+    zero = learned.Network(2, params=np.zeros(net.n_params, np.float32))
+    zero.set_scales(*net.scales())
+    a_net, st = run(net)
+    a_zero, st0 = run(zero)
+    assert 0 < st["learned_particles"] < box.n and st["learned_particles"] == st0["learned_particles"]
+    err = lambda a: float(np.sqrt(np.mean(np.sum((a - ref) ** 2, 1) / np.sum(ref ** 2, 1))))
+    assert err(a_net) < 0.7 * err(a_zero), (err(a_net), err(a_zero))
