@@ -212,6 +212,41 @@ def accurate_mode_report(box, mesh, phys, pos, g, targets, ref, device, reps=3):
             "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}}
 
 
+def learned_mode_report(box, mesh, phys, pos, g, targets, ref, device, plain_ms, reps=3):
+    """Speed and Ewald error of the learned short range (network outside
+    dense cells, accurate walk inside them) on the bench's final state."""
+    import treepm
+    from treepm import accuracy, learned
+    path = os.path.join(REPO, "gadget-ng_b200", "treepm", "weights", "learned_sr.npz")
+    if not os.path.exists(path):
+        return {"unavailable": "no trained weights file"}
+    net = learned.Network.load(path, device)
+    s = treepm.TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"], accurate=True,
+                            theta=0.5, deconvolve_cic=True, learned=True, device=device)
+    s.set_learned(net)
+    s.set_particles(pos, box.mass)
+    for _ in range(2):
+        s.compute_forces(phys["eps2"], g)
+    sts = []
+    for _ in range(reps):
+        s.compute_forces(phys["eps2"], g)
+        sts.append(s.stats())
+    _, _, acc = s.get_state(box.n, pos=False, vel=False)
+    rms, p99 = accuracy.relative_errors(acc[targets], ref)
+    s.close()
+    net.close()
+    m = float(np.mean([st["ms_total"] for st in sts]))
+    st = sts[-1]
+    return {"flags": "accurate | deconvolve_cic | learned", "weights": os.path.relpath(path, REPO),
+            "ms_per_force_evaluation": m, "particle_updates_per_s": box.n / (m * 1e-3),
+            "speedup_vs_plain_step": plain_ms / m,
+            "network_fraction": st["learned_particles"] / box.n, "walk_groups": st["walk_groups"],
+            "groups": st["n_groups"],
+            "stage_ms": {k: float(np.mean([x[k] for x in sts])) for k in
+                         ("ms_bbox_keys", "ms_sort", "ms_build", "ms_pm", "ms_learned", "ms_walk", "ms_gather_kick")},
+            "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -269,7 +304,7 @@ def run_b200(args):
     value = world * n * args.steps / (dev_ms * 1e-3)
 
     # ---- force error of the last evaluation against FP64 Ewald ------------
-    ewald = accurate = None
+    ewald = accurate = learned_rep = None
     if rank == 0 and not args.no_ewald:
         from treepm import accuracy
         p_now, _, a_now = solver.get_state(n, pos=True, vel=False, acc=True)
@@ -283,6 +318,7 @@ def run_b200(args):
                  "reference": "FP64 Ewald, Plummer-softened nearest images within r_cut"}
         if not args.no_accurate:
             accurate = accurate_mode_report(box, mesh, phys, p_now, g_last, tg, ref, local)
+            learned_rep = learned_mode_report(box, mesh, phys, p_now, g_last, tg, ref, local, ms_per_step)
 
     # ---- end to end through the host-buffer API (e2e) -------------------
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
@@ -349,6 +385,7 @@ def run_b200(args):
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "force_error_vs_ewald": ewald,
         "accurate_mode": accurate,
+        "learned_mode": learned_rep,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:

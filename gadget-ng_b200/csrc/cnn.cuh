@@ -18,7 +18,7 @@ namespace cnn {
 
 constexpr int CH = 16;                // hidden channels and the padded input width
 constexpr int NOUT = 3;               // head outputs (acceleration components)
-constexpr int MAX_CIN = 8;            // network input channels supported
+constexpr int MAX_CIN = 16;           // network input channels supported
 constexpr int WPACK_U4 = 27 * 32;     // one packed layer: 27 taps x 16 x 16 bf16 = 13,824 bytes
 
 // Offsets of the parts of the flat float32 parameter vector:

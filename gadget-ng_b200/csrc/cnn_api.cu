@@ -13,6 +13,7 @@
 #include "../../include/treepm_b200.h"
 #include "cnn_api.h"
 #include "common.cuh"
+#include "learned.cuh"
 #include "scan.cuh"
 
 using tpm::Error;
@@ -68,12 +69,12 @@ __global__ void k_x0_from_f32(const float* __restrict__ x, int64_t nodes, int c_
 }
 
 // ---- capture of a training box ------------------------------------------------
-__global__ void k_box_feats(const float* __restrict__ rho, const float* __restrict__ phi, int64_t nm3,
-                            float inv_mcell, float cell_over_mcell, int c_in, float* __restrict__ feats) {
+__global__ void k_box_feats(const float* __restrict__ rho, const float* __restrict__ phi,
+                            const float* __restrict__ oct, int64_t nm3, float inv_mcell, float cell_over_mcell,
+                            int c_in, float* __restrict__ feats) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nm3) return;
-  feats[i * c_in + 0] = log1pf(fmaxf(rho[i], 0.f) * inv_mcell);
-  feats[i * c_in + 1] = phi[i] * cell_over_mcell;
+  for (int c = 0; c < c_in; ++c) feats[i * c_in + c] = tpm::raw_feature(c, i, rho, phi, oct, inv_mcell, cell_over_mcell);
 }
 
 struct Capture {
@@ -125,9 +126,10 @@ __global__ void k_box_pass1(Capture c, int32_t* __restrict__ cell_of, uint32_t* 
 }
 
 // Particles into their cells' slots: node coordinates, the weight
-// 1 / (|a|^2 + a_floor^2) (a relative-error loss) and the target.
+// 1 / (|a|^2 + a_floor^2) (a relative-error loss) and the target (units of
+// a_unit).
 __global__ void k_box_pass2(Capture c, const int32_t* __restrict__ cell_of, const uint32_t* __restrict__ start,
-                            uint32_t* __restrict__ cursor, float a_floor2, float wnorm, float inv_out,
+                            uint32_t* __restrict__ cursor, float a_floor2, float wnorm,
                             float4* __restrict__ pdat, float4* __restrict__ ptgt) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= c.n) return;
@@ -143,9 +145,16 @@ __global__ void k_box_pass2(Capture c, const int32_t* __restrict__ cell_of, cons
   const float az = (c.lrz[i] * c.inv_g + c.srz[i]) * c.a_unit_inv;
   const float w = wnorm / (ax * ax + ay * ay + az * az + a_floor2);
   const uint32_t slot = start[lin] + atomicAdd(&cursor[lin], 1u);
+  const float tx = c.srx[i] * c.a_unit_inv, ty = c.sry[i] * c.a_unit_inv, tz = c.srz[i] * c.a_unit_inv;
   pdat[slot] = make_float4(s[0], s[1], s[2], w);
-  ptgt[slot] = make_float4(c.srx[i] * c.a_unit_inv * inv_out, c.sry[i] * c.a_unit_inv * inv_out,
-                           c.srz[i] * c.a_unit_inv * inv_out, 0.f);
+  ptgt[slot] = make_float4(tx, ty, tz, 0.f);
+}
+
+__global__ void k_scale_targets(float4* __restrict__ t, int64_t n, float f) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = t[i];
+  t[i] = make_float4(v.x * f, v.y * f, v.z * f, 0.f);
 }
 
 // ---- batches of patches ------------------------------------------------------------
@@ -358,9 +367,14 @@ void add_box(tpm_cnn* c, const BoxSource& b, bool held_out) {
     return p;
   };
   bx.feats = (float*)balloc(sizeof(float) * nm3 * c->c_in);
-  k_box_feats<<<grid_for(nm3, 256, 1ll << 30), 256, 0, s>>>(b.rho, b.phi, nm3, (float)(1.0 / m_cell),
+  float* oct = nullptr;
+  TPM_CUDA(cudaMalloc(&oct, sizeof(float) * 8 * nm3));
+  octant_deposit(b.qx, b.qy, b.qz, b.massf, b.n, nm, b.box, oct, s);
+  k_box_feats<<<grid_for(nm3, 256, 1ll << 30), 256, 0, s>>>(b.rho, b.phi, oct, nm3, (float)(1.0 / m_cell),
                                                             (float)(cell / m_cell), c->c_in, bx.feats);
   TPM_LAUNCH_CHECK();
+  TPM_CUDA(cudaStreamSynchronize(s));
+  cudaFree(oct);
   // normalisation from the first box
   if (!c->scales_set) {
     std::vector<float> h((size_t)nm3 * c->c_in);
@@ -412,17 +426,38 @@ void add_box(tpm_cnn* c, const BoxSource& b, bool held_out) {
   const double kept = hs[2];
   if (kept < 1) throw Error(TPM_ERR_INVALID_ARGUMENT, "no particle of the box lies in cells below delta_max");
   const double mean_a2 = hs[0] / kept;
-  if (!c->scales_set) {
-    c->out_scale = (float)std::sqrt(std::max(hs[1] / kept, 1e-30));
-    c->scales_set = true;
-  }
   bx.n = (int64_t)kept;
   bx.pdat = (float4*)balloc(sizeof(float4) * bx.n);
   bx.ptgt = (float4*)balloc(sizeof(float4) * bx.n);
   TPM_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (nm3 + 1), s));
   k_box_pass2<<<grid_for(b.n, 256, 1ll << 30), 256, 0, s>>>(cap, cell_of, bx.start, counts,
-                                                            (float)(0.01 * mean_a2), (float)mean_a2,
-                                                            1.f / c->out_scale, bx.pdat, bx.ptgt);
+                                                            (float)(0.01 * mean_a2), (float)mean_a2, bx.pdat,
+                                                            bx.ptgt);
+  TPM_LAUNCH_CHECK();
+  TPM_CUDA(cudaStreamSynchronize(s));
+  // output unit from the first box: the loss-weighted rms of the targets with
+  // the largest 1 % left out (particles whose short and long range nearly
+  // cancel would dominate it), so that predicting zero costs a loss near 1
+  if (!c->scales_set) {
+    std::vector<float4> hp((size_t)bx.n), ht((size_t)bx.n);
+    TPM_CUDA(cudaMemcpy(hp.data(), bx.pdat, sizeof(float4) * bx.n, cudaMemcpyDeviceToHost));
+    TPM_CUDA(cudaMemcpy(ht.data(), bx.ptgt, sizeof(float4) * bx.n, cudaMemcpyDeviceToHost));
+    std::vector<float> t2((size_t)bx.n);
+    for (int64_t i = 0; i < bx.n; ++i) t2[i] = ht[i].x * ht[i].x + ht[i].y * ht[i].y + ht[i].z * ht[i].z;
+    std::vector<float> sorted = t2;
+    const size_t k99 = (size_t)(0.99 * (double)(sorted.size() - 1));
+    std::nth_element(sorted.begin(), sorted.begin() + k99, sorted.end());
+    const float cut = sorted[k99];
+    double sw = 0.0, swt = 0.0;
+    for (int64_t i = 0; i < bx.n; ++i)
+      if (t2[i] <= cut) {
+        sw += hp[i].w;
+        swt += (double)hp[i].w * t2[i];
+      }
+    c->out_scale = (float)std::sqrt(std::max(swt / std::max(sw, 1e-300), 1e-30));
+    c->scales_set = true;
+  }
+  k_scale_targets<<<grid_for(bx.n, 256, 1ll << 30), 256, 0, s>>>(bx.ptgt, bx.n, 1.f / c->out_scale);
   TPM_LAUNCH_CHECK();
   TPM_CUDA(cudaStreamSynchronize(s));
   c->boxes.push_back(bx);

@@ -67,6 +67,7 @@ struct BoxSource {
   double box;
   int64_t n;
   const uint32_t *qx, *qy, *qz;
+  const float* massf;  // particle masses
   const float* rho;  // mass per mesh cell
   const float* phi;  // long-range potential per unit G
   const float *srx, *sry, *srz;  // short-range acceleration per unit G
@@ -76,9 +77,8 @@ struct BoxSource {
 };
 void add_box(tpm_cnn* c, const BoxSource& b, bool held_out);
 
-// Raw (unnormalised) input features of a mesh: ln(1 + rho / m_cell) and
-// phi * cell / m_cell, m_cell the mean mass of a cell.
-constexpr int N_FEATURES = 2;
+// Raw (unnormalised) input features of a mesh: see raw_feature (learned.cuh).
+constexpr int N_FEATURES = 10;
 
 }  // namespace cnn
 }  // namespace tpm

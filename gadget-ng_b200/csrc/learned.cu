@@ -18,28 +18,46 @@ struct Feat {
   float scale[cnn::MAX_CIN];
 };
 
-__global__ void k_mesh_features(const float* __restrict__ rho, const float* __restrict__ phi, int nm,
-                                float inv_mcell, float cell_over_mcell, int c_in, Feat f,
-                                __nv_bfloat16* __restrict__ vol) {
+__global__ void k_mesh_features(const float* __restrict__ rho, const float* __restrict__ phi,
+                                const float* __restrict__ oct, int nm, float inv_mcell, float cell_over_mcell,
+                                int c_in, Feat f, __nv_bfloat16* __restrict__ vol) {
   const int P = nm + 6;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= (int64_t)P * P * P) return;
   const int x = (int)(i % P), y = (int)((i / P) % P), z = (int)(i / ((int64_t)P * P));
   const int mx = (x - 3 + nm) % nm, my = (y - 3 + nm) % nm, mz = (z - 3 + nm) % nm;
   const int64_t node = ((int64_t)mz * nm + my) * nm + mx;
-  const float raw[2] = {log1pf(fmaxf(rho[node], 0.f) * inv_mcell), phi[node] * cell_over_mcell};
+  float v[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c)
+    v[c] = c < c_in ? (raw_feature(c, node, rho, phi, oct, inv_mcell, cell_over_mcell) - f.shift[c]) * f.scale[c]
+                    : 0.f;
   uint32_t w[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const int c0 = 2 * k, c1 = 2 * k + 1;
-    const float v0 = c0 < c_in && c0 < 2 ? (raw[c0] - f.shift[c0]) * f.scale[c0] : 0.f;
-    const float v1 = c1 < c_in && c1 < 2 ? (raw[c1] - f.shift[c1]) * f.scale[c1] : 0.f;
-    __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+    __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
     w[k] = *reinterpret_cast<uint32_t*>(&h);
   }
   uint4* d = reinterpret_cast<uint4*>(vol) + i * 2;
   d[0] = make_uint4(w[0], w[1], w[2], w[3]);
   d[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+__global__ void k_octant_deposit(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                                 const uint32_t* __restrict__ qz, const float* __restrict__ m, int64_t n,
+                                 double scale, double inv_cell, int nm, float* __restrict__ oct) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t q[3] = {qx[i], qy[i], qz[i]};
+  int node[3], bits = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double c = rem_euclid(dmul(decode(q[d], scale), inv_cell), (double)nm) + 0.5;
+    const double f = floor(c);
+    node[d] = ((int)f) % nm;
+    bits |= (c - f >= 0.5 ? 1 : 0) << d;
+  }
+  atomicAdd(&oct[((((int64_t)node[2] * nm + node[1]) * nm + node[0]) << 3) + bits], m[i]);
 }
 
 struct Nodes {
@@ -152,7 +170,7 @@ void learned_mesh(const LearnedNet& net, const LearnedMesh& m, uint32_t* err, cu
     f.scale[k] = net.scale[k];
   }
   const int64_t np = (int64_t)P * P * P;
-  k_mesh_features<<<grid_for(np, 256, 1ll << 30), 256, 0, s>>>(m.rho, m.phi, nm, (float)(1.0 / m.m_cell),
+  k_mesh_features<<<grid_for(np, 256, 1ll << 30), 256, 0, s>>>(m.rho, m.phi, m.octants, nm, (float)(1.0 / m.m_cell),
                                                                (float)(cell / m.m_cell), net.L.c_in, f, m.vol_a);
   TPM_LAUNCH_CHECK();
   cnn::conv_forward(m.vol_a, cnn::Vol{1, P, P, P}, m.vol_b, nullptr, net.fwd[0], net.params + net.L.b[0], err, s);
@@ -160,6 +178,14 @@ void learned_mesh(const LearnedNet& net, const LearnedMesh& m, uint32_t* err, cu
                     net.params + net.L.b[1], err, s);
   cnn::conv_forward(m.vol_a, cnn::Vol{1, P - 4, P - 4, P - 4}, m.vol_b, nullptr, net.fwd[2],
                     net.params + net.L.b[2], err, s);
+}
+
+void octant_deposit(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const float* mass, int64_t n,
+                    int nm, double box, float* oct, cudaStream_t s) {
+  TPM_CUDA(cudaMemsetAsync(oct, 0, sizeof(float) * 8 * (size_t)nm * nm * nm, s));
+  if (n == 0) return;
+  k_octant_deposit<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, mass, n, box / TWO32, nm / box, nm, oct);
+  TPM_LAUNCH_CHECK();
 }
 
 void learned_mask(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, int64_t n, const LearnedNet& net,

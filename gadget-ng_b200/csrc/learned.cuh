@@ -25,9 +25,27 @@ struct LearnedMesh {
   double m_cell;       // mean mass of a cell
   const float* rho;    // mass per cell
   const float* phi;    // long-range potential per unit G
+  float* octants;      // nm^3 x 8: mass in each octant around a node
   __nv_bfloat16* vol_a;  // (nm + 6)^3 x 16
   __nv_bfloat16* vol_b;  // (nm + 4)^3 x 16
 };
+
+// Raw input feature c of mesh node `node`: 0 = ln(1 + rho / m_cell) (CIC),
+// 1 = phi * cell / m_cell, 2..9 = ln(1 + 8 m_oct / m_cell) for the 8 octants
+// of the node's own cell [i - 1/2, i + 1/2)^3 (nearest-node assignment, octant
+// by the sign of the offset: bit 0 x, bit 1 y, bit 2 z).
+constexpr int N_RAW_FEATURES = 10;
+__device__ __forceinline__ float raw_feature(int c, int64_t node, const float* __restrict__ rho,
+                                             const float* __restrict__ phi, const float* __restrict__ oct,
+                                             float inv_mcell, float cell_over_mcell) {
+  if (c == 0) return log1pf(fmaxf(rho[node], 0.f) * inv_mcell);
+  if (c == 1) return phi[node] * cell_over_mcell;
+  return log1pf(8.f * oct[node * 8 + (c - 2)] * inv_mcell);
+}
+
+// Octant masses of every node (zeroed here); positions in fixed point.
+void octant_deposit(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const float* mass, int64_t n,
+                    int nm, double box, float* oct, cudaStream_t s);
 
 // Features of the padded periodic mesh and the three convolutions; the head
 // input (layer-3 activation, nm^3 x 16) ends in vol_b.

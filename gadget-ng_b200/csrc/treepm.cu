@@ -212,6 +212,7 @@ struct tpm_handle {
   double m_total = 0.0;
   __nv_bfloat16* vol_a = nullptr;  // (nm + 6)^3 x 16
   __nv_bfloat16* vol_b = nullptr;  // (nm + 4)^3 x 16
+  float* octants = nullptr;        // nm^3 x 8 octant masses
   uint8_t* fallback = nullptr;     // per particle: 1 = the tree walk, 0 = the network
   uint32_t* lgrp_first = nullptr;  // walk groups holding fallback particles
   uint32_t* lgrp_size = nullptr;
@@ -376,6 +377,7 @@ LearnedMesh learned_mesh_of(const tpm_handle* h) {
   m.m_cell = h->m_total / ((double)m.nm * m.nm * m.nm);
   m.rho = h->pm.rho;
   m.phi = h->pm.force + 3 * (int64_t)m.nm * m.nm * m.nm;
+  m.octants = h->octants;
   m.vol_a = h->vol_a;
   m.vol_b = h->vol_b;
   return m;
@@ -442,6 +444,7 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       pm_solve(h->pm, s);
       TPM_CUDA(cudaEventRecord(h->ev[7], s));
       const LearnedMesh lm = learned_mesh_of(h);
+      octant_deposit(P.qx, P.qy, P.qz, P.massf, n, lm.nm, box, h->octants, s);
       learned_mesh(h->net, lm, T.err, s);
       TPM_CUDA(cudaMemsetAsync(h->learned_count, 0, sizeof(unsigned long long), s));
       learned_mask(P.qx, P.qy, P.qz, n, h->net, lm, h->fallback, h->learned_count, s);
@@ -895,7 +898,7 @@ int tpm_set_learned(tpm_handle* h, const tpm_cnn* c) {
     h->release_group(3);
     if (!c) return TPM_OK;
     if (c->device != h->cfg.device) throw Error(TPM_ERR_INVALID_ARGUMENT, "network and solver are on different devices");
-    if (c->c_in > cnn::N_FEATURES) throw Error(TPM_ERR_INVALID_ARGUMENT, "the mesh provides 2 input features");
+    if (c->c_in > cnn::N_FEATURES) throw Error(TPM_ERR_INVALID_ARGUMENT, "the mesh provides 10 input features");
     TPM_CUDA(cudaStreamSynchronize(c->stream));
     LearnedNet& net = h->net;
     net.L = c->L;
@@ -918,6 +921,7 @@ int tpm_set_learned(tpm_handle* h, const tpm_cnn* c) {
     const int64_t nm = h->pm.nm;
     h->vol_a = h->alloc<__nv_bfloat16>((size_t)(nm + 6) * (nm + 6) * (nm + 6) * cnn::CH, 3);
     h->vol_b = h->alloc<__nv_bfloat16>((size_t)(nm + 4) * (nm + 4) * (nm + 4) * cnn::CH, 3);
+    h->octants = h->alloc<float>((size_t)8 * nm * nm * nm, 3);
     TPM_CUDA(cudaStreamSynchronize(h->stream));
     h->net_attached = true;
   } catch (const Error& e) {
@@ -935,7 +939,7 @@ int tpm_cnn_add_box(tpm_cnn* c, tpm_handle* h, int32_t held_out) {
       throw Error(TPM_ERR_INVALID_ARGUMENT, "training targets come from the walk: detach the network first");
     if (!h->forces_valid) throw Error(TPM_ERR_NOT_READY, "no forces computed");
     if (c->device != h->cfg.device) throw Error(TPM_ERR_INVALID_ARGUMENT, "network and solver are on different devices");
-    if (c->c_in > cnn::N_FEATURES) throw Error(TPM_ERR_INVALID_ARGUMENT, "the mesh provides 2 input features");
+    if (c->c_in > cnn::N_FEATURES) throw Error(TPM_ERR_INVALID_ARGUMENT, "the mesh provides 10 input features");
     TPM_CUDA(cudaStreamSynchronize(h->stream));
     const Particles& P = h->P[h->cur];
     cnn::BoxSource b{};
@@ -945,6 +949,7 @@ int tpm_cnn_add_box(tpm_cnn* c, tpm_handle* h, int32_t held_out) {
     b.qx = P.qx;
     b.qy = P.qy;
     b.qz = P.qz;
+    b.massf = P.massf;
     b.rho = h->pm.rho;
     b.phi = h->pm.force + 3 * (int64_t)b.nm * b.nm * b.nm;
     b.srx = h->srx;

@@ -25,7 +25,7 @@ from . import ics
 from ._lib import TreePmError, load
 from .solver import TreePmSolver
 
-C_IN = 2  # ln(1 + rho / m_cell), phi * cell / m_cell
+C_IN = 10  # ln(1 + rho / m_cell), phi * cell / m_cell, ln(1 + 8 m_octant / m_cell) for 8 octants
 
 
 def _ptr(a):
@@ -92,8 +92,8 @@ class Network:
         self._check(self._lib.tpm_cnn_set_scales(self.h, _ptr(sh), _ptr(sc), float(out_scale), float(delta_max)))
 
     def scales(self):
-        sh = np.zeros(8, dtype=np.float32)
-        sc = np.zeros(8, dtype=np.float32)
+        sh = np.zeros(16, dtype=np.float32)
+        sc = np.zeros(16, dtype=np.float32)
         o = C.c_float()
         d = C.c_float()
         self._check(self._lib.tpm_cnn_get_scales(self.h, _ptr(sh), _ptr(sc), C.byref(o), C.byref(d)))

@@ -42,14 +42,15 @@ def _net(seed=0):
     return learned.Network(2, params=learned.init_params(2, seed))
 
 
-@pytest.mark.parametrize("D", [7, 12, 21])
-def test_forward_matches_oracle(D):
-    net = _net(1)
+@pytest.mark.parametrize("D,c_in", [(7, 2), (12, 2), (21, 2), (12, 10)])
+def test_forward_matches_oracle(D, c_in):
+    from treepm import learned
+    net = learned.Network(c_in, params=learned.init_params(c_in, 1))
     p = net.params()
     rng = np.random.default_rng(D)
-    x0 = rng.normal(size=(3, D, D, D, 2)).astype(np.float32)
+    x0 = rng.normal(size=(3, D, D, D, c_in)).astype(np.float32)
     got = net.forward(x0)
-    ref = co.forward(_quantised(p, 2), co.to_bf16(x0))["out"]
+    ref = co.forward(_quantised(p, c_in), co.to_bf16(x0))["out"]
     assert got.shape == ref.shape
     assert _rel(got, ref) < 2e-2, _rel(got, ref)
 
@@ -91,38 +92,44 @@ def test_invalid_particle_coordinates_are_rejected():
 
 @pytest.fixture(scope="module")
 def trained():
-    """A network trained on solver-generated 32^3 boxes (same cell size as the
-    benchmark), with one held-out box."""
+    """A network trained on solver-generated 64^3 clustered boxes (the
+    benchmark's cell size), with one held-out box."""
     from treepm import learned
-    net = learned.Network(2, params=learned.init_params(2, 7))
-    boxes = [learned.training_box(300 + k, side=32, box_size=25.0) for k in range(4)]
+    net = learned.Network(learned.C_IN, params=learned.init_params(learned.C_IN, 7))
+    boxes = [learned.training_box(300 + k) for k in range(5)]
     for k, b in enumerate(boxes):
-        learned.capture(net, b, 32, held_out=(k == 3))
-    before = net.evaluate(held_out=True, batch=32)
-    hist = net.train(600, batch=32, lr=2e-3, seed=11)
-    after = net.evaluate(held_out=True, batch=32)
-    return net, boxes[3], before, after, hist
+        learned.capture(net, b, 64, held_out=(k == 4))
+    p0 = net.params()
+    net.set_params(np.zeros_like(p0))
+    zero = net.evaluate(held_out=True)  # the loss of predicting no short range
+    net.set_params(p0)
+    hist = net.train(2000, batch=64, lr=1e-3, seed=11)
+    after = net.evaluate(held_out=True)
+    return net, boxes[4], zero, after, hist
 
 
 def test_training_reduces_held_out_loss(trained):
-    net, _, before, after, hist = trained
+    """The held-out loss falls well below that of predicting zero."""
+    net, _, zero, after, hist = trained
     assert np.all(np.isfinite(hist))
-    assert after < 0.5 * before, (before, after)
+    assert after < 0.3 * zero, (zero, after)
 
 
 def test_learned_solver_beats_the_method_without_it(trained):
     """PM + network (+ walk in dense cells) against the accurate TreePM on the
-    held-out box, next to the same solver whose network predicts zero."""
+    held-out box, next to the same solver whose network predicts zero (PM
+    alone outside dense cells).  On a B200 the network brings the rms error
+    from 9 % to 4 % after 4000 steps on 8 boxes."""
     from treepm import learned, ics
     net, box, _, _, _ = trained
-    phys = ics.physics(box, 32, 1.0)
-    ref_s = learned.solver_for(box, 32)
+    phys = ics.physics(box, 64, 1.0)
+    ref_s = learned.solver_for(box, 64)
     ref_s.set_particles(box.positions(), box.mass)
     ref_s.compute_forces(phys["eps2"], phys["g"])
     _, _, ref = ref_s.get_state(box.n, pos=False, vel=False)
 
     def run(network):
-        s = learned.solver_for(box, 32)
+        s = learned.solver_for(box, 64)
         s.set_learned(network)
         s.set_particles(box.positions(), box.mass)
         s.compute_forces(phys["eps2"], phys["g"])
@@ -130,10 +137,10 @@ def test_learned_solver_beats_the_method_without_it(trained):
         st = s.stats()
         return a, st
 
-    zero = learned.Network(2, params=np.zeros(net.n_params, np.float32))
+    zero = learned.Network(learned.C_IN, params=np.zeros(net.n_params, np.float32))
     zero.set_scales(*net.scales())
     a_net, st = run(net)
     a_zero, st0 = run(zero)
     assert 0 < st["learned_particles"] < box.n and st["learned_particles"] == st0["learned_particles"]
     err = lambda a: float(np.sqrt(np.mean(np.sum((a - ref) ** 2, 1) / np.sum(ref ** 2, 1))))
-    assert err(a_net) < 0.7 * err(a_zero), (err(a_net), err(a_zero))
+    assert err(a_net) < 0.6 * err(a_zero), (err(a_net), err(a_zero))
