@@ -29,7 +29,6 @@ using namespace tpm;
 
 namespace {
 
-constexpr int GROUP_MAX = 32;
 constexpr int STACK_CAP = 2048;
 constexpr uint32_t DEFERRED_CAP = 1u << 16;
 

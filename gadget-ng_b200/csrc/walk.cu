@@ -36,17 +36,22 @@ namespace {
 
 constexpr int WALK_WARPS = 4;
 constexpr int WALK_THREADS = WALK_WARPS * 32;
-constexpr int CHUNK_L = 96;  // leaf-list capacity
+constexpr int CHUNK_L = 64;  // leaf-list capacity (small lists leave the L1 to the tree records)
 // monopole-list capacity: the accurate mode also emits monopoles at pop time
 template <bool ACC> constexpr int chunk_m() { return ACC ? 96 : 64; }
 constexpr int32_t WIDE_GROUP = 1 << 28;  // quanta: 1/16 of the box
 
-enum : uint32_t { KIND_LEAF = 0, KIND_MONO = 1 };
 
+// One interaction-list entry (32 bytes): the source position relative to
+// the group's first target in walk units (one rounding of the exact int32
+// difference; the group is compact, so the rounding stays far below the
+// softening length and the float64 band settles every borderline cut), mass,
+// cull half side (0 for periodic leaves), the mask of targets that see it and
+// the node (LEAF_BIT | particle for leaves).
 struct __align__(16) Entry {
-  float hx, hy, hz, m;   // source position (high part, walk units) and mass
-  float lx, ly, lz, h;   // low part, cull half side (0 for periodic leaves)
-  uint32_t mask, node, kind, pad;
+  float x, y, z, m;
+  float h;
+  uint32_t mask, node, pad;
 };
 
 __device__ __forceinline__ int32_t rel32(uint32_t a, uint32_t b, int periodic) {
@@ -56,11 +61,6 @@ __device__ __forceinline__ int32_t rel32(uint32_t a, uint32_t b, int periodic) {
   return (int32_t)d;
 }
 
-// exact float split: v = hi + lo with hi a multiple of 512 (<= 23 significant bits)
-__device__ __forceinline__ void split_rel(int32_t v, float u_inv, float* hi, float* lo) {
-  *hi = (float)(v & ~511) * u_inv;
-  *lo = (float)(v & 511) * u_inv;
-}
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
 #pragma unroll
@@ -183,26 +183,24 @@ struct Acc {
 // aperiodic walk's leaves carry their half side and take the AABB test too).
 // Borderline pairs are left out here and flagged; resolve_list settles them.
 template <bool MONO, int TPW, bool ACC>
-__device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, int nl, int lane, float thx, float thy,
-                                           float thz, float tlx, float tly, float tlz, float& fx, float& fy,
-                                           float& fz, uint32_t& nok, bool& amb_any) {
+__device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, int nl, int lane, float tx, float ty,
+                                           float tz, float& fx, float& fy, float& fz, uint32_t& nok, bool& amb_any) {
   // TPW targets per warp; with 16, lanes t and t + 16 share target t and
   // take alternate entries
   constexpr int STRIDE = 32 / TPW;
   const int t = lane & (TPW - 1);
-#pragma unroll 2
+#pragma unroll 1
   for (int e = lane / TPW; e < nl; e += STRIDE) {
-    const float4 A = *reinterpret_cast<const float4*>(&L[e].hx);
-    const float4 B = *reinterpret_cast<const float4*>(&L[e].lx);
-    const uint32_t mask = L[e].mask;
-    const float dx = (A.x - thx) + (B.x - tlx);
-    const float dy = (A.y - thy) + (B.y - tly);
-    const float dz = (A.z - thz) + (B.z - tlz);
+    const float4 A = *reinterpret_cast<const float4*>(&L[e].x);
+    const uint4 B = *reinterpret_cast<const uint4*>(&L[e].h);
+    const float h = __uint_as_float(B.x);
+    const uint32_t mask = B.y;
+    const float dx = A.x - tx, dy = A.y - ty, dz = A.z - tz;
     const float r2b = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     float s = r2b;
     if (MONO || !a.periodic) {
-      const float ex = fmaxf(fabsf(dx) - B.w, 0.f), ey = fmaxf(fabsf(dy) - B.w, 0.f);
-      const float ez = fmaxf(fabsf(dz) - B.w, 0.f);
+      const float ex = fmaxf(fabsf(dx) - h, 0.f), ey = fmaxf(fabsf(dy) - h, 0.f);
+      const float ez = fmaxf(fabsf(dz) - h, 0.f);
       s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     }
     const bool in = (mask >> t) & 1u;
@@ -224,23 +222,21 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
 
 // Float64 decisions for this lane's borderline pairs of one list (rare).
 template <bool MONO, int TPW>
-__device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float thx,
-                                          float thy, float thz, float tlx, float tly, float tlz, float* f3,
-                                          uint32_t* nok, uint32_t* nexact) {
+__device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float tx,
+                                          float ty, float tz, float* f3, uint32_t* nok, uint32_t* nexact) {
   constexpr int STRIDE = 32 / TPW;
   const int t = lane & (TPW - 1);
   for (int e = lane / TPW; e < nl; e += STRIDE) {
-    const float4 A = *reinterpret_cast<const float4*>(&L[e].hx);
-    const float4 B = *reinterpret_cast<const float4*>(&L[e].lx);
-    const uint32_t mask = L[e].mask, node = L[e].node;
-    const float dx = (A.x - thx) + (B.x - tlx);
-    const float dy = (A.y - thy) + (B.y - tly);
-    const float dz = (A.z - thz) + (B.z - tlz);
+    const float4 A = *reinterpret_cast<const float4*>(&L[e].x);
+    const uint4 B = *reinterpret_cast<const uint4*>(&L[e].h);
+    const float h = __uint_as_float(B.x);
+    const uint32_t mask = B.y, node = B.z;
+    const float dx = A.x - tx, dy = A.y - ty, dz = A.z - tz;
     const float r2b = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     float s = r2b;
     if (MONO || !a.periodic) {
-      const float ex = fmaxf(fabsf(dx) - B.w, 0.f), ey = fmaxf(fabsf(dy) - B.w, 0.f);
-      const float ez = fmaxf(fabsf(dz) - B.w, 0.f);
+      const float ex = fmaxf(fabsf(dx) - h, 0.f), ey = fmaxf(fabsf(dy) - h, 0.f);
+      const float ez = fmaxf(fabsf(dz) - h, 0.f);
       s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     }
     const bool in = (mask >> t) & 1u;
@@ -262,17 +258,16 @@ __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int
 // Evaluate both interaction lists against this lane's target.
 template <int TPW, bool ACC>
 __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nll, const Entry* Lm, int nlm, int lane,
-                                      uint32_t p, float thx, float thy, float thz, float tlx, float tly, float tlz,
-                                      Acc& acc, uint32_t& nleaf, uint32_t& nmono, uint32_t& nexact, uint32_t& neval) {
+                                      uint32_t p, float tx, float ty, float tz, Acc& acc, uint32_t& nleaf, uint32_t& nmono, uint32_t& nexact, uint32_t& neval) {
   float fx = 0.f, fy = 0.f, fz = 0.f;
   bool amb_any = false;
   neval += (uint32_t)(nll + nlm);
-  flush_list<false, TPW, ACC>(a, Ll, nll, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nleaf, amb_any);
-  flush_list<true, TPW, ACC>(a, Lm, nlm, lane, thx, thy, thz, tlx, tly, tlz, fx, fy, fz, nmono, amb_any);
+  flush_list<false, TPW, ACC>(a, Ll, nll, lane, tx, ty, tz, fx, fy, fz, nleaf, amb_any);
+  flush_list<true, TPW, ACC>(a, Lm, nlm, lane, tx, ty, tz, fx, fy, fz, nmono, amb_any);
   if (!ACC && amb_any) {
     float f3[3] = {fx, fy, fz};
-    resolve_list<false, TPW>(a, Ll, nll, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nleaf, &nexact);
-    resolve_list<true, TPW>(a, Lm, nlm, lane, p, thx, thy, thz, tlx, tly, tlz, f3, &nmono, &nexact);
+    resolve_list<false, TPW>(a, Ll, nll, lane, p, tx, ty, tz, f3, &nleaf, &nexact);
+    resolve_list<true, TPW>(a, Lm, nlm, lane, p, tx, ty, tz, f3, &nmono, &nexact);
     fx = f3[0];
     fy = f3[1];
     fz = f3[2];
@@ -306,11 +301,11 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
 #pragma unroll
   for (int d = 0; d < 3; ++d) oq[d] = __shfl_sync(0xffffffffu, tq[d], 0);
   int32_t tr[3];
-  float th[3], tl[3], bmin[3], bmax[3];
+  float tf[3], bmin[3], bmax[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     tr[d] = rel32(tq[d], oq[d], a.periodic);
-    split_rel(tr[d], a.u_inv, &th[d], &tl[d]);
+    tf[d] = (float)tr[d] * a.u_inv;
     int32_t mn = __reduce_min_sync(0xffffffffu, has ? tr[d] : 0x7FFFFFFF);
     int32_t mx = __reduce_max_sync(0xffffffffu, has ? tr[d] : -0x7FFFFFFF);
     bmin[d] = (float)mn * a.u_inv;
@@ -399,16 +394,15 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
           se.ref = r1.z;
         } else {
           emit = true;
-          split_rel(S[0], a.u_inv, &ent.hx, &ent.lx);
-          split_rel(S[1], a.u_inv, &ent.hy, &ent.ly);
-          split_rel(S[2], a.u_inv, &ent.hz, &ent.lz);
+          ent.x = (float)S[0] * a.u_inv;
+          ent.y = (float)S[1] * a.u_inv;
+          ent.z = (float)S[2] * a.u_inv;
           ent.m = __uint_as_float(r0.w);
           ent.h = h;
           // the reference skips the target's own leaf (j != skip)
           const uint32_t own = leaf ? r1.z - first : 32u;
           ent.mask = own < count ? (imask & ~(1u << own)) : imask;
           ent.node = leaf ? (r1.z | LEAF_BIT) : r1.z;
-          ent.kind = leaf ? KIND_LEAF : KIND_MONO;
           is_leaf = leaf;
         }
       }
@@ -420,9 +414,8 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const unsigned lt = (1u << lane) - 1u;
       Entry* dstE = is_leaf ? &Ll[nll + __popc(eml & lt)] : &Lm[nlm + __popc(emm & lt)];
       float4* dst = reinterpret_cast<float4*>(dstE);
-      dst[0] = make_float4(ent.hx, ent.hy, ent.hz, ent.m);
-      dst[1] = make_float4(ent.lx, ent.ly, ent.lz, ent.h);
-      *reinterpret_cast<uint4*>(&dst[2]) = make_uint4(ent.mask, ent.node, ent.kind, 0u);
+      dst[0] = make_float4(ent.x, ent.y, ent.z, ent.m);
+      *reinterpret_cast<uint4*>(&dst[1]) = make_uint4(__float_as_uint(ent.h), ent.mask, ent.node, 0u);
     }
     nll += __popc(eml);
     nlm += __popc(emm);
@@ -441,7 +434,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     // before the next check the pop adds up to 32 monopole entries (accurate
     // mode) and the next classification up to 32 to either list
     if (nll > CHUNK_L - 32 || nlm > chunk_m<ACC>() - (ACC ? 64 : 32)) {
-      flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
+      flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, tf[0], tf[1], tf[2], acc, nleaf, nmono, nexact, neval);
       __syncwarp();
       nll = 0;
       nlm = 0;
@@ -514,14 +507,11 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const uint32_t am = __ballot_sync(0xffffffffu, accept);
       if (am) {  // one monopole entry for the accepting targets (same slot on every lane)
         if (lane == src) {
-          float hx, lx, hy, ly, hz, lz;
-          split_rel(rel32(w.x, oq[0], a.periodic), a.u_inv, &hx, &lx);
-          split_rel(rel32(w.y, oq[1], a.periodic), a.u_inv, &hy, &ly);
-          split_rel(rel32(w.z, oq[2], a.periodic), a.u_inv, &hz, &lz);
           float4* dst = reinterpret_cast<float4*>(&Lm[nlm]);
-          dst[0] = make_float4(hx, hy, hz, __uint_as_float(w.w));
-          dst[1] = make_float4(lx, ly, lz, 2.f * hnode);
-          *reinterpret_cast<uint4*>(&dst[2]) = make_uint4(am, node, KIND_MONO, 0u);
+          dst[0] = make_float4((float)rel32(w.x, oq[0], a.periodic) * a.u_inv,
+                               (float)rel32(w.y, oq[1], a.periodic) * a.u_inv,
+                               (float)rel32(w.z, oq[2], a.periodic) * a.u_inv, __uint_as_float(w.w));
+          *reinterpret_cast<uint4*>(&dst[1]) = make_uint4(__float_as_uint(2.f * hnode), am, node, 0u);
         }
         ++nlm;
       }
@@ -546,7 +536,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     }
   }
   if (nll + nlm > 0) {
-    flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, th[0], th[1], th[2], tl[0], tl[1], tl[2], acc, nleaf, nmono, nexact, neval);
+    flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, tf[0], tf[1], tf[2], acc, nleaf, nmono, nexact, neval);
   }
   __syncwarp();
   if (TPW < 32) {  // fold the two lanes of each target
