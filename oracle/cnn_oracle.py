@@ -97,14 +97,17 @@ def conv_valid_backward(x, w, dz):
     return dx_, dw, flat.sum(0)
 
 
-def forward(params, x0):
+def forward(params, x0, bf16_activations: bool = False):
+    """Forward pass; `bf16_activations` rounds each layer's GELU output to
+    bfloat16 as the device stores it between layers."""
     w1, b1, w2, b2, w3, b3, wh, bh = unflatten(params, x0.shape[-1])
+    act = (lambda z: to_bf16(gelu(z))) if bf16_activations else gelu
     z1 = conv_valid(x0, w1, b1)
-    a1 = gelu(z1)
+    a1 = act(z1)
     z2 = conv_valid(a1, w2, b2)
-    a2 = gelu(z2)
+    a2 = act(z2)
     z3 = conv_valid(a2, w3, b3)
-    a3 = gelu(z3)
+    a3 = act(z3)
     out = a3 @ wh.T + bh
     return dict(z1=z1, a1=a1, z2=z2, a2=a2, z3=z3, a3=a3, out=out)
 

@@ -53,6 +53,23 @@ def test_forward_matches_oracle(D, c_in):
     ref = co.forward(_quantised(p, c_in), co.to_bf16(x0))["out"]
     assert got.shape == ref.shape
     assert _rel(got, ref) < 2e-2, _rel(got, ref)
+    # with the activations rounded to BF16 between layers, as the device stores them
+    ref16 = co.forward(_quantised(p, c_in), co.to_bf16(x0), bf16_activations=True)["out"]
+    assert _rel(got, ref16) < 5e-3, _rel(got, ref16)
+
+
+def test_trained_network_forward_matches_oracle():
+    """The committed network (trained weights amplify rounding more than a
+    random initialisation) against the BF16-activation restatement."""
+    import os
+    from treepm import learned
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gadget-ng_b200", "treepm",
+                        "weights", "learned_sr.npz")
+    net = learned.Network.load(path)
+    x0 = np.random.default_rng(3).normal(size=(2, 10, 10, 10, net.c_in)).astype(np.float32)
+    got = net.forward(x0)
+    ref = co.forward(_quantised(net.params(), net.c_in), co.to_bf16(x0), bf16_activations=True)["out"]
+    assert _rel(got, ref) < 1e-2, _rel(got, ref)
 
 
 def test_gradients_match_oracle():
