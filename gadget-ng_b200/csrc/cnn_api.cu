@@ -85,8 +85,20 @@ struct Capture {
   const float* rho;
   float rho_max;
   const float *srx, *sry, *srz, *lrx, *lry, *lrz;
+  const float *nrx, *nry, *nrz;
   float inv_g, a_unit_inv;
 };
+
+// Target of particle i: the short range minus its exact near-field part.
+__device__ __forceinline__ float3 target_of(const Capture& c, int64_t i) {
+  float3 t = make_float3(c.srx[i], c.sry[i], c.srz[i]);
+  if (c.nrx) {
+    t.x -= c.nrx[i];
+    t.y -= c.nry[i];
+    t.z -= c.nrz[i];
+  }
+  return make_float3(t.x * c.a_unit_inv, t.y * c.a_unit_inv, t.z * c.a_unit_inv);
+}
 
 __device__ __forceinline__ void node_coord(uint32_t q, double scale, double inv_cell, int nm, int* i0, float* s) {
   const double c = tpm::rem_euclid(tpm::dmul(tpm::decode(q, scale), inv_cell), (double)nm);
@@ -119,7 +131,8 @@ __global__ void k_box_pass1(Capture c, int32_t* __restrict__ cell_of, uint32_t* 
   const float ax = (c.lrx[i] * c.inv_g + c.srx[i]) * c.a_unit_inv;
   const float ay = (c.lry[i] * c.inv_g + c.sry[i]) * c.a_unit_inv;
   const float az = (c.lrz[i] * c.inv_g + c.srz[i]) * c.a_unit_inv;
-  const float tx = c.srx[i] * c.a_unit_inv, ty = c.sry[i] * c.a_unit_inv, tz = c.srz[i] * c.a_unit_inv;
+  const float3 t = target_of(c, i);
+  const float tx = t.x, ty = t.y, tz = t.z;
   atomicAdd(&sums[0], (double)(ax * ax + ay * ay + az * az));
   atomicAdd(&sums[1], (double)(tx * tx + ty * ty + tz * tz));
   atomicAdd(&sums[2], 1.0);
@@ -145,7 +158,8 @@ __global__ void k_box_pass2(Capture c, const int32_t* __restrict__ cell_of, cons
   const float az = (c.lrz[i] * c.inv_g + c.srz[i]) * c.a_unit_inv;
   const float w = wnorm / (ax * ax + ay * ay + az * az + a_floor2);
   const uint32_t slot = start[lin] + atomicAdd(&cursor[lin], 1u);
-  const float tx = c.srx[i] * c.a_unit_inv, ty = c.sry[i] * c.a_unit_inv, tz = c.srz[i] * c.a_unit_inv;
+  const float3 t = target_of(c, i);
+  const float tx = t.x, ty = t.y, tz = t.z;
   pdat[slot] = make_float4(s[0], s[1], s[2], w);
   ptgt[slot] = make_float4(tx, ty, tz, 0.f);
 }
@@ -408,6 +422,9 @@ void add_box(tpm_cnn* c, const BoxSource& b, bool held_out) {
   cap.lrx = b.lrx;
   cap.lry = b.lry;
   cap.lrz = b.lrz;
+  cap.nrx = b.nrx;
+  cap.nry = b.nry;
+  cap.nrz = b.nrz;
   cap.inv_g = (float)(1.0 / b.g);
   cap.a_unit_inv = (float)(1.0 / a_unit);
   int32_t* cell_of = (int32_t*)balloc(sizeof(int32_t) * std::max<int64_t>(b.n, 1));
@@ -582,6 +599,18 @@ int tpm_cnn_set_scales(tpm_cnn* c, const float* shift, const float* scale, float
   c->scales_set = true;
   return TPM_OK;
 }
+
+int tpm_cnn_set_near(tpm_cnn* c, float near_cells) {
+  if (!c || !(near_cells >= 0.f && near_cells <= 1.f)) return TPM_ERR_INVALID_ARGUMENT;
+  if (!c->boxes.empty()) {
+    c->err = "the near-field radius defines the captured targets: set it before tpm_cnn_add_box";
+    return TPM_ERR_INVALID_ARGUMENT;
+  }
+  c->near_cells = near_cells;
+  return TPM_OK;
+}
+
+float tpm_cnn_get_near(const tpm_cnn* c) { return c ? c->near_cells : -1.f; }
 
 int tpm_cnn_get_scales(const tpm_cnn* c, float* shift, float* scale, float* out_scale, float* delta_max) {
   if (!c || !shift || !scale || !out_scale || !delta_max) return TPM_ERR_INVALID_ARGUMENT;

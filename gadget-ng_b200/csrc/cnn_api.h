@@ -28,6 +28,7 @@ struct tpm_cnn {
   float scale[tpm::cnn::MAX_CIN] = {};
   float out_scale = 1.f;
   float delta_max = 200.f;
+  float near_cells = 0.f;  // exact near-field radius (cells); the network learns the rest
   bool scales_set = false;
   // batch workspace (volumes of side ws_d, ws_b of them; ws_p particle slots)
   int ws_b = 0, ws_d = 0;
@@ -72,6 +73,7 @@ struct BoxSource {
   const float* phi;  // long-range potential per unit G
   const float *srx, *sry, *srz;  // short-range acceleration per unit G
   const float *lrx, *lry, *lrz;  // long-range acceleration (times g)
+  const float *nrx, *nry, *nrz;  // near-field part of the short range (per unit G), or null
   double g;
   double m_total;
 };

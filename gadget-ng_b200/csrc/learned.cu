@@ -7,8 +7,11 @@
 // walk, run only over the walk groups that hold them.
 #include <cuda_bf16.h>
 
+#include <cmath>
+
 #include "common.cuh"
 #include "learned.cuh"
+#include "scan.cuh"
 
 namespace tpm {
 namespace {
@@ -58,6 +61,67 @@ __global__ void k_octant_deposit(const uint32_t* __restrict__ qx, const uint32_t
     bits |= (c - f >= 0.5 ? 1 : 0) << d;
   }
   atomicAdd(&oct[((((int64_t)node[2] * nm + node[1]) * nm + node[0]) << 3) + bits], m[i]);
+}
+
+__device__ __forceinline__ int cic_cell(uint32_t q, double scale, double inv_cell, int nm) {
+  const double c = rem_euclid(dmul(decode(q, scale), inv_cell), (double)nm);
+  return min((int)floor(c), nm - 1);
+}
+
+__global__ void k_cell_count(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                             const uint32_t* __restrict__ qz, int64_t n, double scale, double inv_cell, int nm,
+                             uint32_t* __restrict__ cell_of, uint32_t* __restrict__ counts) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int x = cic_cell(qx[i], scale, inv_cell, nm), y = cic_cell(qy[i], scale, inv_cell, nm),
+            z = cic_cell(qz[i], scale, inv_cell, nm);
+  const uint32_t c = (uint32_t)(((int64_t)z * nm + y) * nm + x);
+  cell_of[i] = c;
+  atomicAdd(&counts[c], 1u);
+}
+
+__global__ void k_cell_fill(const uint32_t* __restrict__ cell_of, int64_t n, const uint32_t* __restrict__ start,
+                            uint32_t* __restrict__ cursor, uint32_t* __restrict__ items) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t c = cell_of[i];
+  items[start[c] + atomicAdd(&cursor[c], 1u)] = (uint32_t)i;
+}
+
+__global__ void k_near(NearField f, float scale, float r_near2, float inv_s2rs, float eps2) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= f.n || (f.skip && f.skip[i])) return;
+  const int nm = f.nm;
+  const uint32_t c = f.cell_of[i];
+  const int cx = (int)(c % nm), cy = (int)((c / nm) % nm), cz = (int)(c / ((uint32_t)nm * nm));
+  const uint32_t qi[3] = {f.qx[i], f.qy[i], f.qz[i]};
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  for (int d = 0; d < 27; ++d) {
+    const int x = (cx + d % 3 - 1 + nm) % nm, y = (cy + (d / 3) % 3 - 1 + nm) % nm, z = (cz + d / 9 - 1 + nm) % nm;
+    const int64_t nc = ((int64_t)z * nm + y) * nm + x;
+    const uint32_t e = f.start[nc + 1];
+    for (uint32_t k = f.start[nc]; k < e; ++k) {
+      const uint32_t j = f.items[k];
+      if (j == (uint32_t)i) continue;
+      // exact minimum image of the fixed-point difference, then one rounding
+      const float dx = (float)(int32_t)(f.qx[j] - qi[0]) * scale;
+      const float dy = (float)(int32_t)(f.qy[j] - qi[1]) * scale;
+      const float dz = (float)(int32_t)(f.qz[j] - qi[2]) * scale;
+      const float r2b = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (r2b >= r_near2) continue;
+      const float r2 = r2b + eps2;
+      const float r = sqrtf(r2);
+      const float xx = r * inv_s2rs;
+      const float w = erfcf(xx) + 1.1283791670955126f * xx * expf(-xx * xx);
+      const float g = f.mass[j] * w / (r2 * r);
+      ax = fmaf(g, dx, ax);
+      ay = fmaf(g, dy, ay);
+      az = fmaf(g, dz, az);
+    }
+  }
+  f.nx[i] = ax;
+  f.ny[i] = ay;
+  f.nz[i] = az;
 }
 
 struct Nodes {
@@ -123,7 +187,7 @@ __global__ void k_learned_groups(const uint32_t* __restrict__ gfirst, const uint
 __global__ void k_learned_apply(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
                                 const uint32_t* __restrict__ qz, int64_t n, double scale, double inv_cell, int nm,
                                 const uint8_t* __restrict__ fallback, const __nv_bfloat16* __restrict__ a3,
-                                const float* __restrict__ p, int64_t wh, int64_t bh, float out_unit,
+                                const float* __restrict__ p, int64_t wh, int64_t bh, float out_unit, int add,
                                 float* __restrict__ srx, float* __restrict__ sry, float* __restrict__ srz) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n || fallback[i]) return;
@@ -154,9 +218,15 @@ __global__ void k_learned_apply(const uint32_t* __restrict__ qx, const uint32_t*
     for (int k = 0; k < 16; ++k) s = fmaf(p[wh + c * 16 + k], acc[k], s);
     o[c] = s * out_unit;
   }
-  srx[i] = o[0];
-  sry[i] = o[1];
-  srz[i] = o[2];
+  if (add) {
+    srx[i] += o[0];
+    sry[i] += o[1];
+    srz[i] += o[2];
+  } else {
+    srx[i] = o[0];
+    sry[i] = o[1];
+    srz[i] = o[2];
+  }
 }
 
 }  // namespace
@@ -188,6 +258,31 @@ void octant_deposit(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, 
   TPM_LAUNCH_CHECK();
 }
 
+void cell_list(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, int64_t n, int nm, double box,
+               uint32_t* cell_of, uint32_t* cursor, uint32_t* start, uint32_t* items, void* scan_scratch,
+               cudaStream_t s) {
+  const int64_t nm3 = (int64_t)nm * nm * nm;
+  TPM_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * (nm3 + 1), s));
+  if (n > 0) {
+    k_cell_count<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, n, box / TWO32, nm / box, nm, cell_of, cursor);
+    TPM_LAUNCH_CHECK();
+  }
+  exclusive_scan_u32(cursor, start, nm3 + 1, nullptr, scan_scratch, s);
+  TPM_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * (nm3 + 1), s));
+  if (n > 0) {
+    k_cell_fill<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(cell_of, n, start, cursor, items);
+    TPM_LAUNCH_CHECK();
+  }
+}
+
+void near_field(const NearField& f, cudaStream_t s) {
+  if (f.n == 0) return;
+  const float rn = (float)f.r_near;
+  k_near<<<grid_for(f.n, 128, 1ll << 30), 128, 0, s>>>(f, (float)(f.box / TWO32), rn * rn,
+                                                       (float)(1.0 / (std::sqrt(2.0) * f.r_split)), (float)f.eps2);
+  TPM_LAUNCH_CHECK();
+}
+
 void learned_mask(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, int64_t n, const LearnedNet& net,
                   const LearnedMesh& m, uint8_t* fallback, unsigned long long* count, cudaStream_t s) {
   if (n == 0) return;
@@ -214,7 +309,7 @@ void learned_apply(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, i
   const float out_unit = (float)(net.out_scale * m.m_cell / (cell * cell));
   k_learned_apply<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, n, m.box / TWO32, m.nm / m.box, m.nm,
                                                               fallback, m.vol_b, net.params, net.L.wh, net.L.bh,
-                                                              out_unit, srx, sry, srz);
+                                                              out_unit, net.near_cells > 0.f ? 1 : 0, srx, sry, srz);
   TPM_LAUNCH_CHECK();
 }
 

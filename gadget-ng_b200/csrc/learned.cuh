@@ -10,6 +10,7 @@
 namespace tpm {
 
 struct LearnedNet {
+  float near_cells = 0.f;  // radius of the exact near-field sum, in cells (0: none)
   cnn::Layout L{};
   const float* params = nullptr;
   const uint4* fwd[3] = {nullptr, nullptr, nullptr};
@@ -43,6 +44,32 @@ __device__ __forceinline__ float raw_feature(int c, int64_t node, const float* _
   return log1pf(8.f * oct[node * 8 + (c - 2)] * inv_mcell);
 }
 
+// Particles by mesh cell (the CIC cell floor(x nm / L)): per-cell start
+// offsets (nm^3 + 1) and the particle indices; `cell_of` and `cursor` are
+// scratch of n and nm^3 + 1 entries, `scan_scratch` sized by
+// scan_scratch_bytes(nm^3 + 1).
+void cell_list(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, int64_t n, int nm, double box,
+               uint32_t* cell_of, uint32_t* cursor, uint32_t* start, uint32_t* items, void* scan_scratch,
+               cudaStream_t s);
+
+// Exact short-range pairs closer than r_near (complete split kernel, Plummer
+// softened, minimum image): the part of the short range below the mesh
+// scale.  Targets with skip[i] != 0 are left untouched (skip may be null).
+struct NearField {
+  int64_t n;
+  const uint32_t *qx, *qy, *qz;
+  const float* mass;
+  int nm;
+  double box;
+  const uint32_t* cell_of;
+  const uint32_t* start;
+  const uint32_t* items;
+  const uint8_t* skip;
+  double r_near, r_split, eps2;
+  float *nx, *ny, *nz;  // per unit G
+};
+void near_field(const NearField& f, cudaStream_t s);
+
 // Octant masses of every node (zeroed here); positions in fixed point.
 void octant_deposit(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const float* mass, int64_t n,
                     int nm, double box, float* oct, cudaStream_t s);
@@ -60,7 +87,9 @@ void learned_mask(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, in
 void learned_groups(const uint32_t* gfirst, const uint32_t* gsize, int64_t ngroups, const uint8_t* fallback,
                     uint32_t* out_first, uint32_t* out_size, uint32_t* out_count, cudaStream_t s);
 
-// Short-range acceleration per unit G of the particles the network takes.
+// Short-range acceleration per unit G of the particles the network takes:
+// the network's prediction plus the near-field sum already in sr (when the
+// network has a near field) or alone.
 void learned_apply(const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, int64_t n, const LearnedNet& net,
                    const LearnedMesh& m, const uint8_t* fallback, float* srx, float* sry, float* srz,
                    cudaStream_t s);

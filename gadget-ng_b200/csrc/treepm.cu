@@ -217,6 +217,11 @@ struct tpm_handle {
   uint32_t* lgrp_size = nullptr;
   uint32_t* lgrp_count = nullptr;
   unsigned long long* learned_count = nullptr;
+  uint32_t* cell_of = nullptr;     // near field: cell of each particle, particles by cell
+  uint32_t* cell_items = nullptr;
+  uint32_t* cell_start = nullptr;  // nm^3 + 1
+  uint32_t* cell_cursor = nullptr;
+  void* cell_scan = nullptr;
   size_t mem_used = 0;
   // every device allocation with its size; `group` 0 = persistent,
   // 1 = sized by the particle capacity, 2 = sized by the octree
@@ -327,6 +332,8 @@ void ensure_capacity(tpm_handle* h, int64_t n) {
   h->sort_scratch = h->alloc<char>(h->sort_bytes, 1);
   h->scan_scratch = h->alloc<char>(scan_scratch_bytes(4 * c + 16), 1);
   if (h->learned) {
+    h->cell_of = h->alloc<uint32_t>(c, 1);
+    h->cell_items = h->alloc<uint32_t>(c, 1);
     h->fallback = h->alloc<uint8_t>(c, 1);
     h->lgrp_first = h->alloc<uint32_t>(c + 1, 1);
     h->lgrp_size = h->alloc<uint32_t>(c + 1, 1);
@@ -380,6 +387,37 @@ LearnedMesh learned_mesh_of(const tpm_handle* h) {
   m.vol_a = h->vol_a;
   m.vol_b = h->vol_b;
   return m;
+}
+
+// Exact near-field short range (radius near_cells cells, default: the
+// attached network's) of the resident particles into (nx, ny, nz); targets
+// with skip[i] != 0 are left untouched.
+void near_of(tpm_handle* h, double eps2, const uint8_t* skip, float* nx, float* ny, float* nz,
+             float near_cells = -1.f) {
+  const Particles& P = h->P[h->cur];
+  const int nm = h->pm.nm;
+  const double box = h->cfg.box_size;
+  cell_list(P.qx, P.qy, P.qz, h->n, nm, box, h->cell_of, h->cell_cursor, h->cell_start, h->cell_items, h->cell_scan,
+            h->stream);
+  NearField f{};
+  f.n = h->n;
+  f.qx = P.qx;
+  f.qy = P.qy;
+  f.qz = P.qz;
+  f.mass = P.massf;
+  f.nm = nm;
+  f.box = box;
+  f.cell_of = h->cell_of;
+  f.start = h->cell_start;
+  f.items = h->cell_items;
+  f.skip = skip;
+  f.r_near = (near_cells >= 0.f ? near_cells : h->net.near_cells) * box / nm;
+  f.r_split = h->r_s;
+  f.eps2 = eps2;
+  f.nx = nx;
+  f.ny = ny;
+  f.nz = nz;
+  near_field(f, h->stream);
 }
 
 // One force evaluation of all resident particles.  kick != 0 applies
@@ -447,6 +485,9 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       learned_mesh(h->net, lm, T.err, s);
       TPM_CUDA(cudaMemsetAsync(h->learned_count, 0, sizeof(unsigned long long), s));
       learned_mask(P.qx, P.qy, P.qz, n, h->net, lm, h->fallback, h->learned_count, s);
+      if (h->net.near_cells > 0.f) {  // exact pairs below the mesh scale for the network's particles
+        near_of(h, eps2, h->fallback, h->srx, h->sry, h->srz);
+      }
       learned_groups(T.grp_first, T.grp_size, h->n_groups, h->fallback, h->lgrp_first, h->lgrp_size, h->lgrp_count,
                      s);
       uint32_t ng = 0;
@@ -515,6 +556,7 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       a.stack = h->stack; a.stack_cap = STACK_CAP;
       a.single_target = h->r_cut > 0.2 * box ? 1 : 0;
       a.pcounts = h->pcounts;
+      a.only = use_net ? h->fallback : nullptr;
       TPM_CUDA(cudaMemsetAsync(h->work, 0, sizeof(uint32_t), s));
       TPM_CUDA(cudaMemsetAsync(h->ndeferred, 0, sizeof(uint32_t), s));
       launch_walk(a, h->walk_grid, s);
@@ -683,6 +725,12 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
     h->stats_dev = h->alloc<unsigned long long>(8, 0);
     h->work = h->alloc<uint32_t>(1, 0);
     h->lgrp_count = h->alloc<uint32_t>(1, 0);
+    if (h->learned) {
+      const int64_t nm3 = (int64_t)nm * nm * nm;
+      h->cell_start = h->alloc<uint32_t>(nm3 + 1, 0);
+      h->cell_cursor = h->alloc<uint32_t>(nm3 + 1, 0);
+      h->cell_scan = h->alloc<char>(scan_scratch_bytes(nm3 + 1), 0);
+    }
     h->learned_count = h->alloc<unsigned long long>(1, 0);
     h->ndeferred = h->alloc<uint32_t>(1, 0);
     h->deferred = h->alloc<uint2>(DEFERRED_CAP, 0);
@@ -917,6 +965,7 @@ int tpm_set_learned(tpm_handle* h, const tpm_cnn* c) {
     }
     net.out_scale = c->out_scale;
     net.delta_max = c->delta_max;
+    net.near_cells = c->near_cells;
     const int64_t nm = h->pm.nm;
     h->vol_a = h->alloc<__nv_bfloat16>((size_t)(nm + 6) * (nm + 6) * (nm + 6) * cnn::CH, 3);
     h->vol_b = h->alloc<__nv_bfloat16>((size_t)(nm + 4) * (nm + 4) * (nm + 4) * cnn::CH, 3);
@@ -959,8 +1008,26 @@ int tpm_cnn_add_box(tpm_cnn* c, tpm_handle* h, int32_t held_out) {
     b.lrz = h->lrz;
     b.g = h->g_acc;
     b.m_total = h->m_total;
-    if (!(b.g > 0.0)) throw Error(TPM_ERR_INVALID_ARGUMENT, "the last force evaluation had g <= 0");
-    cnn::add_box(c, b, held_out != 0);
+    float* near = nullptr;
+    if (c->near_cells > 0.f) {
+      TPM_CUDA(cudaMalloc(&near, sizeof(float) * 3 * std::max<int64_t>(h->n, 1)));
+      near_of(h, h->eps2_acc, nullptr, near, near + h->n, near + 2 * h->n, c->near_cells);
+      TPM_CUDA(cudaStreamSynchronize(h->stream));
+      b.nrx = near;
+      b.nry = near + h->n;
+      b.nrz = near + 2 * h->n;
+    }
+    if (!(b.g > 0.0)) {
+      cudaFree(near);
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "the last force evaluation had g <= 0");
+    }
+    try {
+      cnn::add_box(c, b, held_out != 0);
+    } catch (...) {
+      cudaFree(near);
+      throw;
+    }
+    cudaFree(near);
   } catch (const Error& e) {
     c->err = e.what();
     return e.code ? e.code : TPM_ERR_CUDA;

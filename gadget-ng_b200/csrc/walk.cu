@@ -294,8 +294,10 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
                              StackEntry* stk) {
   const int lane = threadIdx.x & 31;
   const int tgt = lane & (TPW - 1);  // this lane's target within the group
-  const bool has = (uint32_t)tgt < count;
-  const uint32_t p = first + (has ? (uint32_t)tgt : 0u);
+  const uint32_t p = first + ((uint32_t)tgt < count ? (uint32_t)tgt : 0u);
+  // targets of this walk: the group's particles, or those of them the caller
+  // selected (the group box then covers only those)
+  const bool has = (uint32_t)tgt < count && (!a.only || a.only[p] != 0);
   const uint32_t tq[3] = {a.qx[p], a.qy[p], a.qz[p]};
   uint32_t oq[3];
 #pragma unroll
@@ -311,7 +313,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     bmin[d] = (float)mn * a.u_inv;
     bmax[d] = (float)mx * a.u_inv;
   }
-  const uint32_t mask0 = count >= 32 ? 0xFFFFFFFFu : ((1u << count) - 1u);  // bit t: target t
+  const uint32_t mask0 = __ballot_sync(0xffffffffu, has && lane < TPW);  // bit t: target t
   Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   uint32_t nleaf = 0, nmono = 0, nexact = 0, neval = 0;
   int nll = 0, nlm = 0, sp = 0;

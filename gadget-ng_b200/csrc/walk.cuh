@@ -58,6 +58,7 @@ struct WalkArgs {
   int stack_cap;
   int single_target;     // walk every target alone (r_cut above a quarter box)
   uint32_t* pcounts;     // per target (sorted order): leaf pairs, monopoles
+  const uint8_t* only;   // nullptr, or: walk only the targets p with only[p] != 0
 };
 
 int walk_blocks_per_sm(bool accurate);

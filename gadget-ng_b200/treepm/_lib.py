@@ -119,6 +119,8 @@ SIGNATURES = {
     "tpm_cnn_get_params": ([_P, _P, _I64], _I),
     "tpm_cnn_set_scales": ([_P, _P, _P, C.c_float, C.c_float], _I),
     "tpm_cnn_get_scales": ([_P, _P, _P, _P, _P], _I),
+    "tpm_cnn_set_near": ([_P, C.c_float], _I),
+    "tpm_cnn_get_near": ([_P], C.c_float),
     "tpm_cnn_forward": ([_P, _P, C.c_int32, C.c_int32, _P], _I),
     "tpm_cnn_loss_grad": ([_P, _P, C.c_int32, C.c_int32, _I64, _P, _P, _P, _P, _P, _P], _I),
     "tpm_cnn_adam_step": ([_P, _P, C.c_float, C.c_float, C.c_float, C.c_float], _I),

@@ -1,7 +1,9 @@
 """Learned short-range network (extension; no counterpart in the reference).
 
 A small 3D CNN maps the long-range mesh (density and potential) to the
-short-range acceleration at each particle.  A solver created with
+short-range acceleration at each particle (optionally less the pairs closer
+than `near_cells` cells, which the solver then sums exactly over the
+neighbouring cells).  A solver created with
 `learned=True` and given a trained `Network` (`TreePmSolver.set_learned`)
 takes the short range from it for particles whose 8 CIC nodes all have
 overdensity <= `delta_max`, and walks the tree only for the rest.
@@ -91,6 +93,13 @@ class Network:
         sc = np.ascontiguousarray(scale, dtype=np.float32)
         self._check(self._lib.tpm_cnn_set_scales(self.h, _ptr(sh), _ptr(sc), float(out_scale), float(delta_max)))
 
+    def set_near(self, near_cells: float):
+        """Radius (cells) of the exact near-field sum the network complements."""
+        self._check(self._lib.tpm_cnn_set_near(self.h, float(near_cells)))
+
+    def near(self) -> float:
+        return float(self._lib.tpm_cnn_get_near(self.h))
+
     def scales(self):
         sh = np.zeros(16, dtype=np.float32)
         sc = np.zeros(16, dtype=np.float32)
@@ -144,12 +153,13 @@ class Network:
     def save(self, path: str):
         sh, sc, o, d = self.scales()
         np.savez(path, params=self.params(), shift=sh, scale=sc, out_scale=np.float32(o), delta_max=np.float32(d),
-                 c_in=np.int32(self.c_in))
+                 c_in=np.int32(self.c_in), near_cells=np.float32(self.near()))
 
     @classmethod
     def load(cls, path: str, device: int = 0) -> "Network":
         z = np.load(path)
         net = cls(int(z["c_in"]), device, params=z["params"])
+        net.set_near(float(z["near_cells"]) if "near_cells" in z else 0.0)
         net.set_scales(z["shift"], z["scale"], float(z["out_scale"]), float(z["delta_max"]))
         return net
 
@@ -162,11 +172,13 @@ def training_box(seed: int, side: int = 64, box_size: float = 50.0) -> ics.Box:
                              name=f"train{side}_s{seed}")
 
 
-def solver_for(box: ics.Box, mesh: int, device: int = 0) -> TreePmSolver:
-    """The solver configuration the network is trained for and used with."""
+def solver_for(box: ics.Box, mesh: int, device: int = 0, theta: float = 0.5) -> TreePmSolver:
+    """The solver configuration the network is trained for and used with
+    (training targets with opening angle 0.5; the fallback walk of the
+    learned solver may use a wider one)."""
     phys = ics.physics(box, mesh, 1.0)
     return TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"], accurate=True,
-                        theta=0.5, deconvolve_cic=True, learned=True, device=device)
+                        theta=theta, deconvolve_cic=True, learned=True, device=device)
 
 
 def capture(net: Network, box: ics.Box, mesh: int, held_out: bool = False, device: int = 0):

@@ -27,8 +27,9 @@ DEFAULT_OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights"
 
 
 def train(n_train=24, n_held=4, steps=(6000, 3000, 1500), lrs=(1e-3, 3e-4, 1e-4), batch=64, seed=7,
-          delta_max=200.0, c_in=learned.C_IN, log=print):
+          delta_max=200.0, c_in=learned.C_IN, near_cells=0.0, log=print):
     net = learned.Network(c_in, params=learned.init_params(c_in, seed))
+    net.set_near(near_cells)
     t0 = time.time()
     for k in range(n_train):
         learned.capture(net, learned.training_box(1000 + k), 64)
@@ -59,8 +60,10 @@ def main():
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--channels", type=int, default=learned.C_IN, help="input features (2: density and potential)")
+    ap.add_argument("--near", type=float, default=0.0, help="exact near-field radius in cells (0: network alone)")
     args = ap.parse_args()
-    net = train(args.boxes, args.held_out, tuple(args.steps), batch=args.batch, seed=args.seed, c_in=args.channels)
+    net = train(args.boxes, args.held_out, tuple(args.steps), batch=args.batch, seed=args.seed, c_in=args.channels,
+                near_cells=args.near)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     net.save(args.out)
     print(json.dumps({"saved": args.out}))

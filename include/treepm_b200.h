@@ -260,6 +260,12 @@ int tpm_cnn_get_params(tpm_cnn* c, float* params, int64_t n);
  * them from the first box unless set here. */
 int tpm_cnn_set_scales(tpm_cnn* c, const float* shift, const float* scale, float out_scale, float delta_max);
 int tpm_cnn_get_scales(const tpm_cnn* c, float* shift, float* scale, float* out_scale, float* delta_max);
+/* Radius (in mesh cells, 0..1; default 0) of the exact near-field pair sum the
+ * network is combined with: the network predicts the short range minus the
+ * pairs closer than this, which the solver sums directly over the 27
+ * neighbouring cells.  Set before capturing boxes; 0 = the network alone. */
+int tpm_cnn_set_near(tpm_cnn* c, float near_cells);
+float tpm_cnn_get_near(const tpm_cnn* c);
 /* Forward of a batch of volumes x0 [batch][d][d][d][c_in] -> head output
  * out [batch][d-6][d-6][d-6][3]. */
 int tpm_cnn_forward(tpm_cnn* c, const float* x0, int32_t batch, int32_t d, float* out);
