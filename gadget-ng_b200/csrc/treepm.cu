@@ -58,6 +58,34 @@ __global__ void k_encode(const double* __restrict__ pos, const double* __restric
   p.id[i] = (uint32_t)i;
 }
 
+// Does the staged host state (positions, velocities, masses by original
+// index) equal the resident state?  Clears *same on any difference.
+__global__ void k_match_state(const double* __restrict__ pos, const double* __restrict__ vel,
+                              const double* __restrict__ mass, int64_t n, double box, Particles p,
+                              uint32_t* __restrict__ same) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t o = p.id[i];
+  bool eq = mass[o] == p.mass[i];
+  const uint32_t q[3] = {p.qx[i], p.qy[i], p.qz[i]};
+  const float v[3] = {p.vx[i], p.vy[i], p.vz[i]};
+  for (int d = 0; d < 3; ++d) {
+    double u = pos[3 * o + d] / box;
+    u = u - floor(u);
+    eq = eq && (uint32_t)((unsigned long long)llrint(u * TWO32) & 0xFFFFFFFFull) == q[d];
+    eq = eq && (vel ? (float)vel[3 * o + d] : 0.f) == v[d];
+  }
+  if (!eq) atomicAnd(same, 0u);
+}
+
+__global__ void k_sum_mass(const double* __restrict__ m, int64_t n, double* __restrict__ out) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s += m[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
 __global__ void k_decode_state(Particles p, int64_t n, double scale, const float* ax, const float* ay,
                                const float* az, double* pos, double* vel, double* acc) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -208,7 +236,8 @@ struct tpm_handle {
   bool learned = false;
   bool net_attached = false;
   LearnedNet net{};
-  double m_total = 0.0;
+  double m_total = 0.0;      // total mass (learned path), summed on the device when first needed
+  bool m_total_valid = false;
   __nv_bfloat16* vol_a = nullptr;  // (nm + 6)^3 x 16
   __nv_bfloat16* vol_b = nullptr;  // (nm + 4)^3 x 16
   float* octants = nullptr;        // nm^3 x 8 octant masses
@@ -338,7 +367,7 @@ void ensure_capacity(tpm_handle* h, int64_t n) {
     h->lgrp_first = h->alloc<uint32_t>(c + 1, 1);
     h->lgrp_size = h->alloc<uint32_t>(c + 1, 1);
   }
-  h->staging_elems = (size_t)9 * c;  // positions, velocities, accelerations (n x 3 float64 each)
+  h->staging_elems = (size_t)9 * c + 1;  // positions, velocities, accelerations (n x 3 float64 each), a scratch word
   h->staging = h->alloc<double>(h->staging_elems, 1);
   h->cap = n;
 }
@@ -376,11 +405,24 @@ float ms_between(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
-LearnedMesh learned_mesh_of(const tpm_handle* h) {
+double total_mass(tpm_handle* h) {
+  if (!h->m_total_valid) {
+    double* d = h->staging + h->staging_elems - 1;  // a scratch word at the end of the staging buffer
+    TPM_CUDA(cudaMemsetAsync(d, 0, sizeof(double), h->stream));
+    k_sum_mass<<<grid_for(h->n, 256, 148 * 8), 256, 0, h->stream>>>(h->P[h->cur].mass, h->n, d);
+    TPM_LAUNCH_CHECK();
+    TPM_CUDA(cudaMemcpyAsync(&h->m_total, d, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TPM_CUDA(cudaStreamSynchronize(h->stream));
+    h->m_total_valid = true;
+  }
+  return h->m_total;
+}
+
+LearnedMesh learned_mesh_of(tpm_handle* h) {
   LearnedMesh m{};
   m.nm = h->pm.nm;
   m.box = h->cfg.box_size;
-  m.m_cell = h->m_total / ((double)m.nm * m.nm * m.nm);
+  m.m_cell = total_mass(h) / ((double)m.nm * m.nm * m.nm);
   m.rho = h->pm.rho;
   m.phi = h->pm.force + 3 * (int64_t)m.nm * m.nm * m.nm;
   m.octants = h->octants;
@@ -639,6 +681,7 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
   h->stats.ms_gather_kick = ms_between(h->ev[5], h->ev[6]);
   h->stats.ms_total = ms_between(h->ev[0], h->ev[6]);
   h->stats.kernel_launches = (int64_t)(g_kernel_launches - launches0);
+  h->stats.force_evaluations += 1;
   h->forces_valid = true;
   h->g_acc = g;
   h->eps2_acc = eps2;
@@ -651,8 +694,7 @@ void upload(tpm_handle* h, const double* pos, const double* vel, const double* m
   h->n = n;
   h->cur = 0;
   h->forces_valid = false;
-  h->m_total = 0.0;
-  for (int64_t i = 0; i < n; ++i) h->m_total += mass[i];
+  h->m_total_valid = false;
   if (n == 0) return;
   cudaStream_t s = h->stream;
   double* dpos = h->staging;
@@ -831,8 +873,7 @@ int tpm_set_particles_fixed(tpm_handle* h, const uint32_t* q, const float* vel, 
     h->n = n;
     h->cur = 0;
     h->forces_valid = false;
-    h->m_total = 0.0;
-    for (int64_t i = 0; i < n; ++i) h->m_total += mass[i];
+    h->m_total_valid = false;
     cudaStream_t s = h->stream;
     std::vector<uint32_t> tmp((size_t)n);
     Particles& P = h->P[0];
@@ -927,7 +968,37 @@ int tpm_get_state(tpm_handle* h, double* pos, double* vel, double* acc) {
 int tpm_kdk_step_host(tpm_handle* h, double* pos, double* vel, const double* mass, int64_t n, double kick_half,
                       double drift, double kick_half2, double eps2, double g) {
   if (!h) return TPM_ERR_INVALID_ARGUMENT;
-  int rc = tpm_set_particles(h, pos, vel, mass, n);
+  // The integrator hands back the state the previous call returned: after
+  // copying this step's inputs, compare them with the resident state on the
+  // device; when they are the same, the resident closing acceleration is the
+  // opening one (as in the device-resident loop) and one force evaluation
+  // is saved.  Any difference re-encodes the inputs and evaluates twice.
+  bool resident = false;
+  if (h->forces_valid && n == h->n && n > 0 && pos && mass && h->eps2_acc == eps2 && h->g_acc != 0.0) {
+    try {
+      TPM_CUDA(cudaSetDevice(h->cfg.device));
+      cudaStream_t s = h->stream;
+      double* dpos = h->staging;
+      double* dmass = h->staging + 3 * n;
+      double* dvel = vel ? h->staging + 4 * n : nullptr;
+      uint32_t* same = reinterpret_cast<uint32_t*>(h->staging + h->staging_elems - 1);
+      TPM_CUDA(cudaMemcpyAsync(dpos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+      TPM_CUDA(cudaMemcpyAsync(dmass, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+      if (vel) TPM_CUDA(cudaMemcpyAsync(dvel, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+      const uint32_t one = 1u;
+      TPM_CUDA(cudaMemcpyAsync(same, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+      k_match_state<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(dpos, dvel, dmass, n, h->cfg.box_size, h->P[h->cur],
+                                                                same);
+      TPM_LAUNCH_CHECK();
+      uint32_t flag = 0;
+      TPM_CUDA(cudaMemcpyAsync(&flag, same, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaStreamSynchronize(s));
+      resident = flag != 0;
+    } catch (const Error& e) {
+      return fail(h, e);
+    }
+  }
+  int rc = resident ? TPM_OK : tpm_set_particles(h, pos, vel, mass, n);
   if (rc) return rc;
   rc = tpm_kdk_step(h, kick_half, drift, kick_half2, eps2, g);
   if (rc) return rc;
@@ -1007,7 +1078,7 @@ int tpm_cnn_add_box(tpm_cnn* c, tpm_handle* h, int32_t held_out) {
     b.lry = h->lry;
     b.lrz = h->lrz;
     b.g = h->g_acc;
-    b.m_total = h->m_total;
+    b.m_total = total_mass(h);
     float* near = nullptr;
     if (c->near_cells > 0.f) {
       TPM_CUDA(cudaMalloc(&near, sizeof(float) * 3 * std::max<int64_t>(h->n, 1)));

@@ -73,6 +73,7 @@ class TpmStats(C.Structure):
         ("learned_particles", C.c_int64),
         ("walk_groups", C.c_int64),
         ("ms_learned", C.c_float),
+        ("force_evaluations", C.c_int64),
     ]
 
     def as_dict(self):

@@ -117,6 +117,7 @@ typedef struct tpm_stats {
   int64_t learned_particles;    /* particles whose short range came from the network (TPM_FLAG_LEARNED) */
   int64_t walk_groups;          /* walk groups walked (all groups, or those holding fallback particles) */
   float ms_learned;             /* device milliseconds of the network and its mask */
+  int64_t force_evaluations;    /* force evaluations since the handle was created */
 } tpm_stats;
 
 typedef struct tpm_handle tpm_handle;
@@ -156,7 +157,11 @@ int tpm_compute_forces(tpm_handle* h, double eps2, double g);
  * when eps2 changed or no acceleration is cached. */
 int tpm_kdk_step(tpm_handle* h, double kick_half, double drift, double kick_half2, double eps2, double g);
 /* Host KDK step: state in host buffers (n x 3 float64 pos / vel), copied to
- * the device, advanced by tpm_kdk_step, copied back (original order). */
+ * the device, advanced by tpm_kdk_step, copied back (original order).  When
+ * the inputs equal the resident state (the caller hands back what the
+ * previous call returned; checked on the device after the copy), the
+ * resident closing acceleration opens the step and one force evaluation is
+ * made; otherwise the inputs are re-encoded and the step evaluates twice. */
 int tpm_kdk_step_host(tpm_handle* h, double* pos, double* vel, const double* mass, int64_t n, double kick_half,
                       double drift, double kick_half2, double eps2, double g);
 /* Read back state in the original particle order (any pointer may be NULL). */

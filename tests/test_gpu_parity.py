@@ -294,3 +294,53 @@ def test_drift_kick_factors_match_oracle_bitwise():
     t = treepm()
     for a0, dt in ((0.02, 0.001), (0.1, 0.0037), (1.0, 0.05)):
         assert t.drift_kick_factors(0.31, 0.69, 1.0, a0, dt) == oracle().drift_kick_factors(0.31, 0.69, 1.0, a0, dt)
+
+
+def test_host_kdk_steps_reuse_the_resident_acceleration():
+    """Host-buffer steps that hand back the returned state reuse the resident
+    closing acceleration: three such steps equal three device-resident steps,
+    with one force evaluation per step after the first; a changed state is
+    re-encoded and evaluated twice."""
+    t = treepm()
+    from treepm import ics
+    b = small_box(16, 100.0, 1.0, 83)
+    nm = 16
+    phys = ics.physics(b, nm, 0.1)
+    a = 0.1
+    steps = []
+    for _ in range(3):
+        dt = ics.time_between(a, a + 0.002)
+        steps.append(t.drift_kick_factors(ics.OMEGA_M, ics.OMEGA_L, 1.0, a, dt))
+        a += 0.002
+    dev = t.TreePmSolver(nm, b.box_size, phys["r_split"], r_cut_factor=4.5)
+    dev.set_particles(b.positions(), b.mass)
+    for d, k1, k2 in steps:
+        dev.kdk_step(k1, d, k2, phys["eps2"], phys["g"])
+    p_dev, v_dev, _ = dev.get_state(b.n)
+    host = t.TreePmSolver(nm, b.box_size, phys["r_split"], r_cut_factor=4.5)
+    pos = np.ascontiguousarray(b.positions())
+    vel = np.zeros_like(pos)
+    evals = []
+    for d, k1, k2 in steps:
+        host.kdk_step_host(pos, vel, b.mass, k1, d, k2, phys["eps2"], phys["g"])
+        evals.append(host.stats()["force_evaluations"])
+    assert evals == [2, 3, 4], evals
+    # the same steps as on the device (float atomics of the deposit make the
+    # two runs differ in the last bits only)
+    assert rel_err(vel, v_dev)[0] < 1e-5
+    dp = (pos - p_dev + 0.5 * b.box_size) % b.box_size - 0.5 * b.box_size
+    assert np.max(np.abs(dp)) < 1e-6 * b.box_size
+    # a perturbed state is not the resident one: the step evaluates twice and
+    # still matches a device step from the same state
+    pos2 = pos.copy()
+    pos2[0, 0] = (pos2[0, 0] + 1e-3) % b.box_size
+    ref = t.TreePmSolver(nm, b.box_size, phys["r_split"], r_cut_factor=4.5)
+    ref.set_particles(pos2, b.mass, vel)
+    d, k1, k2 = steps[0]
+    ref.kdk_step(k1, d, k2, phys["eps2"], phys["g"])
+    p_ref, v_ref, _ = ref.get_state(b.n)
+    host.kdk_step_host(pos2, vel, b.mass, k1, d, k2, phys["eps2"], phys["g"])
+    assert host.stats()["force_evaluations"] == 6
+    assert rel_err(vel, v_ref)[0] < 1e-5
+    dp = (pos2 - p_ref + 0.5 * b.box_size) % b.box_size - 0.5 * b.box_size
+    assert np.max(np.abs(dp)) < 1e-6 * b.box_size
