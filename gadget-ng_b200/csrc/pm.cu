@@ -110,21 +110,70 @@ __device__ __forceinline__ Cic cic_of(uint32_t qx, uint32_t qy, uint32_t qz, dou
   return c;
 }
 
+// The particles arrive in octree order, so lanes of a warp often share a
+// CIC cell (in a Plummer core, hundreds of particles share one).  Lanes with
+// the same base cell (hence the same 8 nodes) are grouped with match_any; the
+// group's first lane sums their 8 weighted masses through shuffles and issues
+// the 8 atomics for all of them.  The cell index and the weights are the
+// reference's (float64 position arithmetic, product m wx wy wz).
 __global__ void k_deposit(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
                           const uint32_t* __restrict__ qz, const float* __restrict__ m, int64_t n, double scale,
                           double inv_cell, int nm, float* __restrict__ rho) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const Cic c = cic_of(qx[i], qy[i], qz[i], scale, inv_cell, nm);
-  const float mi = m[i];
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool live = i < n;
+  Cic c{};
+  float mi = 0.f;
+  uint32_t key = 0xFFFFFFFFu;
+  if (live) {
+    c = cic_of(qx[i], qy[i], qz[i], scale, inv_cell, nm);
+    mi = m[i];
+    key = (uint32_t)(((int64_t)c.iz[0] * nm + c.iy[0]) * nm + c.ix[0]);
+  }
+  const uint32_t peers = __match_any_sync(0xffffffffu, key);
+  const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
   const int64_t nm2 = (int64_t)nm * nm;
+  if (rounds == 1) {  // no two lanes share a cell
+    if (!live) return;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int d = 0; d < 2; ++d)
+          atomicAdd(&rho[c.iz[a] * nm2 + (int64_t)c.iy[b] * nm + c.ix[d]], mi * c.wx[d] * c.wy[b] * c.wz[a]);
+    return;
+  }
+  float sum[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) sum[k] = 0.f;
+  uint32_t rest = peers;
+  for (int r = 0; r < rounds; ++r) {  // the same count on every lane: full-warp shuffles
+    const int src = rest ? __ffs(rest) - 1 : lane;
+    const bool take = rest != 0u;
+    rest &= rest - 1u;
+    const float sm = __shfl_sync(0xffffffffu, mi, src);
+    const float x0 = __shfl_sync(0xffffffffu, c.wx[0], src), x1 = __shfl_sync(0xffffffffu, c.wx[1], src);
+    const float y0 = __shfl_sync(0xffffffffu, c.wy[0], src), y1 = __shfl_sync(0xffffffffu, c.wy[1], src);
+    const float z0 = __shfl_sync(0xffffffffu, c.wz[0], src), z1 = __shfl_sync(0xffffffffu, c.wz[1], src);
+    if (take) {
+      sum[0] += sm * x0 * y0 * z0;
+      sum[1] += sm * x1 * y0 * z0;
+      sum[2] += sm * x0 * y1 * z0;
+      sum[3] += sm * x1 * y1 * z0;
+      sum[4] += sm * x0 * y0 * z1;
+      sum[5] += sm * x1 * y0 * z1;
+      sum[6] += sm * x0 * y1 * z1;
+      sum[7] += sm * x1 * y1 * z1;
+    }
+  }
+  if (!live || lane != __ffs(peers) - 1) return;
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
-      for (int d = 0; d < 2; ++d)
-        atomicAdd(&rho[c.iz[a] * nm2 + (int64_t)c.iy[b] * nm + c.ix[d]], mi * c.wx[d] * c.wy[b] * c.wz[a]);
+      for (int d = 0; d < 2; ++d) atomicAdd(&rho[c.iz[a] * nm2 + (int64_t)c.iy[b] * nm + c.ix[d]], sum[a * 4 + b * 2 + d]);
 }
 
 __global__ void k_cells(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
