@@ -599,6 +599,15 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       a.single_target = h->r_cut > 0.2 * box ? 1 : 0;
       a.pcounts = h->pcounts;
       a.only = use_net ? h->fallback : nullptr;
+      {
+        // a group spans at most L/16 (wider ones are walked target by target),
+        // so for a node of cull half side hc the +-L images lie at least
+        // 7L/16 - hc away: beyond r_cut once hc < 7L/16 - r_cut (hc <= 2 h)
+        const double box_u = std::ldexp(1.0, 32 - U), rc_u = std::sqrt(rc2_u) * 1.001;
+        int dimg = 0;
+        while (dimg < 64 && !(7.0 / 16.0 * box_u - 2.0 * std::ldexp(a.h0_u, -dimg) > rc_u)) ++dimg;
+        a.img_depth = dimg;
+      }
       TPM_CUDA(cudaMemsetAsync(h->work, 0, sizeof(uint32_t), s));
       TPM_CUDA(cudaMemsetAsync(h->ndeferred, 0, sizeof(uint32_t), s));
       launch_walk(a, h->walk_grid, s);

@@ -360,7 +360,9 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
         const float lo = sf - bmax[d], hi = sf - bmin[d];
         float dmin = lo > 0.f ? lo : (hi < 0.f ? -hi : 0.f);
         float dmax = fmaxf(fabsf(lo), fabsf(hi));
-        if (a.periodic) {
+        // the +-L images can only come within r_cut of a group (narrower than
+        // L/16) for nodes of half side near L/2: the top levels
+        if (a.periodic && dep < a.img_depth) {
           dmin = fminf(dmin, fminf(a.box_u - hi, lo + a.box_u));
           const float half = 0.5f * a.box_u;
           if (lo <= -half || hi >= half) dmax = half;

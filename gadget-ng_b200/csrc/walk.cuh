@@ -59,6 +59,7 @@ struct WalkArgs {
   int single_target;     // walk every target alone (r_cut above a quarter box)
   uint32_t* pcounts;     // per target (sorted order): leaf pairs, monopoles
   const uint8_t* only;   // nullptr, or: walk only the targets p with only[p] != 0
+  int img_depth;         // periodic: nodes shallower than this need the +-L images in the group cull
 };
 
 int walk_blocks_per_sm(bool accurate);
