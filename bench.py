@@ -47,6 +47,24 @@ def env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(x: float, device) -> float:
+    """The maximum of a per-rank time over all ranks (barrier first); the
+    value itself on one rank."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: int, steps: int, seconds: float, world: int) -> float:
+    """Units processed by all ranks per second of the slowest rank (replicas:
+    every rank processes the same workload)."""
+    return world * units_per_rank * steps / seconds
+
+
 def make_box(name):
     from treepm import ics
     gen, mesh, a0, a1 = WORKLOADS[name]
@@ -298,14 +316,9 @@ def run_b200(args):
             walk_ms.append(st["ms_walk"])
         ev1.record(stream)
         torch.cuda.synchronize()
-    dev_ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([dev_ms], device="cuda")
-    if world > 1:
-        dist.barrier()
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_ms = float(t.item())
+    dev_ms = max_over_ranks(ev0.elapsed_time(ev1), "cuda")
     ms_per_step = dev_ms / args.steps
-    value = world * n * args.steps / (dev_ms * 1e-3)
+    value = whole_job_rate(n, args.steps, dev_ms * 1e-3, world)
 
     # ---- force error of the last evaluation against FP64 Ewald ------------
     ewald = accurate = learned_rep = None
@@ -346,11 +359,8 @@ def run_b200(args):
         solver.kdk_step_host(pos, vel, mass, k1, d, k2, phys["eps2"], g)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_wall = time.perf_counter() - t0
-    te = torch.tensor([e2e_wall], device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * e2e_steps / float(te.item()) if e2e_steps else None
+    e2e_wall = max_over_ranks(time.perf_counter() - t0, "cuda")
+    e2e_value = whole_job_rate(n, e2e_steps, e2e_wall, world) if e2e_steps else None
     h2d = n * (24 + 24 + 8)
     d2h = n * (24 + 24)
 
