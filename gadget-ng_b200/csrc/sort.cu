@@ -93,19 +93,31 @@ __global__ void k_scan_tiles(const uint32_t* __restrict__ tile_counts, const uin
   }
 }
 
+// Stable scatter of one tile: items are ranked per digit (warp match, warps
+// in order), placed in digit order in shared memory, then written out as
+// contiguous runs per digit, so consecutive threads store to consecutive
+// addresses.
+static_assert(SORT_BLOCK == 256, "the downsweep's digit scan maps one thread to one digit");
+constexpr size_t DOWNSWEEP_SMEM = (size_t)SORT_TILE * (sizeof(uint64_t) + sizeof(uint32_t)) +
+                                  (size_t)SORT_WARPS * 256 * sizeof(uint32_t) + 2 * 256 * sizeof(uint32_t);
+
 __global__ void __launch_bounds__(SORT_BLOCK) k_downsweep(const uint64_t* __restrict__ keys_in,
                                                           const uint32_t* __restrict__ vals_in,
                                                           uint64_t* __restrict__ keys_out,
                                                           uint32_t* __restrict__ vals_out, int64_t n, int shift,
                                                           int64_t ntiles, const uint32_t* __restrict__ offsets) {
-  __shared__ uint32_t wcnt[SORT_WARPS][256];
-  __shared__ uint32_t woff[SORT_WARPS][256];
-  __shared__ uint32_t toff[256];
+  extern __shared__ __align__(16) unsigned char ds_smem[];
+  uint64_t* s_k = reinterpret_cast<uint64_t*>(ds_smem);
+  uint32_t* s_v = reinterpret_cast<uint32_t*>(s_k + SORT_TILE);
+  uint32_t(*wcnt)[256] = reinterpret_cast<uint32_t(*)[256]>(s_v + SORT_TILE);  // per-warp counts, then offsets
+  uint32_t* toff = reinterpret_cast<uint32_t*>(wcnt + SORT_WARPS);             // global start of each digit
+  uint32_t* lstart = toff + 256;                                                // start of each digit in the tile
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int i = tid; i < SORT_WARPS * 256; i += SORT_BLOCK) (&wcnt[0][0])[i] = 0;
   for (int d = tid; d < 256; d += SORT_BLOCK) toff[d] = offsets[(int64_t)d * ntiles + blockIdx.x];
   __syncthreads();
-  const int64_t seg = (int64_t)blockIdx.x * SORT_TILE + (int64_t)warp * (32 * SORT_ITEMS);
+  const int64_t tile0 = (int64_t)blockIdx.x * SORT_TILE;
+  const int64_t seg = tile0 + (int64_t)warp * (32 * SORT_ITEMS);
   const unsigned lt_mask = (1u << lane) - 1u;
   uint64_t k[SORT_ITEMS];
   uint32_t v[SORT_ITEMS];
@@ -128,23 +140,47 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_downsweep(const uint64_t* __rest
     dg[j] = d;
   }
   __syncthreads();
-  for (int d = tid; d < 256; d += SORT_BLOCK) {
-    uint32_t s = 0;
+  // per digit: warp offsets (in place) and the tile total; then the digit
+  // starts inside the tile by a block-wide exclusive scan (256 threads)
+  uint32_t tot = 0;
+  {
+    const int d = tid;
 #pragma unroll
     for (int w = 0; w < SORT_WARPS; ++w) {
-      woff[w][d] = s;
-      s += wcnt[w][d];
+      const uint32_t c = wcnt[w][d];
+      wcnt[w][d] = tot;
+      tot += c;
     }
   }
+  uint32_t x = tot;  // inclusive scan of tot over the 256 threads
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __shared__ uint32_t wsum[SORT_WARPS];
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; ++w) before += wsum[w];
+  lstart[tid] = before + x - tot;
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < SORT_ITEMS; ++j) {
-    uint32_t d = dg[j];
+    const uint32_t d = dg[j];
     if (d < 256u) {
-      uint32_t pos = toff[d] + woff[warp][d] + rk[j];
-      keys_out[pos] = k[j];
-      vals_out[pos] = v[j];
+      const uint32_t pos = lstart[d] + wcnt[warp][d] + rk[j];
+      s_k[pos] = k[j];
+      s_v[pos] = v[j];
     }
+  }
+  __syncthreads();
+  const int count = (int)min((int64_t)SORT_TILE, n - tile0);
+  for (int i = tid; i < count; i += SORT_BLOCK) {
+    const uint64_t key = s_k[i];
+    const uint32_t d = (uint32_t)((key >> shift) & 255u);
+    const uint32_t pos = toff[d] + ((uint32_t)i - lstart[d]);
+    keys_out[pos] = key;
+    vals_out[pos] = s_v[i];
   }
 }
 
@@ -175,6 +211,7 @@ void radix_sort_u64(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, voi
   uint32_t* hist = (uint32_t*)carve(8 * 256 * sizeof(uint32_t));
   (void)p;
 
+  TPM_CUDA(cudaFuncSetAttribute(k_downsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DOWNSWEEP_SMEM));
   TPM_CUDA(cudaMemsetAsync(hist, 0, 8 * 256 * sizeof(uint32_t), s));
   k_hist8<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(keys, n, hist);
   TPM_LAUNCH_CHECK();
@@ -198,7 +235,7 @@ void radix_sort_u64(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, voi
     TPM_LAUNCH_CHECK();
     k_scan_tiles<<<256, 1024, 0, s>>>(tile_counts, hist + pass * 256, ntiles, offsets);
     TPM_LAUNCH_CHECK();
-    k_downsweep<<<(unsigned)ntiles, SORT_BLOCK, 0, s>>>(kin, vin, kout, vout, n, shift, ntiles, offsets);
+    k_downsweep<<<(unsigned)ntiles, SORT_BLOCK, DOWNSWEEP_SMEM, s>>>(kin, vin, kout, vout, n, shift, ntiles, offsets);
     TPM_LAUNCH_CHECK();
     std::swap(kin, kout);
     std::swap(vin, vout);
@@ -225,6 +262,7 @@ void radix_sort_u64_all_passes(uint64_t* keys, uint32_t* vals, int64_t n, void* 
   uint32_t* tile_counts = (uint32_t*)carve((size_t)ntiles * 256 * sizeof(uint32_t));
   uint32_t* offsets = (uint32_t*)carve((size_t)ntiles * 256 * sizeof(uint32_t));
   uint32_t* hist = (uint32_t*)carve(8 * 256 * sizeof(uint32_t));
+  TPM_CUDA(cudaFuncSetAttribute(k_downsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DOWNSWEEP_SMEM));
   TPM_CUDA(cudaMemsetAsync(hist, 0, 8 * 256 * sizeof(uint32_t), s));
   k_hist8<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(keys, n, hist);
   TPM_LAUNCH_CHECK();
@@ -238,7 +276,7 @@ void radix_sort_u64_all_passes(uint64_t* keys, uint32_t* vals, int64_t n, void* 
     TPM_LAUNCH_CHECK();
     k_scan_tiles<<<256, 1024, 0, s>>>(tile_counts, hist + pass * 256, ntiles, offsets);
     TPM_LAUNCH_CHECK();
-    k_downsweep<<<(unsigned)ntiles, SORT_BLOCK, 0, s>>>(kin, vin, kout, vout, n, shift, ntiles, offsets);
+    k_downsweep<<<(unsigned)ntiles, SORT_BLOCK, DOWNSWEEP_SMEM, s>>>(kin, vin, kout, vout, n, shift, ntiles, offsets);
     TPM_LAUNCH_CHECK();
     std::swap(kin, kout);
     std::swap(vin, vout);
