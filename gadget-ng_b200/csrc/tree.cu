@@ -312,7 +312,8 @@ __global__ void k_aggregate(int64_t n, double scale, const uint32_t* __restrict_
   int32_t P = leaf_oparent[p];
   for (int guard = 0; P >= 0; ++guard) {
     if (guard > 2 * KEY_LEVELS + 4) return;  // deeper than any key can describe: malformed tree
-    __threadfence();
+    // release this thread's node before counting it in (a leaf wrote nothing)
+    if (guard > 0) __threadfence();
     const uint32_t arrived = atomicAdd(&cnt[P], 1u);
     if (arrived + 1 != nchild[P]) return;  // another child finishes this node
     __threadfence();
