@@ -301,6 +301,25 @@ __global__ void k_oct_childlist(int64_t n_int, const uint32_t* __restrict__ slot
 // ---------------------------------------------------------------------------
 // bottom-up aggregation (octree.rs:547-629), float64, reference order
 // ---------------------------------------------------------------------------
+// Mass and centre of mass of an octree child (leaf: the particle).
+__device__ __forceinline__ void child_moments(uint32_t c, double scale, const uint32_t* __restrict__ qx,
+                                              const uint32_t* __restrict__ qy, const uint32_t* __restrict__ qz,
+                                              const double* __restrict__ pmass, const double* o_mass,
+                                              const double* o_com, double* m, double* x, double* y, double* z) {
+  if (c & LEAF_BIT) {
+    const uint32_t j = c & ~LEAF_BIT;
+    *m = pmass[j];
+    *x = decode(qx[j], scale);
+    *y = decode(qy[j], scale);
+    *z = decode(qz[j], scale);
+  } else {
+    *m = __ldcg(&o_mass[c]);
+    *x = __ldcg(&o_com[3 * (int64_t)c]);
+    *y = __ldcg(&o_com[3 * (int64_t)c + 1]);
+    *z = __ldcg(&o_com[3 * (int64_t)c + 2]);
+  }
+}
+
 __global__ void k_aggregate(int64_t n, double scale, const uint32_t* __restrict__ qx,
                             const uint32_t* __restrict__ qy, const uint32_t* __restrict__ qz,
                             const double* __restrict__ pmass, const int32_t* __restrict__ leaf_oparent,
@@ -318,7 +337,6 @@ __global__ void k_aggregate(int64_t n, double scale, const uint32_t* __restrict_
     if (arrived + 1 != nchild[P]) return;  // another child finishes this node
     __threadfence();
     // pass 1: mass and centre of mass over the children in octant order
-    double cm[8], cx[8], cy[8], cz[8];
     uint32_t cs[8];
     double mt = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
 #pragma unroll
@@ -327,19 +345,7 @@ __global__ void k_aggregate(int64_t n, double scale, const uint32_t* __restrict_
       cs[s] = c;
       if (c == EMPTY_SLOT) continue;
       double m, x, y, z;
-      if (c & LEAF_BIT) {
-        const uint32_t j = c & ~LEAF_BIT;
-        m = pmass[j];
-        x = decode(qx[j], scale);
-        y = decode(qy[j], scale);
-        z = decode(qz[j], scale);
-      } else {
-        m = __ldcg(&o_mass[c]);
-        x = __ldcg(&o_com[3 * (int64_t)c]);
-        y = __ldcg(&o_com[3 * (int64_t)c + 1]);
-        z = __ldcg(&o_com[3 * (int64_t)c + 2]);
-      }
-      cm[s] = m; cx[s] = x; cy[s] = y; cz[s] = z;
+      child_moments(c, scale, qx, qy, qz, pmass, o_mass, o_com, &m, &x, &y, &z);
       mt = dadd(mt, m);
       ax = dadd(ax, dmul(x, m));
       ay = dadd(ay, dmul(y, m));
@@ -351,15 +357,17 @@ __global__ void k_aggregate(int64_t n, double scale, const uint32_t* __restrict_
       comy = ddiv(ay, mt);
       comz = ddiv(az, mt);
     }
-    // pass 2: quadrupole by the parallel-axis theorem (outer_traceless :197-207)
+    // pass 2: quadrupole by the parallel-axis theorem (outer_traceless :197-207);
+    // the children are read again (cache hits) rather than held in registers
     double qd[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
+#pragma unroll 1
     for (int s = 0; s < 8; ++s) {
       const uint32_t c = cs[s];
       if (c == EMPTY_SLOT) continue;
-      const double m = cm[s];
+      double m, x, y, z;
+      child_moments(c, scale, qx, qy, qz, pmass, o_mass, o_com, &m, &x, &y, &z);
       if (m == 0.0) continue;
-      const double sx = dsub(cx[s], comx), sy = dsub(cy[s], comy), sz = dsub(cz[s], comz);
+      const double sx = dsub(x, comx), sy = dsub(y, comy), sz = dsub(z, comz);
       const double s2 = dadd(dadd(dmul(sx, sx), dmul(sy, sy)), dmul(sz, sz));
       const double m3 = dmul(m, 3.0);
       double oq[6];
