@@ -39,6 +39,9 @@ WORKLOADS = {
     "treepm64": ("treepm_box_64", 64, 0.1, 0.12),
     "clustered512": ("clustered_box_512", 512, 0.1, 0.12),
     "pm64": ("pm_box_64", 64, 0.02, 0.0202),
+    # profiling case for the mesh kernels: the 256^3 mesh (working set above
+    # the 126 MB L2) with 128^3 particles
+    "treepm128_mesh256": ("treepm_box_128", 256, 0.1, 0.12),
 }
 FLOP_PER_INTERACTION = 37  # FMA = 2, MUFU = 1: the pair-kernel convention of the cost model
 

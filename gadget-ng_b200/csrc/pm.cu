@@ -32,44 +32,90 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
-// Batched radix-2 Stockham FFT in shared memory.  ROWMAJOR: element (j, c) at
+// Batched Stockham FFT in shared memory.  ROWMAJOR: element (j, c) at
 // a[c * n + j]; otherwise at a[j * cols + c].  Returns the buffer holding the
 // result (a or b).
 template <bool ROWMAJOR>
-__device__ float2* fft_smem(float2* a, float2* b, int n, int logn, int cols, const float2* tw, bool inv) {
+__device__ __forceinline__ int fft_addr(int c, int j, int n, int cols) {
+  return ROWMAJOR ? c * n + j : j * cols + c;
+}
+
+// Twiddle exp(-+2 pi i m / n) from the half table tw[m] = exp(-2 pi i m / n), m < n/2.
+__device__ __forceinline__ float2 twiddle(const float2* tw, int m, int n, bool inv) {
   const int half = n >> 1;
-  const int total = half * cols;
-  int Ns = 1;
-  for (int s = 0; s < logn; ++s, Ns <<= 1) {
+  float2 w = m < half ? tw[m] : make_float2(-tw[m - half].x, -tw[m - half].y);
+  if (inv) w.y = -w.y;
+  return w;
+}
+
+// Stockham radix-4 passes (one radix-2 pass last when log2 n is odd): each
+// pass reads a, writes b, then swaps; between passes only shared memory and
+// one barrier.  Pass with Ns outputs done so far: element j of a column,
+// k = j mod Ns, inputs a[j + i n/4] twiddled by w^(i k) with w = exp(-2 pi i /
+// (4 Ns)), a 4-point DFT, outputs b[(j / Ns) 4 Ns + k + i Ns].  cols is a
+// power of two (log2 = lcols).
+template <bool ROWMAJOR>
+__device__ float2* fft_smem(float2* a, float2* b, int n, int logn, int cols, const float2* tw, bool inv) {
+  const int lcols = __ffs(cols) - 1;
+  int Ns = 1, lNs = 0;
+  while (logn - lNs >= 2) {
+    const int q = n >> 2, lq = logn - 2;
+    const int total = q << lcols;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      int j, c;
+      if (ROWMAJOR) {
+        j = idx & (q - 1);
+        c = idx >> lq;
+      } else {
+        c = idx & (cols - 1);
+        j = idx >> lcols;
+      }
+      const int k = j & (Ns - 1);
+      float2 v0 = a[fft_addr<ROWMAJOR>(c, j, n, cols)];
+      float2 v1 = a[fft_addr<ROWMAJOR>(c, j + q, n, cols)];
+      float2 v2 = a[fft_addr<ROWMAJOR>(c, j + 2 * q, n, cols)];
+      float2 v3 = a[fft_addr<ROWMAJOR>(c, j + 3 * q, n, cols)];
+      if (k) {  // w^(i k) = exp(-2 pi i i k / (4 Ns)) = tw[i k n / (4 Ns)]
+        const int sh = logn - lNs - 2;
+        v1 = cmul(v1, twiddle(tw, k << sh, n, inv));
+        v2 = cmul(v2, twiddle(tw, (2 * k) << sh, n, inv));
+        v3 = cmul(v3, twiddle(tw, (3 * k) << sh, n, inv));
+      }
+      const float2 a0 = cadd(v0, v2), a1 = csub(v0, v2), a2 = cadd(v1, v3), d = csub(v1, v3);
+      // (v1 - v3) * (-i) forward, * (+i) inverse
+      const float2 a3 = inv ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);
+      const int o = ((j - k) << 2) + k;
+      b[fft_addr<ROWMAJOR>(c, o, n, cols)] = cadd(a0, a2);
+      b[fft_addr<ROWMAJOR>(c, o + Ns, n, cols)] = cadd(a1, a3);
+      b[fft_addr<ROWMAJOR>(c, o + 2 * Ns, n, cols)] = csub(a0, a2);
+      b[fft_addr<ROWMAJOR>(c, o + 3 * Ns, n, cols)] = csub(a1, a3);
+    }
+    __syncthreads();
+    float2* t = a;
+    a = b;
+    b = t;
+    Ns <<= 2;
+    lNs += 2;
+  }
+  if (lNs < logn) {  // the last radix-2 pass
+    const int half = n >> 1;
+    const int total = half << lcols;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
       int j, c;
       if (ROWMAJOR) {
         j = idx & (half - 1);
         c = idx >> (logn - 1);
       } else {
-        c = idx % cols;
-        j = idx / cols;
+        c = idx & (cols - 1);
+        j = idx >> lcols;
       }
       const int k = j & (Ns - 1);
-      float2 w = tw[k << (logn - 1 - s)];
-      if (inv) w.y = -w.y;
-      float2 x0, x1;
-      if (ROWMAJOR) {
-        x0 = a[c * n + j];
-        x1 = a[c * n + j + half];
-      } else {
-        x0 = a[j * cols + c];
-        x1 = a[(j + half) * cols + c];
-      }
-      const float2 t = cmul(x1, w);
+      const float2 w = twiddle(tw, k << (logn - 1 - lNs), n, inv);
+      const float2 x0 = a[fft_addr<ROWMAJOR>(c, j, n, cols)];
+      const float2 t = cmul(a[fft_addr<ROWMAJOR>(c, j + half, n, cols)], w);
       const int o = ((j - k) << 1) + k;
-      if (ROWMAJOR) {
-        b[c * n + o] = cadd(x0, t);
-        b[c * n + o + Ns] = csub(x0, t);
-      } else {
-        b[o * cols + c] = cadd(x0, t);
-        b[(o + Ns) * cols + c] = csub(x0, t);
-      }
+      b[fft_addr<ROWMAJOR>(c, o, n, cols)] = cadd(x0, t);
+      b[fft_addr<ROWMAJOR>(c, o + Ns, n, cols)] = csub(x0, t);
     }
     __syncthreads();
     float2* t = a;

@@ -63,28 +63,45 @@ def test_gravity_coupling():
 
 
 def _stockham_mirror(x, inverse=False):
-    """The radix-2 Stockham indexing of the device FFT (pm.cu fft_smem)."""
+    """The Stockham indexing of the device FFT (pm.cu fft_smem): radix-4
+    passes, then one radix-2 pass when log2 n is odd."""
     n = len(x)
     logn = n.bit_length() - 1
     a = x.astype(complex).copy()
     b = np.empty_like(a)
     tw = np.exp(-2j * np.pi * np.arange(n // 2) / n)
-    Ns = 1
-    for s in range(logn):
+
+    def twiddle(m):
+        w = tw[m] if m < n // 2 else -tw[m - n // 2]
+        return np.conj(w) if inverse else w
+
+    Ns, lNs = 1, 0
+    while logn - lNs >= 2:
+        q = n // 4
+        for j in range(q):
+            k = j & (Ns - 1)
+            v = [a[j + i * q] for i in range(4)]
+            if k:
+                sh = logn - lNs - 2
+                v = [v[0]] + [v[i] * twiddle((i * k) << sh) for i in (1, 2, 3)]
+            a0, a1, a2, d = v[0] + v[2], v[0] - v[2], v[1] + v[3], v[1] - v[3]
+            a3 = d * (1j if inverse else -1j)
+            o = ((j - k) << 2) + k
+            b[o], b[o + Ns], b[o + 2 * Ns], b[o + 3 * Ns] = a0 + a2, a1 + a3, a0 - a2, a1 - a3
+        a, b = b, a
+        Ns, lNs = Ns * 4, lNs + 2
+    if lNs < logn:
         for j in range(n // 2):
             k = j & (Ns - 1)
-            w = tw[k << (logn - 1 - s)]
-            if inverse:
-                w = np.conj(w)
+            w = twiddle(k << (logn - 1 - lNs))
             x0, x1 = a[j], a[j + n // 2] * w
             o = ((j - k) << 1) + k
             b[o], b[o + Ns] = x0 + x1, x0 - x1
         a, b = b, a
-        Ns *= 2
     return a
 
 
-@pytest.mark.parametrize("n", [2, 4, 8, 32, 128])
+@pytest.mark.parametrize("n", [2, 4, 8, 16, 32, 128, 256])
 def test_stockham_indexing_is_a_dft(n):
     x = np.random.default_rng(n).standard_normal(n) + 1j * np.random.default_rng(n + 1).standard_normal(n)
     assert np.max(np.abs(_stockham_mirror(x) - np.fft.fft(x))) < 1e-12 * n
