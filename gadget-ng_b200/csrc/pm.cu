@@ -422,6 +422,108 @@ inline int ilog2(int n) {
   return l;
 }
 // rows of one x-pass block: 4096 complex values, never more than the mesh has
+// ---- power spectrum (crates/gadget-ng-analysis/src/power_spectrum.rs) --------------
+// CIC assignment of power_spectrum.rs:146-166: fx = x / cell, floor, weights
+// (1 - t, t), indices rem_euclid(n), m * wx * wy * wz; stored z-major like the
+// PM mesh (the binned spectrum does not depend on the axis order).
+__device__ __forceinline__ void pk_deposit_one(double x, double y, double z, double m, double cell, int nm,
+                                               float* __restrict__ rho) {
+  const double f[3] = {ddiv(x, cell), ddiv(y, cell), ddiv(z, cell)};
+  int i0[3];
+  double t[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double fl = floor(f[d]);
+    i0[d] = (int)fl;
+    t[d] = dsub(f[d], fl);
+  }
+#pragma unroll
+  for (int dx = 0; dx < 2; ++dx)
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dz = 0; dz < 2; ++dz) {
+        const double wx = dx ? t[0] : dsub(1.0, t[0]), wy = dy ? t[1] : dsub(1.0, t[1]);
+        const double wz = dz ? t[2] : dsub(1.0, t[2]);
+        const int jx = ((i0[0] + dx) % nm + nm) % nm, jy = ((i0[1] + dy) % nm + nm) % nm,
+                  jz = ((i0[2] + dz) % nm + nm) % nm;
+        atomicAdd(&rho[((int64_t)jz * nm + jy) * nm + jx], (float)dmul(dmul(dmul(m, wx), wy), wz));
+      }
+}
+
+__global__ void k_pk_deposit_pos(const double* __restrict__ pos, const double* __restrict__ m, int64_t n,
+                                 double cell, int nm, float* __restrict__ rho) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  pk_deposit_one(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], m[i], cell, nm, rho);
+}
+
+__global__ void k_pk_deposit_q(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                               const uint32_t* __restrict__ qz, const double* __restrict__ m, int64_t n,
+                               double scale, double cell, int nm, float* __restrict__ rho) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  pk_deposit_one(decode(qx[i], scale), decode(qy[i], scale), decode(qz[i], scale), m[i], cell, nm, rho);
+}
+
+__device__ __forceinline__ double pk_sinc(int k, int nm) {
+  if (k == 0) return 1.0;
+  const double x = (double)k / (double)nm;
+  return sinpi(x) / (M_PI * x);
+}
+
+// Forward z pass of the half spectrum, then every mode into its |k| shell:
+// sum of |rho_k|^2 / W^2 and the mode count, modes with 0 < kx < nm/2 twice
+// (their conjugates are not stored), as power_spectrum.rs:74-110 over the full
+// cube.
+__global__ void k_fft_z_pk(const float2* __restrict__ spec, int nm, int logn, int nh, int tx,
+                           const float2* __restrict__ tw, double* __restrict__ pk_sum,
+                           unsigned long long* __restrict__ pk_n) {
+  extern __shared__ float2 sm[];
+  float2* s_tw = sm;
+  float2* a = sm + (nm >> 1);
+  float2* b = a + nm * tx;
+  double* hs = reinterpret_cast<double*>(b + nm * tx);
+  unsigned long long* hn = reinterpret_cast<unsigned long long*>(hs + (nm >> 1));
+  load_twiddles(s_tw, tw, nm);
+  for (int i = threadIdx.x; i < (nm >> 1); i += blockDim.x) {
+    hs[i] = 0.0;
+    hn[i] = 0ull;
+  }
+  const int kx0 = blockIdx.x * tx, y = blockIdx.y;
+  const int64_t plane = (int64_t)nm * nh;
+  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+    const int z = idx / tx, c = idx % tx;
+    a[idx] = (kx0 + c < nh) ? spec[z * plane + (int64_t)y * nh + kx0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* res = fft_smem<false>(a, b, nm, logn, tx, s_tw, false);
+  const int nb = nm >> 1;
+  const int fy = y <= nb ? y : y - nm;
+  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+    const int z = idx / tx, c = idx % tx;
+    const int kx = kx0 + c;
+    if (kx >= nh) continue;
+    const int fz = z <= nb ? z : z - nm;
+    const double k2 = (double)kx * kx + (double)fy * fy + (double)fz * fz;
+    if (k2 == 0.0) continue;
+    const double bf = sqrt(k2) - 0.5;
+    if (bf < 0.0 || bf >= (double)nb) continue;
+    const int bin = (int)bf;
+    const double w = pk_sinc(kx, nm) * pk_sinc(fy, nm) * pk_sinc(fz, nm);
+    const double re = res[idx].x, im = res[idx].y;
+    const int mult = (kx == 0 || kx == nb) ? 1 : 2;
+    atomicAdd(&hs[bin], mult * (re * re + im * im) / (w * w));
+    atomicAdd(&hn[bin], (unsigned long long)mult);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    if (hn[i]) {
+      atomicAdd(&pk_sum[i], hs[i]);
+      atomicAdd(&pk_n[i], hn[i]);
+    }
+}
+
 inline int rows_for(int nm) {
   int r = nm >= 4096 ? 1 : 4096 / nm;
   return r > nm * nm ? nm * nm : r;
@@ -547,6 +649,53 @@ void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uin
   k_cells<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, id, n, p.box / TWO32, (double)p.nm / p.box, p.nm,
                                                       cells_by_id);
   TPM_LAUNCH_CHECK();
+}
+
+void pm_power_spectrum(const PmPlan& p, const double* pos, const uint32_t* qx, const uint32_t* qy,
+                       const uint32_t* qz, const double* mass, int64_t n, double total_mass, double* pk_sum,
+                       unsigned long long* pk_n, double* k_out, double* pk_out, unsigned long long* n_out,
+                       cudaStream_t s) {
+  const int nm = p.nm, nh = p.nh, logn = p.logn, nb = nm / 2;
+  const int64_t nm3 = (int64_t)nm * nm * nm;
+  const double cell = p.box / nm;
+  TPM_CUDA(cudaMemsetAsync(p.rho, 0, sizeof(float) * nm3, s));
+  TPM_CUDA(cudaMemsetAsync(pk_sum, 0, sizeof(double) * nb, s));
+  TPM_CUDA(cudaMemsetAsync(pk_n, 0, sizeof(unsigned long long) * nb, s));
+  if (n > 0) {
+    if (pos)
+      k_pk_deposit_pos<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(pos, mass, n, cell, nm, p.rho);
+    else
+      k_pk_deposit_q<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, mass, n, p.box / TWO32, cell, nm,
+                                                                 p.rho);
+    TPM_LAUNCH_CHECK();
+  }
+  const int rows = rows_for(nm), tx = tx_for(nm);
+  const int64_t nrows = (int64_t)nm * nm;
+  const size_t sm_x = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)rows * nm);
+  const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
+  const size_t sm_pk = sm_y + (sizeof(double) + sizeof(unsigned long long)) * (size_t)nb;
+  TPM_CUDA(cudaFuncSetAttribute(k_fft_z_pk, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  const int nblk_x = (int)((nrows + rows - 1) / rows);
+  const int ntx = (nh + tx - 1) / tx;
+  k_fft_x_r2c<<<nblk_x, 256, sm_x, s>>>(p.rho, p.spec, nm, logn, nh, rows, nrows, p.twiddle);
+  TPM_LAUNCH_CHECK();
+  k_fft_y<<<dim3(ntx, nm, 1), 256, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
+  TPM_LAUNCH_CHECK();
+  k_fft_z_pk<<<dim3(ntx, nm), 256, sm_pk, s>>>(p.spec, nm, logn, nh, tx, p.twiddle, pk_sum, pk_n);
+  TPM_LAUNCH_CHECK();
+  std::vector<double> hs((size_t)nb);
+  std::vector<unsigned long long> hn((size_t)nb);
+  TPM_CUDA(cudaMemcpyAsync(hs.data(), pk_sum, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+  TPM_CUDA(cudaMemcpyAsync(hn.data(), pk_n, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost, s));
+  TPM_CUDA(cudaStreamSynchronize(s));
+  // delta_k = rho_k / (mean_rho V_cell) = rho_k nm^3 / M for k != 0; norm (V / nm^3)^2
+  const double vol = p.box * p.box * p.box;
+  const double scale = (double)nm3 / total_mass, norm = (vol / (double)nm3) * (vol / (double)nm3);
+  for (int i = 0; i < nb; ++i) {
+    k_out[i] = (i + 1.0) * 2.0 * M_PI / p.box;
+    n_out[i] = hn[i];
+    pk_out[i] = hn[i] ? hs[i] * scale * scale * norm / (double)hn[i] : 0.0;
+  }
 }
 
 }  // namespace tpm

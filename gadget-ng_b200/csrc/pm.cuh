@@ -54,4 +54,14 @@ void pm_gather_kick(const PmPlan& p, const GatherArgs& a, cudaStream_t s);
 void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const uint32_t* id,
               int64_t n, int32_t* cells_by_id, cudaStream_t s);
 
+// Power spectrum of power_spectrum.rs: CIC assignment (from float64 positions
+// pos, or from fixed-point q when pos is null), the plan's FFT passes, shells
+// of |k|.  pk_sum / pk_n: device scratch of nm/2; outputs (host, nm/2 each):
+// k, P(k) (0 where a shell has no modes) and the mode counts.  Overwrites the
+// plan's density and spectrum work arrays.
+void pm_power_spectrum(const PmPlan& p, const double* pos, const uint32_t* qx, const uint32_t* qy,
+                       const uint32_t* qz, const double* mass, int64_t n, double total_mass, double* pk_sum,
+                       unsigned long long* pk_n, double* k_out, double* pk_out, unsigned long long* n_out,
+                       cudaStream_t s);
+
 }  // namespace tpm

@@ -246,6 +246,8 @@ struct tpm_handle {
   uint32_t* lgrp_size = nullptr;
   uint32_t* lgrp_count = nullptr;
   unsigned long long* learned_count = nullptr;
+  double* pk_sum = nullptr;        // power-spectrum shells (nm/2)
+  unsigned long long* pk_n = nullptr;
   uint32_t* cell_of = nullptr;     // near field: cell of each particle, particles by cell
   uint32_t* cell_items = nullptr;
   uint32_t* cell_start = nullptr;  // nm^3 + 1
@@ -1012,6 +1014,68 @@ int tpm_kdk_step_host(tpm_handle* h, double* pos, double* vel, const double* mas
   rc = tpm_kdk_step(h, kick_half, drift, kick_half2, eps2, g);
   if (rc) return rc;
   return tpm_get_state(h, pos, vel, nullptr);
+}
+
+int tpm_power_spectrum(const double* pos, const double* mass, int64_t n, double box, int32_t mesh, int32_t device,
+                       double* k, double* pk, uint64_t* n_modes) {
+  if (!pos || !mass || !k || !pk || !n_modes || n < 1 || !(box > 0.0) || !std::isfinite(box) || mesh < 4 ||
+      mesh > 1024 || (mesh & (mesh - 1)) != 0)
+    return TPM_ERR_INVALID_ARGUMENT;
+  PmPlan plan;
+  double *dpos = nullptr, *dmass = nullptr, *dsum = nullptr;
+  unsigned long long* dn = nullptr;
+  int rc = TPM_OK;
+  try {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      throw Error(TPM_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev) throw Error(TPM_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    TPM_CUDA(cudaSetDevice(device));
+    double mtot = 0.0;
+    for (int64_t i = 0; i < n; ++i) mtot += mass[i];
+    if (!(mtot > 0.0) || !std::isfinite(mtot)) throw Error(TPM_ERR_INVALID_ARGUMENT, "total mass must be positive");
+    pm_plan_init(plan, mesh, box, 0.0, 0u, device);
+    TPM_CUDA(cudaMalloc(&dpos, sizeof(double) * 3 * n));
+    TPM_CUDA(cudaMalloc(&dmass, sizeof(double) * n));
+    TPM_CUDA(cudaMalloc(&dsum, sizeof(double) * (mesh / 2)));
+    TPM_CUDA(cudaMalloc(&dn, sizeof(unsigned long long) * (mesh / 2)));
+    TPM_CUDA(cudaMemcpy(dpos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+    TPM_CUDA(cudaMemcpy(dmass, mass, sizeof(double) * n, cudaMemcpyHostToDevice));
+    std::vector<unsigned long long> hn((size_t)mesh / 2);
+    pm_power_spectrum(plan, dpos, nullptr, nullptr, nullptr, dmass, n, mtot, dsum, dn, k, pk, hn.data(), 0);
+    for (int i = 0; i < mesh / 2; ++i) n_modes[i] = hn[i];
+  } catch (const Error& e) {
+    rc = e.code ? e.code : TPM_ERR_CUDA;
+  }
+  cudaFree(dpos);
+  cudaFree(dmass);
+  cudaFree(dsum);
+  cudaFree(dn);
+  pm_plan_free(plan);
+  return rc;
+}
+
+int tpm_get_power_spectrum(tpm_handle* h, double* k, double* pk, uint64_t* n_modes) {
+  if (!h || !k || !pk || !n_modes) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (h->n == 0) throw Error(TPM_ERR_NOT_READY, "no particles set");
+    const int nb = h->pm.nm / 2;
+    if (!h->pk_sum) {
+      h->pk_sum = h->alloc<double>(nb, 0);
+      h->pk_n = h->alloc<unsigned long long>(nb, 0);
+    }
+    const Particles& P = h->P[h->cur];
+    std::vector<unsigned long long> hn((size_t)nb);
+    pm_power_spectrum(h->pm, nullptr, P.qx, P.qy, P.qz, P.mass, h->n, total_mass(h), h->pk_sum, h->pk_n, k, pk,
+                      hn.data(), h->stream);
+    for (int i = 0; i < nb; ++i) n_modes[i] = hn[i];
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
 }
 
 int tpm_set_learned(tpm_handle* h, const tpm_cnn* c) {

@@ -130,6 +130,8 @@ SIGNATURES = {
     "tpm_cnn_train": ([_P, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _P], _I),
     "tpm_cnn_evaluate": ([_P, C.c_int32, C.c_int32, _P], _I),
     "tpm_set_learned": ([_P, _P], _I),
+    "tpm_power_spectrum": ([_P, _P, _I64, _D, C.c_int32, C.c_int32, _P, _P, _P], _I),
+    "tpm_get_power_spectrum": ([_P, _P, _P, _P], _I),
 }
 NOALLOC_MAX_PARTICLES = 1 << 18
 

@@ -86,6 +86,16 @@ class TreePmSolver:
         self.r_split = float(r_split)
         self._h = _Handle(cfg)
 
+    def power_spectrum(self):
+        """P(k) of the resident particles on this solver's mesh (in-situ
+        analysis, power_spectrum.rs estimator): (k, pk, n_modes) of the shells
+        that hold modes."""
+        nb = self.grid_size // 2
+        k, pk, nm = np.empty(nb), np.empty(nb), np.empty(nb, dtype=np.uint64)
+        check(self._h.h, self._h._lib.tpm_get_power_spectrum(self._h.h, _ptr(k), _ptr(pk), _ptr(nm)))
+        keep = nm > 0
+        return k[keep], pk[keep], nm[keep].astype(np.int64)
+
     def set_learned(self, network):
         """Attach a trained network (a copy is taken); None detaches it."""
         check(self._h.h, self._h._lib.tpm_set_learned(self._h.h, None if network is None else network.h))
@@ -240,6 +250,21 @@ def make_solver(cfg: dict):
                         opening_criterion=1 if crit in ("relative", 1) else 0,
                         err_tol_force_acc=float(grav.get("err_tol_force_acc", 0.005)),
                         accurate=bool(grav.get("treepm_accurate", False)))
+
+
+def power_spectrum(positions, masses, box_size: float, mesh: int, device: int = 0):
+    """power_spectrum(positions, masses, box_size, mesh)
+    (crates/gadget-ng-analysis/src/power_spectrum.rs:35-120) on the GPU:
+    (k, pk, n_modes) of the shells that hold modes, by increasing k."""
+    pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+    m = np.ascontiguousarray(masses, dtype=np.float64).reshape(-1)
+    nb = int(mesh) // 2
+    k, pk, nm = np.empty(max(nb, 1)), np.empty(max(nb, 1)), np.empty(max(nb, 1), dtype=np.uint64)
+    rc = load().tpm_power_spectrum(_ptr(pos), _ptr(m), pos.shape[0], float(box_size), int(mesh), int(device),
+                                   _ptr(k), _ptr(pk), _ptr(nm))
+    check(None, rc)
+    keep = nm[:nb] > 0
+    return k[:nb][keep], pk[:nb][keep], nm[:nb][keep].astype(np.int64)
 
 
 def drift_kick_factors(omega_m: float, omega_lambda: float, h0: float, a0: float, dt: float):

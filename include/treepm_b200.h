@@ -241,6 +241,19 @@ int tpm_ewald(const double* pos, const double* mass, int64_t n, double box, doub
  * FP32 roofline denominator of the short-range walk. */
 int tpm_fp32_peak(int device, double* tflops);
 
+/* ---- power spectrum (in-situ analysis) ----------------------------------------
+ * power_spectrum(positions, masses, box_size, mesh)
+ * (crates/gadget-ng-analysis/src/power_spectrum.rs:35-120): CIC assignment,
+ * 3D FFT, |delta_k|^2 / (sinc sinc sinc)^2 * (V/mesh^3)^2 averaged in shells
+ * floor(|k| - 1/2) of the fundamental.  Outputs hold mesh/2 shells: k (bin + 1)
+ * 2 pi / L, P(k) (0 where n_modes is 0 — the reference drops those shells)
+ * and the mode counts.  mesh: power of two in [4, 1024]. */
+int tpm_power_spectrum(const double* pos, const double* mass, int64_t n, double box, int32_t mesh, int32_t device,
+                       double* k, double* pk, uint64_t* n_modes);
+/* The same estimator on a handle's resident particles (mesh = its pm_grid_size);
+ * overwrites the density mesh that tpm_get_mesh returns. */
+int tpm_get_power_spectrum(tpm_handle* h, double* k, double* pk, uint64_t* n_modes);
+
 /* ---- learned short-range network (extension) --------------------------------
  * No counterpart in the reference.  A small 3D CNN reads the long-range mesh
  * (density and potential) and predicts the short-range acceleration at each
