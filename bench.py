@@ -340,6 +340,18 @@ def run_b200(args):
             accurate = accurate_mode_report(box, mesh, phys, p_now, g_last, tg, ref, local)
             learned_rep = learned_mode_report(box, mesh, phys, p_now, g_last, tg, ref, local, ms_per_step)
 
+    # ---- in-situ P(k) of the final state (analysis, not part of the step) --
+    pk_rep = None
+    if rank == 0:
+        t_pk = []
+        for _ in range(3):
+            c0 = time.perf_counter()
+            kk, pk, nmod = solver.power_spectrum()
+            t_pk.append(time.perf_counter() - c0)
+        pk_rep = {"ms": 1e3 * float(np.median(t_pk)), "shells": int(len(kk)),
+                  "k_h_per_mpc": [float(kk[0]), float(kk[-1])], "pk_first_last": [float(pk[0]), float(pk[-1])],
+                  "estimator": "power_spectrum.rs (CIC, |delta_k|^2 / W, shells floor(|k| - 1/2))"}
+
     # ---- end to end through the host-buffer API (e2e) -------------------
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
     pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -404,6 +416,7 @@ def run_b200(args):
         "force_error_vs_ewald": ewald,
         "accurate_mode": accurate,
         "learned_mode": learned_rep,
+        "power_spectrum": pk_rep,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
