@@ -272,6 +272,29 @@ def learned_mode_report(box, mesh, phys, pos, g, targets, ref, device, plain_ms,
             "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}}
 
 
+def zeldovich_report(device, n_side=256, reps=3):
+    """Time tpm_set_particles_zeldovich for n_side^3 particles (EH spectrum,
+    sigma_8 = 0.8, a_init = 0.02) into a solver whose PM mesh is the IC lattice
+    (no allocation inside the call): modes, three inverse transforms, particle
+    write; wall time of the synchronous call, median of `reps`."""
+    import treepm
+    solver = treepm.TreePmSolver(n_side, 100.0, r_split=2.5 * 100.0 / n_side, device=device)
+    cfg = dict(transfer="eisenstein_hu", sigma8=0.8, omega_m=0.315, omega_lambda=0.685, omega_b=0.049, h=0.674,
+               box_size_mpc_h=100.0, spectral_index=0.965, cosmology=True, a_init=0.02, h0=0.1)
+    solver.set_particles_zeldovich(n_side, 1, **cfg)  # warm
+    ts = []
+    for r in range(reps):
+        c0 = time.perf_counter()
+        solver.set_particles_zeldovich(n_side, 2 + r, **cfg)
+        ts.append(time.perf_counter() - c0)
+    solver.close()
+    ms = 1e3 * float(np.median(ts))
+    n3 = n_side ** 3
+    return {"ms": ms, "particles": n3, "particles_per_s": n3 / (ms * 1e-3),
+            "spectrum": "Eisenstein-Hu no-wiggle, sigma_8 0.8, n_s 0.965, a_init 0.02",
+            "path": "tpm_set_particles_zeldovich (ic_zeldovich.rs zeldovich_ics): modes, 3 inverse FFTs, particle write"}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -352,6 +375,11 @@ def run_b200(args):
                   "k_h_per_mpc": [float(kk[0]), float(kk[-1])], "pk_first_last": [float(pk[0]), float(pk[-1])],
                   "estimator": "power_spectrum.rs (CIC, |delta_k|^2 / W, shells floor(|k| - 1/2))"}
 
+    # ---- Zel'dovich ICs generated on the device (not part of the step) -----
+    ic_rep = None
+    if rank == 0 and not args.no_ics:
+        ic_rep = zeldovich_report(local)
+
     # ---- end to end through the host-buffer API (e2e) -------------------
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
     pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -417,6 +445,7 @@ def run_b200(args):
         "accurate_mode": accurate,
         "learned_mode": learned_rep,
         "power_spectrum": pk_rep,
+        "zeldovich_ics": ic_rep,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -447,6 +476,7 @@ def main():
     ap.add_argument("--cpu-targets", type=int, default=65536)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--no-ics", action="store_true", help="skip the Zel'dovich IC timing")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak measurement (profiling runs)")
     ap.add_argument("--no-ewald", action="store_true", help="skip the FP64 Ewald error report")
     ap.add_argument("--no-accurate", action="store_true", help="skip the accurate-mode report")

@@ -1,0 +1,278 @@
+// Zel'dovich initial conditions on the device, written straight into a
+// solver handle (crates/gadget-ng-core/src/ic_zeldovich.rs:287-760).
+//
+// The Gaussian field is generated on the half spectrum [z][y][kx] that the
+// mesh FFT uses: modes with kx > 0 are their own representatives; in the kx = 0
+// plane a mode and its conjugate twin share the representative with the
+// smaller packed index ix n^2 + iy n + iz (the reference's rule), so
+// delta(-k) = conj(delta(k)).  DC and every mode with a Nyquist component are
+// zero, as in the reference.  Psi_a(k) = i n_a / |n|^2 delta(k) for the three
+// axes, three inverse transforms, then particles on the lattice in the
+// reference's order (gid = ix n^2 + iy n + iz) at cell centres plus Psi, and
+// momenta a^2 f H Psi.  Each mode's seed is the reference's mode_seed of its
+// representative; the two uniforms behind its Gaussian come from SplitMix64
+// seeded there instead of the reference's StdRng (ChaCha12 in rand 0.10), so a
+// realisation is reproducible here but not equal to the reference's; spectrum,
+// symmetry, displacement and momentum conventions are the reference's.
+#include <cmath>
+#include <vector>
+
+#include "../../include/treepm_b200.h"
+#include "common.cuh"
+#include "pm.cuh"
+#include "tree.cuh"
+
+namespace tpm {
+
+// Per-mode standard deviation sigma(|n|) (ic_zeldovich.rs:387-466 with the
+// Eisenstein-Hu no-wiggle transfer of transfer_fn.rs:89-127).
+struct IcSpectrum {
+  int kind;        // 0 power law, 1 Eisenstein-Hu
+  double amp;      // A (sigma_8 already applied)
+  double n_s;
+  double omega_m, omega_b, h;
+  double two_pi_h_over_bsm;
+  double inv_sqrt_n3;
+};
+
+__host__ __device__ inline double eh_transfer(double k, double omega_m, double omega_b, double h) {
+  if (k <= 0.0) return 1.0;
+  const double om_h2 = omega_m * h * h, ob_h2 = omega_b * h * h, fb = omega_b / omega_m;
+  const double s = 44.5 * log(9.83 / om_h2) / sqrt(1.0 + 10.0 * pow(ob_h2, 0.75));
+  const double ag = 1.0 - 0.328 * log(431.0 * om_h2) * fb + 0.38 * log(22.3 * om_h2) * fb * fb;
+  const double ks = 0.43 * (k * h) * s;
+  const double ks2 = ks * ks;
+  const double gamma = omega_m * h * (ag + (1.0 - ag) / (1.0 + ks2 * ks2));
+  const double q = k / (gamma > 1e-30 ? gamma : 1e-30);
+  const double l0 = log(2.718281828459045 * 2.0 + 1.8 * q);
+  const double c0 = 14.2 + 731.0 / (1.0 + 62.5 * q);
+  const double t = l0 / (l0 + c0 * q * q);
+  return t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+}
+
+__host__ __device__ inline double ic_sigma(const IcSpectrum& sp, double n_abs) {
+  if (n_abs <= 0.0) return 0.0;
+  if (sp.kind == 0) return sp.amp * pow(n_abs, sp.n_s / 4.0) * sp.inv_sqrt_n3;
+  const double k = sp.two_pi_h_over_bsm * n_abs;
+  return sp.amp * pow(k, sp.n_s / 2.0) * eh_transfer(k, sp.omega_m, sp.omega_b, sp.h) * sp.inv_sqrt_n3;
+}
+
+namespace {
+
+// Murmur3's 64-bit finalizer, the reference's hash_u64 (ic_zeldovich.rs:27-35);
+// per-mode seeds are the reference's mode_seed (:38-42) unchanged.
+__device__ __forceinline__ uint64_t fmix64(uint64_t x) {
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdull;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ull;
+  x ^= x >> 33;
+  return x;
+}
+
+// SplitMix64 (Steele, Lea and Flood 2014): the uniform stream behind each
+// mode's Gaussian, standing in for the reference's StdRng seeded by mode_seed.
+__device__ __forceinline__ uint64_t splitmix_next(uint64_t& state) {
+  state += 0x9E3779B97F4A7C15ull;
+  uint64_t z = state;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double u53(uint64_t x) { return (double)(x >> 11) * (1.0 / 9007199254740992.0); }
+
+// gaussian_std (ic_zeldovich.rs:51-57): Box-Muller on the first two uniforms
+// of the stream seeded by `seed`.
+__device__ __forceinline__ double gaussian_std(uint64_t seed) {
+  uint64_t st = seed;
+  const double u1 = fmax(u53(splitmix_next(st)), 1e-300);
+  const double u2 = u53(splitmix_next(st));
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+__device__ __forceinline__ int mode_int(int j, int n) { return j <= n / 2 ? j : j - n; }
+
+__global__ void k_ic_modes(int n, int nh, uint64_t seed, IcSpectrum sp, float2* __restrict__ spec3,
+                           int64_t comp_stride) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)n * n * nh;
+  if (i >= total) return;
+  const int kx = (int)(i % nh), y = (int)((i / nh) % n), z = (int)(i / ((int64_t)n * nh));
+  const int nx = kx, ny = mode_int(y, n), nz = mode_int(z, n), half = n / 2;
+  const double n2 = (double)nx * nx + (double)ny * ny + (double)nz * nz;
+  float2 out[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  if (n2 > 0.0 && nx != half && abs(ny) != half && abs(nz) != half) {
+    // representative of the pair {k, -k} and whether this mode is its twin
+    const int64_t self = ((int64_t)kx * n + y) * n + z;
+    bool twin = false;
+    int64_t rep = self;
+    if (kx == 0) {
+      const int yn = (n - y) % n, zn = (n - z) % n;
+      const int64_t other = (int64_t)yn * n + zn;
+      if (other < self) {
+        rep = other;
+        twin = true;
+      }
+    }
+    const double sig = ic_sigma(sp, sqrt(n2));
+    const uint64_t ms = fmix64(seed ^ fmix64((uint64_t)rep));
+    double re = sig * gaussian_std(ms), im = sig * gaussian_std(fmix64(ms ^ 0x9E3779B97F4A7C15ull));
+    if (twin) im = -im;
+    const double inv_n2 = 1.0 / n2;
+    const int na[3] = {nx, ny, nz};
+#pragma unroll
+    for (int c = 0; c < 3; ++c)  // i n_a / |n|^2 (re + i im)
+      out[c] = make_float2((float)(-na[c] * im * inv_n2), (float)(na[c] * re * inv_n2));
+  }
+  for (int c = 0; c < 3; ++c) spec3[c * comp_stride + i] = out[c];
+}
+
+__global__ void k_ic_particles(int n, double box, double psi_scale, double vel_factor, const float* __restrict__ psi,
+                               int64_t n3, Particles p) {
+  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gid >= n3) return;
+  const int ix = (int)(gid / ((int64_t)n * n)), iy = (int)((gid / n) % n), iz = (int)(gid % n);
+  const int64_t node = ((int64_t)iz * n + iy) * n + ix;  // the mesh's [z][y][x] layout
+  const double d = box / n;
+  const int ii[3] = {ix, iy, iz};
+  uint32_t q[3];
+  float v[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double s = (double)psi[c * n3 + node] * psi_scale;
+    double u = ((ii[c] + 0.5) * d + s) / box;
+    u = u - floor(u);
+    q[c] = (uint32_t)((unsigned long long)llrint(u * TWO32) & 0xFFFFFFFFull);
+    v[c] = (float)(s * vel_factor);
+  }
+  p.qx[gid] = q[0];
+  p.qy[gid] = q[1];
+  p.qz[gid] = q[2];
+  p.vx[gid] = v[0];
+  p.vy[gid] = v[1];
+  p.vz[gid] = v[2];
+  const double m = 1.0 / (double)n3;
+  p.mass[gid] = m;
+  p.massf[gid] = (float)m;
+  p.id[gid] = (uint32_t)gid;
+}
+
+// transfer_fn.rs:146-184, :190-199, :222-228
+double sigma_sq_unit(double r, double n_s, double om, double ob, double h) {
+  const double lk0 = std::log(1e-5), lk1 = std::log(5e2);
+  const int steps = 8192;
+  const double dl = (lk1 - lk0) / steps;
+  auto integrand = [&](double k) {
+    const double t = eh_transfer(k, om, ob, h);
+    const double x = k * r;
+    const double w = std::fabs(x) < 1e-4 ? 1.0 - x * x / 10.0 : 3.0 * (std::sin(x) - x * std::cos(x)) / (x * x * x);
+    return std::pow(k, n_s + 3.0) * t * t * w * w;
+  };
+  double sum = 0.0, fprev = integrand(1e-5);
+  for (int i = 1; i <= steps; ++i) {
+    const double f = integrand(std::exp(lk0 + i * dl));
+    sum += 0.5 * (fprev + f) * dl;
+    fprev = f;
+  }
+  return sum / (2.0 * M_PI * M_PI);
+}
+
+}  // namespace
+
+// Spectrum, growth and momentum factors of a configuration (host).
+bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, double* vel_factor, double* scale) {
+  if (!c || c->n_side < 4 || c->n_side > 1024 || (c->n_side & (c->n_side - 1)) != 0) return false;
+  if (c->transfer != 0 && c->transfer != 1) return false;
+  if (c->transfer == 1 && !(c->omega_m > 0.0 && c->omega_b >= 0.0 && c->h > 0.0 && c->box_size_mpc_h > 0.0))
+    return false;
+  const double n3 = (double)c->n_side * c->n_side * c->n_side;
+  sp->kind = c->transfer;
+  sp->n_s = c->spectral_index;
+  sp->omega_m = c->omega_m;
+  sp->omega_b = c->omega_b;
+  sp->h = c->h;
+  sp->two_pi_h_over_bsm = c->transfer == 1 ? 2.0 * M_PI * c->h / c->box_size_mpc_h : 0.0;
+  sp->inv_sqrt_n3 = 1.0 / std::sqrt(n3);
+  sp->amp = c->amplitude;
+  if (c->transfer == 1 && c->sigma8 > 0.0) {
+    const double v = sigma_sq_unit(8.0, c->spectral_index, c->omega_m, c->omega_b, c->h);
+    sp->amp = v > 0.0 ? c->sigma8 / std::sqrt(v) : c->sigma8;
+  }
+  // cosmology.rs:509-520 (H, LCDM), :598-610 (f), :650-666 / :736-742 (CPT92 ratio)
+  double a = 1.0, om = 1.0, ol = 0.0;
+  if (c->cosmology) {
+    a = c->a_init;
+    om = c->omega_m;
+    ol = c->omega_lambda;
+  }
+  if (!(a > 0.0) || !(c->h0 > 0.0)) return false;
+  const double hh = c->h0 * std::sqrt(std::max(om / (a * a * a) + ol, 0.0));
+  const double om_a = om / (a * a * a) / ((hh / c->h0) * (hh / c->h0));
+  const double f = std::pow(std::max(om_a, 0.0), 0.55);
+  *vel_factor = a * a * f * hh;
+  *scale = 1.0;
+  if (c->rescale_to_a_init && c->cosmology) {
+    auto growth = [&](double aa) {
+      const double a3 = aa * aa * aa, den = om + ol * a3;
+      if (den <= 0.0) return aa;
+      const double oma = om / den, ola = ol * a3 / den;
+      const double br = std::pow(std::max(oma, 0.0), 4.0 / 7.0) - ola + (1.0 + oma / 2.0) * (1.0 + ola / 70.0);
+      return br <= 0.0 ? aa : aa * 2.5 * oma / br;
+    };
+    const double d1 = growth(1.0);
+    *scale = d1 == 0.0 ? 1.0 : growth(a) / d1;
+  }
+  return true;
+}
+
+// `mesh` is a plan of the solver whose spectrum and force buffers may be
+// overwritten; it is used when its mesh is the IC lattice (no allocation),
+// otherwise a temporary plan of n_side^3 is made and freed.
+void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cudaStream_t s, PmPlan* mesh) {
+  IcSpectrum sp{};
+  double vel = 0.0, scale = 1.0;
+  if (!zeldovich_factors(c, &sp, &vel, &scale)) throw Error(TPM_ERR_INVALID_ARGUMENT, "bad Zel'dovich configuration");
+  const int n = c->n_side;
+  const bool reuse = mesh && mesh->nm == n && mesh->ncomp >= 3 && mesh->spec3 && mesh->force;
+  PmPlan temp;
+  PmPlan& plan = reuse ? *mesh : temp;
+  try {
+    if (!reuse) {
+      int dev = 0;
+      TPM_CUDA(cudaGetDevice(&dev));
+      pm_plan_init(temp, n, box, 0.0, 0u, dev);
+    }
+    const int64_t nh = n / 2 + 1, plane = (int64_t)n * n * nh, n3 = (int64_t)n * n * n;
+    const int64_t comp_stride = (int64_t)n * n * nh;  // spec3 holds ncomp planes of this size
+    k_ic_modes<<<grid_for(plane, 256, 1ll << 30), 256, 0, s>>>(n, (int)nh, c->seed, sp, plan.spec3, comp_stride);
+    TPM_LAUNCH_CHECK();
+    pm_inverse_components(plan, 3, s);
+    // rustfft's inverse is unnormalised: Psi = Re(ifft) / n^3 * cell (ic_zeldovich.rs:602-614)
+    const double psi_scale = (box / n) / (double)n3 * scale;
+    k_ic_particles<<<grid_for(n3, 256, 1ll << 30), 256, 0, s>>>(n, box, psi_scale, vel, plan.force, n3, out);
+    TPM_LAUNCH_CHECK();
+    TPM_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    if (!reuse) pm_plan_free(temp);
+    throw;
+  }
+  if (!reuse) pm_plan_free(temp);
+}
+
+}  // namespace tpm
+
+extern "C" int tpm_zeldovich_sigma(const tpm_zeldovich* c, const double* n_abs, int64_t count, double* sigma,
+                                   double* factors) {
+  tpm::IcSpectrum sp{};
+  double vel = 0.0, scale = 1.0;
+  if (!tpm::zeldovich_factors(c, &sp, &vel, &scale) || count < 0 || (count > 0 && (!n_abs || !sigma)))
+    return TPM_ERR_INVALID_ARGUMENT;
+  for (int64_t i = 0; i < count; ++i) sigma[i] = tpm::ic_sigma(sp, n_abs[i]);
+  if (factors) {
+    factors[0] = sp.amp;
+    factors[1] = vel;
+    factors[2] = scale;
+  }
+  return TPM_OK;
+}

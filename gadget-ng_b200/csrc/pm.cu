@@ -277,6 +277,29 @@ __global__ void k_fft_y(float2* __restrict__ spec, int64_t comp_stride, int nm, 
   }
 }
 
+// ---- z pass (c2c) on [z][y][kx] half spectra, one component per blockIdx.z --------
+__global__ void k_fft_z_c2c(float2* __restrict__ spec, int64_t comp_stride, int nm, int logn, int nh, int tx,
+                            const float2* __restrict__ tw, int inv) {
+  extern __shared__ float2 sm[];
+  float2* s_tw = sm;
+  float2* a = sm + (nm >> 1);
+  float2* b = a + nm * tx;
+  load_twiddles(s_tw, tw, nm);
+  const int kx0 = blockIdx.x * tx, y = blockIdx.y;
+  const int64_t plane = (int64_t)nm * nh;
+  float2* base = spec + blockIdx.z * comp_stride + (int64_t)y * nh;
+  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+    const int z = idx / tx, c = idx % tx;
+    a[idx] = (kx0 + c < nh) ? base[z * plane + kx0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* res = fft_smem<false>(a, b, nm, logn, tx, s_tw, inv != 0);
+  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
+    const int z = idx / tx, c = idx % tx;
+    if (kx0 + c < nh) base[z * plane + kx0 + c] = res[idx];
+  }
+}
+
 // ---- z pass + Green's function x filter x gradient + inverse z pass ---------------
 __global__ void k_fft_z_poisson(const float2* __restrict__ spec, float2* __restrict__ spec3, int nm, int logn,
                                 int nh, int tx, const float2* __restrict__ tw, const float* __restrict__ kval,
@@ -648,6 +671,23 @@ void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uin
   if (n == 0) return;
   k_cells<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, id, n, p.box / TWO32, (double)p.nm / p.box, p.nm,
                                                       cells_by_id);
+  TPM_LAUNCH_CHECK();
+}
+
+void pm_inverse_components(const PmPlan& p, int ncomp, cudaStream_t s) {
+  const int nm = p.nm, nh = p.nh, logn = p.logn;
+  const int rows = rows_for(nm), tx = tx_for(nm);
+  const int64_t nrows = (int64_t)nm * nm;
+  const size_t sm_x = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)rows * nm);
+  const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
+  TPM_CUDA(cudaFuncSetAttribute(k_fft_z_c2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  const int nblk_x = (int)((nrows + rows - 1) / rows);
+  const int ntx = (nh + tx - 1) / tx;
+  k_fft_z_c2c<<<dim3(ntx, nm, ncomp), 256, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
+  TPM_LAUNCH_CHECK();
+  k_fft_y<<<dim3(ntx, nm, ncomp), 256, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
+  TPM_LAUNCH_CHECK();
+  k_fft_x_c2r<<<dim3(nblk_x, ncomp), 256, sm_x, s>>>(p.spec3, p.force, nm, logn, nh, rows, nrows, p.twiddle);
   TPM_LAUNCH_CHECK();
 }
 

@@ -54,6 +54,12 @@ void pm_gather_kick(const PmPlan& p, const GatherArgs& a, cudaStream_t s);
 void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const uint32_t* id,
               int64_t n, int32_t* cells_by_id, cudaStream_t s);
 
+struct Particles;
+
+// Unnormalised inverse 3D transforms of the first ncomp half spectra in
+// spec3 ([z][y][kx] each) into the real grids force[c * nm^3 + (z nm + y) nm + x].
+void pm_inverse_components(const PmPlan& p, int ncomp, cudaStream_t s);
+
 // Power spectrum of power_spectrum.rs: CIC assignment (from float64 positions
 // pos, or from fixed-point q when pos is null), the plan's FFT passes, shells
 // of |k|.  pk_sum / pk_n: device scratch of nm/2; outputs (host, nm/2 each):

@@ -23,6 +23,7 @@
 
 namespace tpm {
 thread_local unsigned long long g_kernel_launches = 0;
+void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cudaStream_t s, PmPlan* mesh);
 }
 
 using namespace tpm;
@@ -1014,6 +1015,26 @@ int tpm_kdk_step_host(tpm_handle* h, double* pos, double* vel, const double* mas
   rc = tpm_kdk_step(h, kick_half, drift, kick_half2, eps2, g);
   if (rc) return rc;
   return tpm_get_state(h, pos, vel, nullptr);
+}
+
+int tpm_set_particles_zeldovich(tpm_handle* h, const tpm_zeldovich* cfg) {
+  if (!h || !cfg) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (cfg->n_side < 4 || cfg->n_side > 1024 || (cfg->n_side & (cfg->n_side - 1)) != 0)
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "n_side must be a power of two in [4, 1024]");
+    const int64_t n = (int64_t)cfg->n_side * cfg->n_side * cfg->n_side;
+    if (n >= ((int64_t)1 << 31)) throw Error(TPM_ERR_INVALID_ARGUMENT, "too many particles");
+    ensure_capacity(h, n);
+    h->n = n;
+    h->cur = 0;
+    h->forces_valid = false;
+    h->m_total_valid = false;
+    zeldovich_fill(cfg, h->cfg.box_size, h->P[0], h->stream, &h->pm);
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
 }
 
 int tpm_power_spectrum(const double* pos, const double* mass, int64_t n, double box, int32_t mesh, int32_t device,

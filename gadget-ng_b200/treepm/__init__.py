@@ -6,7 +6,8 @@ seeded workload generators in `treepm.ics`.
 """
 from ._lib import TreePmError, load  # noqa: F401
 from .solver import (PmSolver, TreePmSolver, advance_a, drift_kick_factors,  # noqa: F401
-                     gravity_coupling_qksl, make_solver, power_spectrum)
+                     gravity_coupling_qksl, make_solver, power_spectrum, zeldovich_config,
+                     zeldovich_sigma)
 
 __all__ = ["TreePmSolver", "PmSolver", "make_solver", "drift_kick_factors", "advance_a", "gravity_coupling_qksl",
-           "power_spectrum", "TreePmError", "load"]
+           "power_spectrum", "zeldovich_config", "zeldovich_sigma", "TreePmError", "load"]

@@ -49,6 +49,28 @@ class TpmConfig(C.Structure):
     ]
 
 
+class TpmZeldovich(C.Structure):
+    """tpm_zeldovich: the reference's Zel'dovich IC configuration
+    (crates/gadget-ng-core/src/ic_zeldovich.rs:621-640 arguments)."""
+    _fields_ = [
+        ("n_side", C.c_int32),
+        ("transfer", C.c_int32),
+        ("seed", C.c_uint64),
+        ("amplitude", C.c_double),
+        ("spectral_index", C.c_double),
+        ("sigma8", C.c_double),
+        ("omega_m", C.c_double),
+        ("omega_lambda", C.c_double),
+        ("omega_b", C.c_double),
+        ("h", C.c_double),
+        ("box_size_mpc_h", C.c_double),
+        ("a_init", C.c_double),
+        ("h0", C.c_double),
+        ("cosmology", C.c_int32),
+        ("rescale_to_a_init", C.c_int32),
+    ]
+
+
 class TpmStats(C.Structure):
     _fields_ = [
         ("n_particles", C.c_int64),
@@ -132,6 +154,8 @@ SIGNATURES = {
     "tpm_set_learned": ([_P, _P], _I),
     "tpm_power_spectrum": ([_P, _P, _I64, _D, C.c_int32, C.c_int32, _P, _P, _P], _I),
     "tpm_get_power_spectrum": ([_P, _P, _P, _P], _I),
+    "tpm_set_particles_zeldovich": ([_P, _P], _I),
+    "tpm_zeldovich_sigma": ([_P, _P, _I64, _P, _P], _I),
 }
 NOALLOC_MAX_PARTICLES = 1 << 18
 

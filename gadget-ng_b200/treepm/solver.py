@@ -16,7 +16,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import TpmConfig, TpmStats, TreePmError, check, load
+from ._lib import TpmConfig, TpmStats, TpmZeldovich, TreePmError, check, load
 
 
 def _ptr(a):
@@ -124,6 +124,14 @@ class TreePmSolver:
         mass = np.ascontiguousarray(mass, dtype=np.float64).reshape(-1)
         v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64).reshape(-1, 3)
         check(self._h.h, self._h._lib.tpm_set_particles(self._h.h, _ptr(pos), _ptr(v), _ptr(mass), pos.shape[0]))
+
+    def set_particles_zeldovich(self, n_side: int, seed: int = 42, **cfg):
+        """Zel'dovich initial conditions (ic_zeldovich.rs:621-760) generated on
+        the device into this solver: n_side^3 particles of mass 1/N, gid = ix n^2
+        + iy n + iz.  Keywords as `zeldovich_config`."""
+        c = zeldovich_config(n_side, seed, **cfg)
+        check(self._h.h, self._h._lib.tpm_set_particles_zeldovich(self._h.h, C.byref(c)))
+        return int(n_side) ** 3
 
     def set_particles_fixed(self, q, mass, vel=None):
         q = np.ascontiguousarray(q, dtype=np.uint32).reshape(-1, 3)
@@ -265,6 +273,34 @@ def power_spectrum(positions, masses, box_size: float, mesh: int, device: int = 
     check(None, rc)
     keep = nm[:nb] > 0
     return k[:nb][keep], pk[:nb][keep], nm[:nb][keep].astype(np.int64)
+
+
+def zeldovich_config(n_side: int, seed: int = 42, *, transfer: str = "power_law", amplitude: float = 1e-4,
+                     spectral_index: float = -2.0, sigma8: float = 0.0, omega_m: float = 1.0,
+                     omega_lambda: float = 0.0, omega_b: float = 0.049, h: float = 0.674,
+                     box_size_mpc_h: float = 0.0, a_init: float = 1.0, h0: float = 1.0, cosmology: bool = False,
+                     rescale_to_a_init: bool = False) -> "TpmZeldovich":
+    """IcKind::Zeldovich fields with the defaults of
+    crates/gadget-ng-core/src/config/sections/simulation_ic.rs:285-303 (seed
+    42, amplitude 1e-4, spectral index -2, omega_b 0.049, h 0.674); transfer
+    "power_law" or "eisenstein_hu"."""
+    kinds = {"power_law": 0, "eisenstein_hu": 1}
+    if transfer not in kinds:
+        raise ValueError(f"transfer must be one of {sorted(kinds)}")
+    return TpmZeldovich(n_side=int(n_side), transfer=kinds[transfer], seed=int(seed), amplitude=float(amplitude),
+                        spectral_index=float(spectral_index), sigma8=float(sigma8), omega_m=float(omega_m),
+                        omega_lambda=float(omega_lambda), omega_b=float(omega_b), h=float(h),
+                        box_size_mpc_h=float(box_size_mpc_h), a_init=float(a_init), h0=float(h0),
+                        cosmology=int(bool(cosmology)), rescale_to_a_init=int(bool(rescale_to_a_init)))
+
+
+def zeldovich_sigma(n_abs, n_side: int, **cfg):
+    """sigma(|n|) of the IC spectrum and the factors (A, a^2 f H, D(a)/D(1))."""
+    c = zeldovich_config(n_side, 0, **cfg)
+    x = np.ascontiguousarray(n_abs, dtype=np.float64).reshape(-1)
+    sig, fac = np.empty_like(x), np.empty(3)
+    check(None, load().tpm_zeldovich_sigma(C.byref(c), _ptr(x), x.shape[0], _ptr(sig), _ptr(fac)))
+    return sig, (float(fac[0]), float(fac[1]), float(fac[2]))
 
 
 def drift_kick_factors(omega_m: float, omega_lambda: float, h0: float, a0: float, dt: float):

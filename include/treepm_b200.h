@@ -241,6 +241,39 @@ int tpm_ewald(const double* pos, const double* mass, int64_t n, double box, doub
  * FP32 roofline denominator of the short-range walk. */
 int tpm_fp32_peak(int device, double* tflops);
 
+/* ---- Zel'dovich initial conditions -----------------------------------------------
+ * zeldovich_ics (crates/gadget-ng-core/src/ic_zeldovich.rs:287-760) generated
+ * on the device into a handle: n_side^3 particles of mass 1/N on the lattice
+ * (cell centres, gid = ix n^2 + iy n + iz) displaced by the 1LPT field of a
+ * Gaussian density with per-mode sigma(|n|) = A |n|^(n_s/4) / sqrt(N^3)
+ * (transfer 0, power law) or A k^(n_s/2) T_EH(k) / sqrt(N^3) (transfer 1,
+ * Eisenstein-Hu no-wiggle, k = 2 pi |n| h / box_size_mpc_h, A from sigma8 when
+ * sigma8 > 0); momenta a^2 f(a) H(a) Psi (cosmology != 0) or H0 Psi (a = 1,
+ * f = 1).  rescale_to_a_init multiplies Psi by D(a_init)/D(1) (CPT92).  Each
+ * mode is seeded by the reference's mode_seed (murmur3 fmix64 of seed and the
+ * packed mode index); the two uniforms of its Box-Muller Gaussians come from
+ * SplitMix64 seeded there instead of the reference's StdRng, so realisations
+ * are reproducible but differ from the reference's; statistics and
+ * conventions match. */
+typedef struct tpm_zeldovich {
+  int32_t n_side;         /* power of two, 4..1024 */
+  int32_t transfer;       /* 0 power law, 1 Eisenstein-Hu no-wiggle */
+  uint64_t seed;
+  double amplitude;
+  double spectral_index;
+  double sigma8;          /* <= 0: use amplitude */
+  double omega_m, omega_lambda, omega_b, h;
+  double box_size_mpc_h;  /* box in Mpc/h for k (Eisenstein-Hu) */
+  double a_init;
+  double h0;              /* H0 in internal time units */
+  int32_t cosmology;      /* 0: a = 1, f = 1, H = h0 */
+  int32_t rescale_to_a_init;
+} tpm_zeldovich;
+int tpm_set_particles_zeldovich(tpm_handle* h, const tpm_zeldovich* cfg);
+/* Host evaluation of sigma(|n|) for count values and the factors
+ * [A, momentum factor a^2 f H, growth rescale] (factors may be NULL). */
+int tpm_zeldovich_sigma(const tpm_zeldovich* cfg, const double* n_abs, int64_t count, double* sigma, double* factors);
+
 /* ---- power spectrum (in-situ analysis) ----------------------------------------
  * power_spectrum(positions, masses, box_size, mesh)
  * (crates/gadget-ng-analysis/src/power_spectrum.rs:35-120): CIC assignment,

@@ -1,0 +1,296 @@
+"""Zel'dovich initial conditions (crates/gadget-ng-core/src/ic_zeldovich.rs).
+
+The CPU restatement (oracle/ic_oracle.py) is pinned by the reference's own
+unit tests (transfer_fn.rs:289-440 properties of T(k), sigma_8 and the top-hat;
+ic_zeldovich.rs:1019-1104 DC mode, Hermitian symmetry, real Psi, zero mean
+displacement) and by figures the reference committed from its own runs:
+rms(Psi) = 4.8831e-6 and 1.2409e-7 for N = 32, seed 42 with and without the
+growth rescale (ratio 0.025413), and v_rms at a = 0.02 for seeds 42, 137 and
+271.  Those runs used the reference's StdRng stream, which this build does not
+reproduce (the mode seeds are the reference's, the uniforms behind each
+Gaussian come from SplitMix64), so a realisation is compared with the
+reference through its ensemble statistics, and with the oracle value by value.
+
+The device generator must match the oracle particle by particle: positions
+within 1e-5 rms(Psi) plus the 2^-32 box fixed-point step, momenta within
+1e-5 rms(p) (float32 spectrum, transforms and velocities).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import ic_oracle as ico
+import pk_oracle as pko
+
+# The reference's IC tests and committed runs (phase37_growth_rescaled_ics.rs:53-72,
+# phase40_physical_ics_normalization.rs:57-72): Planck-like EH spectrum, BOX = 1.
+EH = dict(omega_m=0.315, omega_b=0.049, h=0.674, box_mpc_h=100.0, sigma8=0.8)
+A_INIT, H0, OMEGA_L = 0.02, 0.1, 0.685
+
+
+def _nabs(n):
+    f = ico.mode_int(n)
+    nx, ny, nz = np.meshgrid(f, f, f, indexing="ij")
+    return np.sqrt(nx * nx + ny * ny + nz * nz)
+
+
+def _sig_eh(n):
+    return ico.sigma_of_n(_nabs(n), n, "eisenstein_hu", 0.0, 0.965, **EH)
+
+
+def _sig_pl(n, amp=1e-4, ns=-2.0):
+    return ico.sigma_of_n(_nabs(n), n, "power_law", amp, ns)
+
+
+def _vel_factor(a=A_INIT):
+    return a * a * ico.growth_rate_f(a, EH["omega_m"], OMEGA_L, H0) * ico.hubble(a, EH["omega_m"], OMEGA_L, H0)
+
+
+# ---- oracle pinned by the reference's unit tests ------------------------------
+P18 = (0.315, 0.049, 0.674)
+
+
+def test_oracle_eh_transfer_properties():  # transfer_fn.rs:289-440
+    t = lambda k: float(ico.transfer_eh_nowiggle(k, *P18))  # noqa: E731
+    assert abs(t(1e-4) - 1.0) < 1e-3
+    assert t(10.0) < t(0.1) and 0.05 < t(0.1) < 0.30 and t(10.0) < 0.01
+    for e in range(-4, 3):
+        assert 0.0 < t(10.0 ** e) <= 1.0 + 1e-10
+    assert t(1e-3) > 0.90 and t(0.01) > t(0.1) > t(1.0)
+
+
+def test_oracle_sigma8_and_tophat():  # transfer_fn.rs:346-398
+    s2 = ico.sigma_sq_unit(8.0, 0.965, *P18)
+    assert math.isfinite(s2) and s2 > 0.0
+    a = ico.amplitude_for_sigma8(0.8, 0.965, *P18)
+    assert abs(a * math.sqrt(s2) - 0.8) / 0.8 < 1e-3
+    assert abs(float(ico.tophat(0.0)) - 1.0) < 1e-12
+    assert ico.tophat(1.0) < ico.tophat(0.1) and ico.tophat(10.0) < ico.tophat(1.0)
+
+
+def test_oracle_dc_mode_is_zero():  # ic_zeldovich.rs:1019-1030
+    d = ico.delta_kspace(8, 42, _sig_pl(8))
+    assert d[0, 0, 0] == 0.0
+
+
+def test_oracle_hermitian_symmetry():  # ic_zeldovich.rs:1032-1067
+    n = 8
+    d = ico.delta_kspace(n, 99, _sig_pl(n))
+    f = ico.mode_int(n)
+    neg = (-np.arange(n)) % n
+    err = 0.0
+    for ix in range(n):
+        for iy in range(n):
+            for iz in range(n):
+                if n // 2 in (abs(f[ix]), abs(f[iy]), abs(f[iz])):
+                    continue
+                v, c = d[ix, iy, iz], d[neg[ix], neg[iy], neg[iz]]
+                err = max(err, abs(v.real - c.real) + abs(v.imag + c.imag))
+    assert err < 1e-14
+
+
+def test_oracle_displacement_is_real_and_zero_mean():  # ic_zeldovich.rs:1069-1104
+    _, max_im = ico.displacement(ico.delta_kspace(8, 7, _sig_pl(8)), 8, 1.0)
+    assert max_im < 1e-10
+    psi, _ = ico.displacement(ico.delta_kspace(16, 1234, _sig_pl(16)), 16, 1.0)
+    for p in psi:
+        assert abs(float(np.mean(p))) < 1e-12
+
+
+def test_oracle_nyquist_planes_are_zero():  # ic_zeldovich.rs:317-320
+    n = 8
+    d = ico.delta_kspace(n, 3, _sig_pl(n))
+    assert np.all(d[n // 2] == 0) and np.all(d[:, n // 2] == 0) and np.all(d[:, :, n // 2] == 0)
+
+
+def test_oracle_growth_and_momentum_factors_match_reference_runs():
+    """docs/reports/2026-04-phase37-growth-rescaled-ics.md section 5.1:
+    rms(Psi) 4.8831e-6 legacy and 1.2409e-7 rescaled, ratio s = 0.025413; and
+    docs/reports/figures/phase40/phase40_summary.csv: v_rms(a = 0.02, seed 42)
+    = 3.875860e-08 of the same field, so a^2 f H = v_rms / rms(Psi)."""
+    om = EH["omega_m"]
+    s = ico.growth_d(A_INIT, om, OMEGA_L) / ico.growth_d(1.0, om, OMEGA_L)
+    assert abs(s - 0.025413) < 1e-6
+    assert abs(4.8831e-6 * s - 1.2409e-7) / 1.2409e-7 < 1e-4
+    assert abs(_vel_factor() - 3.875860e-08 / 4.8831e-6) / _vel_factor() < 2e-5
+
+
+def test_oracle_ensemble_rms_matches_reference_runs():
+    """The reference's three committed realisations (N = 32, seeds 42, 137,
+    271: v_rms 3.875860e-08, 3.577938e-08, 3.576682e-08) against the
+    ensemble expectation E<|Psi|^2> of this spectrum.  One realisation
+    scatters by about 8.5 % in rms (measured over 40 oracle draws), so the mean
+    of three is held to 15 % (about 3 sigma)."""
+    n = 32
+    sig = _sig_eh(n)
+    expected = math.sqrt(ico.expected_psi2(n, 1.0, sig))
+    ref = np.array([3.875860e-08, 3.577938e-08, 3.576682e-08]) / _vel_factor()
+    assert abs(ref.mean() / expected - 1.0) < 0.15
+    ours = []
+    for seed in (42, 137, 271, 1, 2, 3):
+        _, mom = ico.zeldovich(n, 1.0, sig, seed=seed)
+        ours.append(math.sqrt(np.mean(np.sum(mom * mom, 1))))
+    assert abs(np.mean(ours) / expected - 1.0) < 0.12
+
+
+def _pk_expected(n, box, sig):
+    """Linear-order P(k) of Zel'dovich ICs through the reference's estimator:
+    CIC of a lattice displaced by Psi onto the coincident mesh is a centred
+    difference per axis times the neighbour average of the others, and the
+    estimator divides by one sinc product (power_spectrum.rs:74-110), so per
+    mode E[P] = (2 pi / n)^2 2 sigma^2 (V / n^3)^2 R(k) with
+    R = [sum_a (n_a^2 / |n|^2) sinc_a prod_{b != a} cos(pi n_b / n)]^2 / (prod sinc)^2,
+    averaged over each shell's modes."""
+    f = ico.mode_int(n)
+    nx, ny, nz = np.meshgrid(f, f, f, indexing="ij")
+    n2 = (nx * nx + ny * ny + nz * nz).astype(np.float64)
+    sc = [pko.sinc(c / n) for c in (nx, ny, nz)]
+    co = [np.cos(np.pi * c / n) for c in (nx, ny, nz)]
+    with np.errstate(all="ignore"):
+        term = (nx ** 2 * sc[0] * co[1] * co[2] + ny ** 2 * sc[1] * co[0] * co[2] + nz ** 2 * sc[2] * co[0] * co[1]) / n2
+        r = (term / (sc[0] * sc[1] * sc[2])) ** 2
+    half = n // 2
+    keep = (np.abs(nx) != half) & (np.abs(ny) != half) & (np.abs(nz) != half)
+    per_mode = np.where(keep, (2 * np.pi / n) ** 2 * 2 * sig ** 2 * (box ** 3 / n ** 3) ** 2 * r, 0.0)
+    bf = np.sqrt(n2) - 0.5
+    ok = (n2 > 0) & (bf >= 0) & (bf < half)
+    b = np.floor(bf[ok]).astype(np.int64)
+    return np.bincount(b, weights=per_mode[ok], minlength=half) / np.maximum(np.bincount(b, minlength=half), 1)
+
+
+def _shell_ratio(pk, nm, expected, lo, hi):
+    return float(np.sum(pk[lo:hi] * nm[lo:hi]) / np.sum(expected[lo:hi] * nm[lo:hi]))
+
+
+@pytest.mark.parametrize("spec", ["power_law", "eisenstein_hu"])
+def test_oracle_ics_recover_input_spectrum(spec):
+    """P(k) of the oracle's ICs over shells 1..n/4 against the linear
+    expectation: about 1300 independent modes, 3 % scatter, held to 10 %."""
+    n, box = 32, 1.0
+    sig = _sig_pl(n) if spec == "power_law" else _sig_eh(n)
+    pos, _ = ico.zeldovich(n, box, sig, seed=42)
+    _, pk, nm = pko.power_spectrum(pos, np.full(n ** 3, 1.0 / n ** 3), box, n)
+    assert abs(_shell_ratio(pk, nm, _pk_expected(n, box, sig), 1, n // 4) - 1.0) < 0.10
+
+
+# ---- the C ABI on the host (no GPU) -----------------------------------------------
+def test_cabi_sigma_and_factors_match_oracle():
+    import treepm
+    x = np.array([0.0, 1.0, 1.5, 3.0, 7.2, 20.0, 27.7])
+    s, fac = treepm.zeldovich_sigma(x, 32)
+    ref = ico.sigma_of_n(x, 32, "power_law", 1e-4, -2.0)
+    np.testing.assert_allclose(s, ref, rtol=1e-13, atol=0.0)
+    assert fac == (1e-4, 1.0, 1.0)
+    kw = dict(transfer="eisenstein_hu", sigma8=0.8, omega_m=0.315, omega_lambda=OMEGA_L, omega_b=0.049, h=0.674,
+              box_size_mpc_h=100.0, spectral_index=0.965, cosmology=True, a_init=A_INIT, h0=H0,
+              rescale_to_a_init=True)
+    s, fac = treepm.zeldovich_sigma(x, 32, **kw)
+    np.testing.assert_allclose(s, ico.sigma_of_n(x, 32, "eisenstein_hu", 0.0, 0.965, **EH), rtol=1e-12, atol=0.0)
+    amp = ico.amplitude_for_sigma8(0.8, 0.965, *P18)
+    s_ref = ico.growth_d(A_INIT, 0.315, OMEGA_L) / ico.growth_d(1.0, 0.315, OMEGA_L)
+    np.testing.assert_allclose(fac, (amp, _vel_factor(), s_ref), rtol=1e-12)
+
+
+def test_cabi_rejects_bad_configurations():
+    import treepm
+    with pytest.raises(treepm.TreePmError):
+        treepm.zeldovich_sigma([1.0], 24)  # not a power of two
+    with pytest.raises(treepm.TreePmError):
+        treepm.zeldovich_sigma([1.0], 32, transfer="eisenstein_hu", box_size_mpc_h=0.0)
+    with pytest.raises(ValueError):
+        treepm.zeldovich_sigma([1.0], 32, transfer="tabulated")
+
+
+# ---- the device generator ---------------------------------------------------------
+def _device_ics(n, box, grid, seed, **cfg):
+    import treepm
+    solver = treepm.TreePmSolver(grid, box, r_split=2.5 * box / grid)
+    count = solver.set_particles_zeldovich(n, seed, **cfg)
+    pos, vel, _ = solver.get_state(count, acc=False)
+    return solver, pos, vel
+
+
+def _min_image(d, box):
+    return d - box * np.round(d / box)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["power_law", "eisenstein_hu_rescaled"])
+def test_device_matches_oracle_particle_by_particle(case):
+    n, box, seed = 32, 1.0, 42
+    if case == "power_law":  # amplitude for rms(Psi) = 0.1 cell
+        cfg = dict(amplitude=6.5e4, spectral_index=-2.0)
+        sig, vf, scale = _sig_pl(n, 6.5e4, -2.0), 1.0, 1.0
+    else:
+        cfg = dict(transfer="eisenstein_hu", sigma8=0.8, omega_m=0.315, omega_lambda=OMEGA_L, omega_b=0.049,
+                   h=0.674, box_size_mpc_h=100.0, spectral_index=0.965, cosmology=True, a_init=A_INIT, h0=H0,
+                   rescale_to_a_init=True)
+        sig, vf = _sig_eh(n), _vel_factor()
+        scale = ico.growth_d(A_INIT, 0.315, OMEGA_L) / ico.growth_d(1.0, 0.315, OMEGA_L)
+    _, pos, vel = _device_ics(n, box, 32, seed, **cfg)
+    ref_pos, ref_mom = ico.zeldovich(n, box, sig, seed=seed, vel_factor=vf, scale=scale)
+    psi_rms = math.sqrt(np.mean(np.sum(ref_mom * ref_mom, 1))) / vf
+    dpos = _min_image(pos - ref_pos, box)
+    assert np.max(np.abs(dpos)) < 1e-5 * psi_rms + 2.0 ** -31 * box
+    p_rms = psi_rms * vf
+    assert np.max(np.abs(vel - ref_mom)) < 1e-5 * p_rms
+    assert np.all((pos >= 0.0) & (pos < box))
+
+
+@pytest.mark.gpu
+def test_device_ics_statistics_at_128():
+    """n = 128 (2.1M particles, rms(Psi) = 0.05 cell): zero mean displacement,
+    rms(Psi) against the ensemble expectation (n_s = +1 spreads the variance
+    over ~10^6 modes: 0.03 % off over two oracle seeds, held to 2 %), and P(k)
+    of the device ICs through the device estimator against the linear
+    expectation in shells 1..32 (0.3 % off on the oracle, held to 4 %)."""
+    import treepm
+    n, box = 128, 1.0
+    solver, pos, vel = _device_ics(n, box, n, 9, amplitude=1.4e6, spectral_index=1.0)
+    g = (np.arange(n) + 0.5) * (box / n)
+    qx, qy, qz = np.meshgrid(g, g, g, indexing="ij")
+    q = np.stack([qx, qy, qz], -1).reshape(-1, 3)
+    psi = _min_image(pos - q, box)
+    sig = _sig_pl(n, 1.4e6, 1.0)
+    expected = math.sqrt(ico.expected_psi2(n, box, sig))
+    rms = math.sqrt(np.mean(np.sum(psi * psi, 1)))
+    assert abs(rms / expected - 1.0) < 0.02
+    assert np.max(np.abs(psi.mean(0))) < 1e-5 * rms + 2.0 ** -32 * box
+    np.testing.assert_allclose(vel, psi, rtol=0, atol=1e-5 * rms + 2.0 ** -31 * box)  # H0 = 1, a = 1, f = 1
+    k, pk, nm = solver.power_spectrum()
+    full_pk, full_nm = np.zeros(n // 2), np.zeros(n // 2, dtype=np.int64)
+    idx = np.rint(k / (2 * np.pi / box) - 1).astype(np.int64)
+    full_pk[idx], full_nm[idx] = pk, nm
+    assert abs(_shell_ratio(full_pk, full_nm, _pk_expected(n, box, sig), 1, n // 4) - 1.0) < 0.04
+    assert treepm.power_spectrum(pos, np.full(n ** 3, 1.0 / n ** 3), box, n)[1].shape == pk.shape
+
+
+@pytest.mark.gpu
+def test_device_ics_feed_the_solver():
+    """ICs written on the device give the same forces as the same particles
+    handed over through set_particles (box 1: the fixed-point round trip is
+    exact), and the handle steps from them."""
+    import treepm
+    n, box, grid = 32, 1.0, 32
+    solver, pos, vel = _device_ics(n, box, grid, 5, amplitude=9e4, spectral_index=-1.0)  # rms(Psi) 0.2 cell
+    solver.compute_forces(1e-6, 1.0)
+    _, _, acc = solver.get_state(n ** 3, pos=False, vel=False)
+    other = treepm.TreePmSolver(grid, box, r_split=2.5 * box / grid)
+    other.set_particles(pos, np.full(n ** 3, 1.0 / n ** 3), vel)
+    other.compute_forces(1e-6, 1.0)
+    _, _, acc2 = other.get_state(n ** 3, pos=False, vel=False)
+    np.testing.assert_allclose(acc, acc2, rtol=0, atol=1e-6 * np.sqrt(np.mean(acc2 ** 2)))
+    solver.kdk_step(1e-3, 2e-3, 1e-3, 1e-6, 1.0)
+    p2, _, _ = solver.get_state(n ** 3, vel=False, acc=False)
+    assert np.all(np.isfinite(p2))
+
+
+@pytest.mark.gpu
+def test_device_rejects_bad_sizes():
+    import treepm
+    solver = treepm.TreePmSolver(16, 1.0, r_split=0.1)
+    with pytest.raises(treepm.TreePmError):
+        solver.set_particles_zeldovich(24)
+    with pytest.raises(treepm.TreePmError):
+        solver.set_particles_zeldovich(2)
