@@ -93,8 +93,15 @@ __device__ __forceinline__ double gaussian_std(uint64_t seed) {
 
 __device__ __forceinline__ int mode_int(int j, int n) { return j <= n / 2 ? j : j - n; }
 
+// Which field of delta the mode kernel writes (three spectral components):
+// PSI1  i n_a / |n|^2 delta                   (ic_zeldovich.rs:541-585)
+// DIAG  -n_a^2 / |n|^2 delta, a = x, y, z      (ic_2lpt.rs:86-140, phi_aa)
+// OFF   -n_a n_b / |n|^2 delta, ab = xy, xz, yz (phi_ab)
+enum IcField { IC_PSI1 = 0, IC_DIAG = 1, IC_OFF = 2 };
+
+// delta(k) regenerated per call from the mode seeds (cheaper than keeping it).
 __global__ void k_ic_modes(int n, int nh, uint64_t seed, IcSpectrum sp, float2* __restrict__ spec3,
-                           int64_t comp_stride) {
+                           int64_t comp_stride, int field) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t total = (int64_t)n * n * nh;
   if (i >= total) return;
@@ -120,31 +127,97 @@ __global__ void k_ic_modes(int n, int nh, uint64_t seed, IcSpectrum sp, float2* 
     double re = sig * gaussian_std(ms), im = sig * gaussian_std(fmix64(ms ^ 0x9E3779B97F4A7C15ull));
     if (twin) im = -im;
     const double inv_n2 = 1.0 / n2;
-    const int na[3] = {nx, ny, nz};
+    const double na[3] = {(double)nx, (double)ny, (double)nz};
+    if (field == IC_PSI1) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c)  // i n_a / |n|^2 (re + i im)
-      out[c] = make_float2((float)(-na[c] * im * inv_n2), (float)(na[c] * re * inv_n2));
+      for (int c = 0; c < 3; ++c)  // i n_a / |n|^2 (re + i im)
+        out[c] = make_float2((float)(-na[c] * im * inv_n2), (float)(na[c] * re * inv_n2));
+    } else {
+      const int a0[3] = {0, 0, 1}, b0[3] = {1, 2, 2};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double f = field == IC_DIAG ? -na[c] * na[c] * inv_n2 : -na[a0[c]] * na[b0[c]] * inv_n2;
+        out[c] = make_float2((float)(f * re), (float)(f * im));
+      }
+    }
   }
   for (int c = 0; c < 3; ++c) spec3[c * comp_stride + i] = out[c];
 }
 
-__global__ void k_ic_particles(int n, double box, double psi_scale, double vel_factor, const float* __restrict__ psi,
-                               int64_t n3, Particles p) {
+// The 2LPT source (ic_2lpt.rs:146-165) from unnormalised inverse transforms of
+// phi_ab (scaled by 1/n^3 here): the diagonal pass sets rho to
+// xx yy + yy zz + zz xx, the off-diagonal pass subtracts xy^2 + xz^2 + yz^2.
+__global__ void k_ic_source(const float* __restrict__ f, float* __restrict__ rho, int64_t n3, float inv_n3,
+                            int off_diagonal) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  const float a = f[i] * inv_n3, b = f[n3 + i] * inv_n3, c = f[2 * n3 + i] * inv_n3;
+  if (!off_diagonal)
+    rho[i] = fmaf(a, b, fmaf(b, c, c * a));
+  else
+    rho[i] -= fmaf(a, a, fmaf(b, b, c * c));
+}
+
+// Psi2_a(k) = -i n_a / |n|^2 S(k), zero at DC and on the Nyquist planes
+// (ic_2lpt.rs:181-240).
+__global__ void k_ic_psi2_modes(const float2* __restrict__ src, int n, int nh, float2* __restrict__ spec3,
+                                int64_t comp_stride) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)n * n * nh;
+  if (i >= total) return;
+  const int kx = (int)(i % nh), y = (int)((i / nh) % n), z = (int)(i / ((int64_t)n * nh));
+  const int nx = kx, ny = mode_int(y, n), nz = mode_int(z, n), half = n / 2;
+  const float n2 = (float)(nx * nx + ny * ny + nz * nz);
+  float2 out[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  if (n2 > 0.f && nx != half && abs(ny) != half && abs(nz) != half) {
+    const float2 sk = src[i];
+    const float na[3] = {(float)nx, (float)ny, (float)nz};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] = make_float2(na[c] * sk.y / n2, -na[c] * sk.x / n2);
+  }
+  for (int c = 0; c < 3; ++c) spec3[c * comp_stride + i] = out[c];
+}
+
+__device__ __forceinline__ void lattice_of(int64_t gid, int n, int64_t* node, int ii[3]) {
+  ii[0] = (int)(gid / ((int64_t)n * n));
+  ii[1] = (int)((gid / n) % n);
+  ii[2] = (int)(gid % n);
+  *node = ((int64_t)ii[2] * n + ii[1]) * n + ii[0];  // the mesh's [z][y][x] layout
+}
+
+// Keep the scaled Psi2 of each particle in its velocity slots until the
+// Psi1 pass writes the final state.
+__global__ void k_ic_stash_psi2(int n, double psi2_scale, const float* __restrict__ psi2, int64_t n3, Particles p) {
   const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (gid >= n3) return;
-  const int ix = (int)(gid / ((int64_t)n * n)), iy = (int)((gid / n) % n), iz = (int)(gid % n);
-  const int64_t node = ((int64_t)iz * n + iy) * n + ix;  // the mesh's [z][y][x] layout
+  int64_t node;
+  int ii[3];
+  lattice_of(gid, n, &node, ii);
+  p.vx[gid] = (float)(psi2[node] * psi2_scale);
+  p.vy[gid] = (float)(psi2[n3 + node] * psi2_scale);
+  p.vz[gid] = (float)(psi2[2 * n3 + node] * psi2_scale);
+}
+
+// Lattice position at the cell centre + Psi1 (+ D2/D1^2 Psi2), wrapped;
+// momentum vel1 Psi1 (+ vel2 Psi2) (ic_zeldovich.rs:726-757, ic_2lpt.rs:520-548).
+__global__ void k_ic_particles(int n, double box, double psi_scale, double vel1, double d21, double vel2, int lpt2,
+                               const float* __restrict__ psi, int64_t n3, Particles p) {
+  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gid >= n3) return;
+  int64_t node;
+  int ii[3];
+  lattice_of(gid, n, &node, ii);
   const double d = box / n;
-  const int ii[3] = {ix, iy, iz};
+  const float s2v[3] = {lpt2 ? p.vx[gid] : 0.f, lpt2 ? p.vy[gid] : 0.f, lpt2 ? p.vz[gid] : 0.f};
   uint32_t q[3];
   float v[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const double s = (double)psi[c * n3 + node] * psi_scale;
-    double u = ((ii[c] + 0.5) * d + s) / box;
+    const double s1 = (double)psi[c * n3 + node] * psi_scale, s2 = (double)s2v[c];
+    double u = ((ii[c] + 0.5) * d + s1 + d21 * s2) / box;
     u = u - floor(u);
     q[c] = (uint32_t)((unsigned long long)llrint(u * TWO32) & 0xFFFFFFFFull);
-    v[c] = (float)(s * vel_factor);
+    v[c] = (float)(s1 * vel1 + s2 * vel2);
   }
   p.qx[gid] = q[0];
   p.qy[gid] = q[1];
@@ -180,10 +253,19 @@ double sigma_sq_unit(double r, double n_s, double om, double ob, double h) {
 
 }  // namespace
 
-// Spectrum, growth and momentum factors of a configuration (host).
-bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, double* vel_factor, double* scale) {
+// Growth and momentum factors of a configuration.
+struct IcFactors {
+  double vel1;   // a^2 f1 H
+  double scale;  // D(a_init)/D(1) when rescaled, else 1
+  double d21;    // D2/D1^2 = -3/7 Omega_m(a)^(-1/143)
+  double vel2;   // a^2 f2 H D2/D1^2, f2 = 2 Omega_m(a)^(6/11)
+};
+
+// Spectrum and factors of a configuration (host); false when it is invalid.
+bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, IcFactors* fa) {
   if (!c || c->n_side < 4 || c->n_side > 1024 || (c->n_side & (c->n_side - 1)) != 0) return false;
   if (c->transfer != 0 && c->transfer != 1) return false;
+  if (c->use_2lpt != 0 && c->use_2lpt != 1) return false;
   if (c->transfer == 1 && !(c->omega_m > 0.0 && c->omega_b >= 0.0 && c->h > 0.0 && c->box_size_mpc_h > 0.0))
     return false;
   const double n3 = (double)c->n_side * c->n_side * c->n_side;
@@ -199,7 +281,8 @@ bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, double* vel_facto
     const double v = sigma_sq_unit(8.0, c->spectral_index, c->omega_m, c->omega_b, c->h);
     sp->amp = v > 0.0 ? c->sigma8 / std::sqrt(v) : c->sigma8;
   }
-  // cosmology.rs:509-520 (H, LCDM), :598-610 (f), :650-666 / :736-742 (CPT92 ratio)
+  // cosmology.rs:509-520 (H, LCDM), :598-610 (f), :650-666 / :736-742 (CPT92
+  // ratio); without cosmology a = 1, Omega_m = 1, Omega_L = 0, H = H0
   double a = 1.0, om = 1.0, ol = 0.0;
   if (c->cosmology) {
     a = c->a_init;
@@ -208,10 +291,14 @@ bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, double* vel_facto
   }
   if (!(a > 0.0) || !(c->h0 > 0.0)) return false;
   const double hh = c->h0 * std::sqrt(std::max(om / (a * a * a) + ol, 0.0));
-  const double om_a = om / (a * a * a) / ((hh / c->h0) * (hh / c->h0));
-  const double f = std::pow(std::max(om_a, 0.0), 0.55);
-  *vel_factor = a * a * f * hh;
-  *scale = 1.0;
+  const double om_a = std::max(om / (a * a * a) / ((hh / c->h0) * (hh / c->h0)), 0.0);
+  const double f1 = std::pow(om_a, 0.55);
+  fa->vel1 = a * a * f1 * hh;
+  // ic_2lpt.rs:420-446 (Bouchet et al. 1995 fits)
+  const double f2 = 2.0 * std::pow(om_a, 6.0 / 11.0);
+  fa->d21 = -3.0 / 7.0 * std::pow(om_a, -1.0 / 143.0);
+  fa->vel2 = a * a * f2 * hh * fa->d21;
+  fa->scale = 1.0;
   if (c->rescale_to_a_init && c->cosmology) {
     auto growth = [&](double aa) {
       const double a3 = aa * aa * aa, den = om + ol * a3;
@@ -221,20 +308,22 @@ bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, double* vel_facto
       return br <= 0.0 ? aa : aa * 2.5 * oma / br;
     };
     const double d1 = growth(1.0);
-    *scale = d1 == 0.0 ? 1.0 : growth(a) / d1;
+    fa->scale = d1 == 0.0 ? 1.0 : growth(a) / d1;
   }
   return true;
 }
 
-// `mesh` is a plan of the solver whose spectrum and force buffers may be
-// overwritten; it is used when its mesh is the IC lattice (no allocation),
-// otherwise a temporary plan of n_side^3 is made and freed.
+// `mesh` is a plan of the solver whose buffers may be overwritten; it is used
+// when its mesh is the IC lattice (no allocation), otherwise a temporary plan
+// of n_side^3 is made and freed.  Sequence: [2LPT: phi_aa -> source, phi_ab ->
+// source, forward transform, Psi2 -> velocity slots], then Psi1 -> particles.
 void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cudaStream_t s, PmPlan* mesh) {
   IcSpectrum sp{};
-  double vel = 0.0, scale = 1.0;
-  if (!zeldovich_factors(c, &sp, &vel, &scale)) throw Error(TPM_ERR_INVALID_ARGUMENT, "bad Zel'dovich configuration");
+  IcFactors fa{};
+  if (!zeldovich_factors(c, &sp, &fa)) throw Error(TPM_ERR_INVALID_ARGUMENT, "bad Zel'dovich configuration");
   const int n = c->n_side;
-  const bool reuse = mesh && mesh->nm == n && mesh->ncomp >= 3 && mesh->spec3 && mesh->force;
+  const bool reuse = mesh && mesh->nm == n && mesh->ncomp >= 3 && mesh->spec3 && mesh->force && mesh->rho &&
+                     mesh->spec;
   PmPlan temp;
   PmPlan& plan = reuse ? *mesh : temp;
   try {
@@ -244,13 +333,29 @@ void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cu
       pm_plan_init(temp, n, box, 0.0, 0u, dev);
     }
     const int64_t nh = n / 2 + 1, plane = (int64_t)n * n * nh, n3 = (int64_t)n * n * n;
-    const int64_t comp_stride = (int64_t)n * n * nh;  // spec3 holds ncomp planes of this size
-    k_ic_modes<<<grid_for(plane, 256, 1ll << 30), 256, 0, s>>>(n, (int)nh, c->seed, sp, plan.spec3, comp_stride);
+    const unsigned gm = grid_for(plane, 256, 1ll << 30), gp = grid_for(n3, 256, 1ll << 30);
+    const double cell_over_n3 = (box / n) / (double)n3;  // rustfft's inverse is unnormalised
+    if (c->use_2lpt) {
+      const float inv_n3 = (float)(1.0 / (double)n3);
+      for (int off = 0; off < 2; ++off) {
+        k_ic_modes<<<gm, 256, 0, s>>>(n, (int)nh, c->seed, sp, plan.spec3, plane, off ? IC_OFF : IC_DIAG);
+        TPM_LAUNCH_CHECK();
+        pm_inverse_components(plan, 3, s);
+        k_ic_source<<<gp, 256, 0, s>>>(plan.force, plan.rho, n3, inv_n3, off);
+        TPM_LAUNCH_CHECK();
+      }
+      pm_forward_real(plan, s);
+      k_ic_psi2_modes<<<gm, 256, 0, s>>>(plan.spec, n, (int)nh, plan.spec3, plane);
+      TPM_LAUNCH_CHECK();
+      pm_inverse_components(plan, 3, s);
+      k_ic_stash_psi2<<<gp, 256, 0, s>>>(n, cell_over_n3 * fa.scale * fa.scale, plan.force, n3, out);
+      TPM_LAUNCH_CHECK();
+    }
+    k_ic_modes<<<gm, 256, 0, s>>>(n, (int)nh, c->seed, sp, plan.spec3, plane, IC_PSI1);
     TPM_LAUNCH_CHECK();
     pm_inverse_components(plan, 3, s);
-    // rustfft's inverse is unnormalised: Psi = Re(ifft) / n^3 * cell (ic_zeldovich.rs:602-614)
-    const double psi_scale = (box / n) / (double)n3 * scale;
-    k_ic_particles<<<grid_for(n3, 256, 1ll << 30), 256, 0, s>>>(n, box, psi_scale, vel, plan.force, n3, out);
+    k_ic_particles<<<gp, 256, 0, s>>>(n, box, cell_over_n3 * fa.scale, fa.vel1, fa.d21, fa.vel2, c->use_2lpt,
+                                      plan.force, n3, out);
     TPM_LAUNCH_CHECK();
     TPM_CUDA(cudaStreamSynchronize(s));
   } catch (...) {
@@ -265,14 +370,16 @@ void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cu
 extern "C" int tpm_zeldovich_sigma(const tpm_zeldovich* c, const double* n_abs, int64_t count, double* sigma,
                                    double* factors) {
   tpm::IcSpectrum sp{};
-  double vel = 0.0, scale = 1.0;
-  if (!tpm::zeldovich_factors(c, &sp, &vel, &scale) || count < 0 || (count > 0 && (!n_abs || !sigma)))
+  tpm::IcFactors fa{};
+  if (!tpm::zeldovich_factors(c, &sp, &fa) || count < 0 || (count > 0 && (!n_abs || !sigma)))
     return TPM_ERR_INVALID_ARGUMENT;
   for (int64_t i = 0; i < count; ++i) sigma[i] = tpm::ic_sigma(sp, n_abs[i]);
   if (factors) {
     factors[0] = sp.amp;
-    factors[1] = vel;
-    factors[2] = scale;
+    factors[1] = fa.vel1;
+    factors[2] = fa.scale;
+    factors[3] = fa.d21;
+    factors[4] = fa.vel2;
   }
   return TPM_OK;
 }

@@ -674,6 +674,23 @@ void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uin
   TPM_LAUNCH_CHECK();
 }
 
+void pm_forward_real(const PmPlan& p, cudaStream_t s) {
+  const int nm = p.nm, nh = p.nh, logn = p.logn;
+  const int rows = rows_for(nm), tx = tx_for(nm);
+  const int64_t nrows = (int64_t)nm * nm;
+  const size_t sm_x = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)rows * nm);
+  const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
+  TPM_CUDA(cudaFuncSetAttribute(k_fft_z_c2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  const int nblk_x = (int)((nrows + rows - 1) / rows);
+  const int ntx = (nh + tx - 1) / tx;
+  k_fft_x_r2c<<<nblk_x, 256, sm_x, s>>>(p.rho, p.spec, nm, logn, nh, rows, nrows, p.twiddle);
+  TPM_LAUNCH_CHECK();
+  k_fft_y<<<dim3(ntx, nm, 1), 256, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
+  TPM_LAUNCH_CHECK();
+  k_fft_z_c2c<<<dim3(ntx, nm, 1), 256, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
+  TPM_LAUNCH_CHECK();
+}
+
 void pm_inverse_components(const PmPlan& p, int ncomp, cudaStream_t s) {
   const int nm = p.nm, nh = p.nh, logn = p.logn;
   const int rows = rows_for(nm), tx = tx_for(nm);

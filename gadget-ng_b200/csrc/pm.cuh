@@ -56,6 +56,10 @@ void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uin
 
 struct Particles;
 
+// Unnormalised forward 3D transform of the real field p.rho into the half
+// spectrum p.spec ([z][y][kx], kx <= nm/2).
+void pm_forward_real(const PmPlan& p, cudaStream_t s);
+
 // Unnormalised inverse 3D transforms of the first ncomp half spectra in
 // spec3 ([z][y][kx] each) into the real grids force[c * nm^3 + (z nm + y) nm + x].
 void pm_inverse_components(const PmPlan& p, int ncomp, cudaStream_t s);

@@ -68,6 +68,8 @@ class TpmZeldovich(C.Structure):
         ("h0", C.c_double),
         ("cosmology", C.c_int32),
         ("rescale_to_a_init", C.c_int32),
+        ("use_2lpt", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

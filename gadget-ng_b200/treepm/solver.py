@@ -279,7 +279,7 @@ def zeldovich_config(n_side: int, seed: int = 42, *, transfer: str = "power_law"
                      spectral_index: float = -2.0, sigma8: float = 0.0, omega_m: float = 1.0,
                      omega_lambda: float = 0.0, omega_b: float = 0.049, h: float = 0.674,
                      box_size_mpc_h: float = 0.0, a_init: float = 1.0, h0: float = 1.0, cosmology: bool = False,
-                     rescale_to_a_init: bool = False) -> "TpmZeldovich":
+                     rescale_to_a_init: bool = False, use_2lpt: bool = False) -> "TpmZeldovich":
     """IcKind::Zeldovich fields with the defaults of
     crates/gadget-ng-core/src/config/sections/simulation_ic.rs:285-303 (seed
     42, amplitude 1e-4, spectral index -2, omega_b 0.049, h 0.674); transfer
@@ -291,16 +291,18 @@ def zeldovich_config(n_side: int, seed: int = 42, *, transfer: str = "power_law"
                         spectral_index=float(spectral_index), sigma8=float(sigma8), omega_m=float(omega_m),
                         omega_lambda=float(omega_lambda), omega_b=float(omega_b), h=float(h),
                         box_size_mpc_h=float(box_size_mpc_h), a_init=float(a_init), h0=float(h0),
-                        cosmology=int(bool(cosmology)), rescale_to_a_init=int(bool(rescale_to_a_init)))
+                        cosmology=int(bool(cosmology)), rescale_to_a_init=int(bool(rescale_to_a_init)),
+                        use_2lpt=int(bool(use_2lpt)), reserved=0)
 
 
 def zeldovich_sigma(n_abs, n_side: int, **cfg):
-    """sigma(|n|) of the IC spectrum and the factors (A, a^2 f H, D(a)/D(1))."""
+    """sigma(|n|) of the IC spectrum and the factors (A, a^2 f1 H, D(a)/D(1),
+    D2/D1^2, a^2 f2 H D2/D1^2)."""
     c = zeldovich_config(n_side, 0, **cfg)
     x = np.ascontiguousarray(n_abs, dtype=np.float64).reshape(-1)
-    sig, fac = np.empty_like(x), np.empty(3)
+    sig, fac = np.empty_like(x), np.empty(5)
     check(None, load().tpm_zeldovich_sigma(C.byref(c), _ptr(x), x.shape[0], _ptr(sig), _ptr(fac)))
-    return sig, (float(fac[0]), float(fac[1]), float(fac[2]))
+    return sig, tuple(float(v) for v in fac)
 
 
 def drift_kick_factors(omega_m: float, omega_lambda: float, h0: float, a0: float, dt: float):

@@ -249,7 +249,10 @@ int tpm_fp32_peak(int device, double* tflops);
  * (transfer 0, power law) or A k^(n_s/2) T_EH(k) / sqrt(N^3) (transfer 1,
  * Eisenstein-Hu no-wiggle, k = 2 pi |n| h / box_size_mpc_h, A from sigma8 when
  * sigma8 > 0); momenta a^2 f(a) H(a) Psi (cosmology != 0) or H0 Psi (a = 1,
- * f = 1).  rescale_to_a_init multiplies Psi by D(a_init)/D(1) (CPT92).  Each
+ * f = 1).  rescale_to_a_init multiplies Psi by D(a_init)/D(1) (CPT92).  With
+ * use_2lpt, x = q + Psi1 + (D2/D1^2) Psi2 and p = a^2 H (f1 Psi1 + f2 (D2/D1^2)
+ * Psi2), Psi2 = -i n / |n|^2 S(k) from the sum of the 2x2 minors of phi_ab
+ * (Psi2 scaled by the rescale squared).  Each
  * mode is seeded by the reference's mode_seed (murmur3 fmix64 of seed and the
  * packed mode index); the two uniforms of its Box-Muller Gaussians come from
  * SplitMix64 seeded there instead of the reference's StdRng, so realisations
@@ -268,10 +271,13 @@ typedef struct tpm_zeldovich {
   double h0;              /* H0 in internal time units */
   int32_t cosmology;      /* 0: a = 1, f = 1, H = h0 */
   int32_t rescale_to_a_init;
+  int32_t use_2lpt;       /* 1: second-order displacements (ic_2lpt.rs:386-550) */
+  int32_t reserved;       /* 0 */
 } tpm_zeldovich;
 int tpm_set_particles_zeldovich(tpm_handle* h, const tpm_zeldovich* cfg);
-/* Host evaluation of sigma(|n|) for count values and the factors
- * [A, momentum factor a^2 f H, growth rescale] (factors may be NULL). */
+/* Host evaluation of sigma(|n|) for count values and the five factors
+ * [A, a^2 f1 H, growth rescale D(a)/D(1), D2/D1^2, a^2 f2 H D2/D1^2]
+ * (factors may be NULL). */
 int tpm_zeldovich_sigma(const tpm_zeldovich* cfg, const double* n_abs, int64_t count, double* sigma, double* factors);
 
 /* ---- power spectrum (in-situ analysis) ----------------------------------------

@@ -209,3 +209,66 @@ def zeldovich(n, box, sig, seed=0, vel_factor=1.0, scale=1.0):
     pos = np.stack([(qx + psi[0]) % box, (qy + psi[1]) % box, (qz + psi[2]) % box], -1).reshape(-1, 3)
     mom = np.stack(psi, -1).reshape(-1, 3) * vel_factor
     return pos, mom
+
+
+# ---- second order (crates/gadget-ng-core/src/ic_2lpt.rs) -------------------------
+def phi_second_derivatives(delta, n):
+    """phi_ab = Re(IFFT(-n_a n_b / |n|^2 delta)) / n^3 for ab = xx, yy, zz, xy,
+    xz, yz (ic_2lpt.rs:86-140)."""
+    (nx, ny, nz), n2, _ = _modes(n)
+    comps = (nx, ny, nz)
+    out = []
+    for a, b in ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)):
+        with np.errstate(invalid="ignore", divide="ignore"):
+            ph = np.where(n2 > 0, -comps[a] * comps[b] / n2 * delta, 0.0)
+        out.append(np.fft.ifftn(ph).real)  # ifftn divides by n^3, as the reference's ifft_norm
+    return out
+
+
+def source_2lpt(d):
+    """S = (xx yy - xy^2) + (yy zz - yz^2) + (zz xx - xz^2) (ic_2lpt.rs:146-165)."""
+    xx, yy, zz, xy, xz, yz = d
+    return (xx * yy - xy * xy) + (yy * zz - yz * yz) + (zz * xx - xz * xz)
+
+
+def source_to_psi2(s, n, box):
+    """Psi2_a = Re(IFFT(-i n_a / |n|^2 FFT(S))) / n^3 * cell, zero at DC and on
+    the Nyquist planes (ic_2lpt.rs:181-240)."""
+    (nx, ny, nz), n2, keep = _modes(n)
+    sk = np.fft.fftn(s)
+    d = box / n
+    out = []
+    for comp in (nx, ny, nz):
+        with np.errstate(invalid="ignore", divide="ignore"):
+            ph = np.where(keep, -1j * comp / n2 * sk, 0.0)
+        out.append(np.fft.ifftn(ph).real * d)
+    return out
+
+
+def lpt_factors(a_init=1.0, omega_m=1.0, omega_l=0.0, h0=1.0, cosmology=False):
+    """(a^2 f1 H, D2/D1^2, a^2 f2 H D2/D1^2) of ic_2lpt.rs:404-446; without
+    cosmology a = 1, Omega_m = 1, Omega_L = 0."""
+    a, om, ol = (a_init, omega_m, omega_l) if cosmology else (1.0, 1.0, 0.0)
+    hh = hubble(a, om, ol, h0)
+    om_a = max(om / a ** 3 / (hh / h0) ** 2, 0.0)
+    f1 = om_a ** 0.55
+    f2 = 2.0 * om_a ** (6.0 / 11.0)
+    d21 = -3.0 / 7.0 * om_a ** (-1.0 / 143.0)
+    return a * a * f1 * hh, d21, a * a * f2 * hh * d21
+
+
+def zeldovich_2lpt(n, box, sig, seed=0, vel1=1.0, d21=-3.0 / 7.0, vel2=-6.0 / 7.0, scale=1.0):
+    """zeldovich_2lpt_ics (ic_2lpt.rs:386-550) on the realisation of `seed`:
+    x = q + scale Psi1 + d21 scale^2 Psi2 wrapped, p = vel1 scale Psi1 + vel2
+    scale^2 Psi2.  Returns positions, momenta and the scaled Psi2."""
+    delta = delta_kspace(n, seed, sig)
+    psi1, _ = displacement(delta, n, box)
+    psi2 = source_to_psi2(source_2lpt(phi_second_derivatives(delta, n)), n, box)
+    d = box / n
+    g = (np.arange(n) + 0.5) * d
+    qx, qy, qz = np.meshgrid(g, g, g, indexing="ij")
+    s1 = [p * scale for p in psi1]
+    s2 = [p * scale * scale for p in psi2]
+    pos = np.stack([(q + a + d21 * b) % box for q, a, b in zip((qx, qy, qz), s1, s2)], -1).reshape(-1, 3)
+    mom = np.stack([vel1 * a + vel2 * b for a, b in zip(s1, s2)], -1).reshape(-1, 3)
+    return pos, mom, np.stack(s2, -1).reshape(-1, 3)

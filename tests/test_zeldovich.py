@@ -174,6 +174,85 @@ def test_oracle_ics_recover_input_spectrum(spec):
     assert abs(_shell_ratio(pk, nm, _pk_expected(n, box, sig), 1, n // 4) - 1.0) < 0.10
 
 
+# ---- second order, pinned by ic_2lpt.rs:560-929 and an analytic case ---------------
+def _strong_sig(n):  # ic_2lpt.rs:578-590: sigma = 1/|n|
+    nabs = _nabs(n)
+    with np.errstate(divide="ignore"):
+        return np.where(nabs > 0, 1.0 / np.where(nabs > 0, nabs, 1.0), 0.0)
+
+
+def test_oracle_2lpt_source_and_psi2_are_finite():  # ic_2lpt.rs:593-630
+    n = 8
+    delta = ico.delta_kspace(n, 42, 1e-2 * _strong_sig(n) / math.sqrt(n ** 3))
+    s = ico.source_2lpt(ico.phi_second_derivatives(delta, n))
+    assert np.all(np.isfinite(s))
+    assert all(np.all(np.isfinite(p)) for p in ico.source_to_psi2(s, n, 1.0))
+
+
+def test_oracle_psi2_matches_canonical_kspace_formula():  # ic_2lpt.rs:633-745
+    n, box = 16, 1.0
+    s = ico.source_2lpt(ico.phi_second_derivatives(ico.delta_kspace(n, 42, _strong_sig(n)), n))
+    psi2 = ico.source_to_psi2(s, n, box)
+    sk = np.fft.fftn(s)
+    (nx, ny, nz), n2, keep = ico._modes(n)
+    worst, big = 0.0, 0.0
+    for comp, p in zip((nx, ny, nz), psi2):
+        got = np.fft.fftn(p)[keep]
+        exp = (comp[keep] / n2[keep] * (box / n)) * (sk[keep].imag - 1j * sk[keep].real)
+        worst, big = max(worst, float(np.max(np.abs(got - exp)))), max(big, float(np.max(np.abs(exp))))
+    assert worst / big < 1e-10
+
+
+def test_oracle_psi2_scales_quadratically_with_delta():  # ic_2lpt.rs:836-890
+    n = 16
+    one = ico.source_to_psi2(ico.source_2lpt(ico.phi_second_derivatives(ico.delta_kspace(n, 7, _strong_sig(n)), n)),
+                             n, 1.0)
+    two = ico.source_to_psi2(
+        ico.source_2lpt(ico.phi_second_derivatives(ico.delta_kspace(n, 7, 2.0 * _strong_sig(n)), n)), n, 1.0)
+    scale = max(float(np.max(np.abs(p))) for p in one)
+    assert scale > 0.0
+    assert max(float(np.max(np.abs(b - 4.0 * a))) for a, b in zip(one, two)) < 1e-12 * scale
+
+
+def _cosines(n, waves):
+    """delta(j) = sum A cos(2 pi m.j / n) as the unnormalised spectrum."""
+    d = np.zeros((n, n, n), dtype=np.complex128)
+    for amp, m in waves:
+        d[tuple(c % n for c in m)] += amp * n ** 3 / 2
+        d[tuple(-c % n for c in m)] += amp * n ** 3 / 2
+    return d
+
+
+def test_oracle_psi2_analytic_cases():
+    """One plane wave: phi_ab has a single non-zero entry, every minor
+    vanishes, Psi2 = 0.  Waves A cos X along x (m_x) and B cos Y along y (m_y):
+    phi_xx = -A cos X, phi_yy = -B cos Y, S = AB cos X cos Y and
+    Psi2_x = cell AB m_x / (m_x^2 + m_y^2) sin X cos Y."""
+    n, box = 16, 1.0
+    s = ico.source_2lpt(ico.phi_second_derivatives(_cosines(n, [(0.3, (2, 0, 0))]), n))
+    assert float(np.max(np.abs(s))) < 1e-15
+    A, B, mx, my = 0.3, 0.2, 2, 3
+    s = ico.source_2lpt(ico.phi_second_derivatives(_cosines(n, [(A, (mx, 0, 0)), (B, (0, my, 0))]), n))
+    j = np.arange(n)
+    X, Y, _ = np.meshgrid(2 * np.pi * mx * j / n, 2 * np.pi * my * j / n, j, indexing="ij")
+    np.testing.assert_allclose(s, A * B * np.cos(X) * np.cos(Y), atol=1e-14)
+    px, py, pz = ico.source_to_psi2(s, n, box)
+    cell = box / n
+    np.testing.assert_allclose(px, cell * A * B * mx / (mx * mx + my * my) * np.sin(X) * np.cos(Y), atol=1e-15)
+    np.testing.assert_allclose(py, cell * A * B * my / (mx * mx + my * my) * np.cos(X) * np.sin(Y), atol=1e-15)
+    assert float(np.max(np.abs(pz))) < 1e-15
+
+
+def test_oracle_lpt_factors():  # ic_2lpt.rs:420-446; no cosmology: f1 = 1, f2 = 2, D2/D1^2 = -3/7
+    assert ico.lpt_factors(h0=1.0) == pytest.approx((1.0, -3.0 / 7.0, -6.0 / 7.0), rel=1e-15)
+    v1, d21, v2 = ico.lpt_factors(A_INIT, 0.315, OMEGA_L, H0, True)
+    hh = ico.hubble(A_INIT, 0.315, OMEGA_L, H0)
+    om_a = 0.315 / A_INIT ** 3 / (hh / H0) ** 2
+    assert v1 == pytest.approx(_vel_factor(), rel=1e-14)
+    assert d21 == pytest.approx(-3.0 / 7.0 * om_a ** (-1.0 / 143.0), rel=1e-14)
+    assert v2 == pytest.approx(A_INIT ** 2 * 2.0 * om_a ** (6.0 / 11.0) * hh * d21, rel=1e-14)
+
+
 # ---- the C ABI on the host (no GPU) -----------------------------------------------
 def test_cabi_sigma_and_factors_match_oracle():
     import treepm
@@ -181,7 +260,7 @@ def test_cabi_sigma_and_factors_match_oracle():
     s, fac = treepm.zeldovich_sigma(x, 32)
     ref = ico.sigma_of_n(x, 32, "power_law", 1e-4, -2.0)
     np.testing.assert_allclose(s, ref, rtol=1e-13, atol=0.0)
-    assert fac == (1e-4, 1.0, 1.0)
+    assert fac == pytest.approx((1e-4, 1.0, 1.0, -3.0 / 7.0, -6.0 / 7.0), rel=1e-15)
     kw = dict(transfer="eisenstein_hu", sigma8=0.8, omega_m=0.315, omega_lambda=OMEGA_L, omega_b=0.049, h=0.674,
               box_size_mpc_h=100.0, spectral_index=0.965, cosmology=True, a_init=A_INIT, h0=H0,
               rescale_to_a_init=True)
@@ -189,7 +268,8 @@ def test_cabi_sigma_and_factors_match_oracle():
     np.testing.assert_allclose(s, ico.sigma_of_n(x, 32, "eisenstein_hu", 0.0, 0.965, **EH), rtol=1e-12, atol=0.0)
     amp = ico.amplitude_for_sigma8(0.8, 0.965, *P18)
     s_ref = ico.growth_d(A_INIT, 0.315, OMEGA_L) / ico.growth_d(1.0, 0.315, OMEGA_L)
-    np.testing.assert_allclose(fac, (amp, _vel_factor(), s_ref), rtol=1e-12)
+    v1, d21, v2 = ico.lpt_factors(A_INIT, 0.315, OMEGA_L, H0, True)
+    np.testing.assert_allclose(fac, (amp, v1, s_ref, d21, v2), rtol=1e-12)
 
 
 def test_cabi_rejects_bad_configurations():
@@ -236,6 +316,38 @@ def test_device_matches_oracle_particle_by_particle(case):
     p_rms = psi_rms * vf
     assert np.max(np.abs(vel - ref_mom)) < 1e-5 * p_rms
     assert np.all((pos >= 0.0) & (pos < box))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["power_law", "eisenstein_hu_rescaled"])
+def test_device_2lpt_matches_oracle(case):
+    """Second order: positions and momenta against the oracle as for 1LPT, and
+    the second-order part of the momentum (2LPT minus 1LPT of the same
+    realisation, = a^2 f2 H D2/D1^2 Psi2) within 1e-3 of its rms."""
+    n, box, seed = 32, 1.0, 11
+    if case == "power_law":  # rms(Psi1) = 0.3 cell, cosmological factors at a = 0.02
+        cfg = dict(amplitude=2.0e5, spectral_index=-2.0, omega_m=0.315, omega_lambda=OMEGA_L, cosmology=True,
+                   a_init=A_INIT, h0=H0)
+        sig, scale = _sig_pl(n, 2.0e5, -2.0), 1.0
+    else:
+        cfg = dict(transfer="eisenstein_hu", sigma8=0.8, omega_m=0.315, omega_lambda=OMEGA_L, omega_b=0.049,
+                   h=0.674, box_size_mpc_h=100.0, spectral_index=0.965, cosmology=True, a_init=A_INIT, h0=H0,
+                   rescale_to_a_init=True)
+        sig = _sig_eh(n)
+        scale = ico.growth_d(A_INIT, 0.315, OMEGA_L) / ico.growth_d(1.0, 0.315, OMEGA_L)
+    v1, d21, v2 = ico.lpt_factors(A_INIT, 0.315, OMEGA_L, H0, True)
+    _, pos, vel = _device_ics(n, box, 32, seed, use_2lpt=True, **cfg)
+    _, _, vel1 = _device_ics(n, box, 32, seed, use_2lpt=False, **cfg)
+    ref_pos, ref_mom, s2 = ico.zeldovich_2lpt(n, box, sig, seed=seed, vel1=v1, d21=d21, vel2=v2, scale=scale)
+    p_rms = math.sqrt(np.mean(np.sum(ref_mom * ref_mom, 1)))
+    psi_rms = p_rms / v1
+    assert np.max(np.abs(_min_image(pos - ref_pos, box))) < 1e-5 * psi_rms + 2.0 ** -31 * box
+    assert np.max(np.abs(vel - ref_mom)) < 1e-5 * p_rms
+    if case == "power_law":
+        second = v2 * s2
+        rms2 = math.sqrt(np.mean(np.sum(second * second, 1)))
+        assert rms2 > 1e-3 * p_rms  # the second order is resolved in float32
+        assert np.max(np.abs((vel - vel1) - second)) < 1e-3 * rms2 + 2e-7 * p_rms
 
 
 @pytest.mark.gpu
