@@ -272,27 +272,62 @@ def learned_mode_report(box, mesh, phys, pos, g, targets, ref, device, plain_ms,
             "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}}
 
 
+IC_CFG = dict(transfer="eisenstein_hu", sigma8=0.8, omega_m=0.315, omega_lambda=0.685, omega_b=0.049, h=0.674,
+              box_size_mpc_h=100.0, spectral_index=0.965, cosmology=True, a_init=0.02, h0=0.1)
+
+
 def zeldovich_report(device, n_side=256, reps=3):
     """Time tpm_set_particles_zeldovich for n_side^3 particles (EH spectrum,
-    sigma_8 = 0.8, a_init = 0.02) into a solver whose PM mesh is the IC lattice
-    (no allocation inside the call): modes, three inverse transforms, particle
-    write; wall time of the synchronous call, median of `reps`."""
+    sigma_8 = 0.8, a_init = 0.02), first and second order, into a solver whose
+    PM mesh is the IC lattice (no allocation inside the call); wall time of the
+    synchronous call, median of `reps`, with CUDA-event stage times."""
     import treepm
     solver = treepm.TreePmSolver(n_side, 100.0, r_split=2.5 * 100.0 / n_side, device=device)
-    cfg = dict(transfer="eisenstein_hu", sigma8=0.8, omega_m=0.315, omega_lambda=0.685, omega_b=0.049, h=0.674,
-               box_size_mpc_h=100.0, spectral_index=0.965, cosmology=True, a_init=0.02, h0=0.1)
-    solver.set_particles_zeldovich(n_side, 1, **cfg)  # warm
-    ts = []
-    for r in range(reps):
-        c0 = time.perf_counter()
-        solver.set_particles_zeldovich(n_side, 2 + r, **cfg)
-        ts.append(time.perf_counter() - c0)
+    out = {"particles": n_side ** 3, "spectrum": "Eisenstein-Hu no-wiggle, sigma_8 0.8, n_s 0.965, a_init 0.02",
+           "path": "tpm_set_particles_zeldovich (ic_zeldovich.rs zeldovich_ics / ic_2lpt.rs zeldovich_2lpt_ics)"}
+    for order, lpt2 in (("1lpt", False), ("2lpt", True)):
+        solver.set_particles_zeldovich(n_side, 1, use_2lpt=lpt2, **IC_CFG)  # warm
+        ts = []
+        for r in range(reps):
+            c0 = time.perf_counter()
+            solver.set_particles_zeldovich(n_side, 2 + r, use_2lpt=lpt2, **IC_CFG)
+            ts.append(time.perf_counter() - c0)
+        ms = 1e3 * float(np.median(ts))
+        out[order] = {"ms": ms, "particles_per_s": n_side ** 3 / (ms * 1e-3)}
     solver.close()
-    ms = 1e3 * float(np.median(ts))
-    n3 = n_side ** 3
-    return {"ms": ms, "particles": n3, "particles_per_s": n3 / (ms * 1e-3),
-            "spectrum": "Eisenstein-Hu no-wiggle, sigma_8 0.8, n_s 0.965, a_init 0.02",
-            "path": "tpm_set_particles_zeldovich (ic_zeldovich.rs zeldovich_ics): modes, 3 inverse FFTs, particle write"}
+    return out
+
+
+def zeldovich_cpu_sample(n_side=64):
+    """The numpy restatement (float64, pocketfft) of the same ICs, first and
+    second order, on n_side^3 particles: particles/s of one call each."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ic_oracle as ico
+    f = ico.mode_int(n_side)
+    nx, ny, nz = np.meshgrid(f, f, f, indexing="ij")
+    nabs = np.sqrt(nx * nx + ny * ny + nz * nz)
+    c = IC_CFG
+    sig = ico.sigma_of_n(nabs, n_side, "eisenstein_hu", 0.0, c["spectral_index"], omega_m=c["omega_m"],
+                         omega_b=c["omega_b"], h=c["h"], box_mpc_h=c["box_size_mpc_h"], sigma8=c["sigma8"])
+    v1, d21, v2 = ico.lpt_factors(c["a_init"], c["omega_m"], c["omega_lambda"], c["h0"], True)
+    t0 = time.perf_counter()
+    ico.zeldovich(n_side, 100.0, sig, seed=2, vel_factor=v1)
+    t1 = time.perf_counter()
+    ico.zeldovich_2lpt(n_side, 100.0, sig, seed=2, vel1=v1, d21=d21, vel2=v2)
+    t2 = time.perf_counter()
+    return {"1lpt": n_side ** 3 / (t1 - t0), "2lpt": n_side ** 3 / (t2 - t1), "particles": n_side ** 3,
+            "kind": "port", "cores": 1,
+            "sample": f"oracle/ic_oracle.py (numpy float64, single thread) at {n_side}^3"}
+
+
+def run_ics_only(args):
+    """One JSON line for the IC generator alone (profiling and the IC row)."""
+    import torch
+    torch.cuda.set_device(0)
+    rep = zeldovich_report(0, n_side=args.ics_side, reps=max(1, args.steps))
+    rep["cpu_baseline"] = None if args.no_cpu_baseline else zeldovich_cpu_sample()
+    print(json.dumps({"metric": "IC particles/s", "zeldovich_ics": rep}), flush=True)
+    return 0
 
 
 def run_b200(args):
@@ -477,6 +512,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--no-ics", action="store_true", help="skip the Zel'dovich IC timing")
+    ap.add_argument("--ics-only", action="store_true", help="time only the Zel'dovich IC generator")
+    ap.add_argument("--ics-side", type=int, default=256, help="particles per side for the IC timing")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak measurement (profiling runs)")
     ap.add_argument("--no-ewald", action="store_true", help="skip the FP64 Ewald error report")
     ap.add_argument("--no-accurate", action="store_true", help="skip the accurate-mode report")
@@ -486,6 +523,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.ics_only:
+        return run_ics_only(args)
     return run_b200(args)
 
 

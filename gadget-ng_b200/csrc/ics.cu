@@ -93,15 +93,56 @@ __device__ __forceinline__ double gaussian_std(uint64_t seed) {
 
 __device__ __forceinline__ int mode_int(int j, int n) { return j <= n / 2 ? j : j - n; }
 
-// Which field of delta the mode kernel writes (three spectral components):
-// PSI1  i n_a / |n|^2 delta                   (ic_zeldovich.rs:541-585)
-// DIAG  -n_a^2 / |n|^2 delta, a = x, y, z      (ic_2lpt.rs:86-140, phi_aa)
-// OFF   -n_a n_b / |n|^2 delta, ab = xy, xz, yz (phi_ab)
-enum IcField { IC_PSI1 = 0, IC_DIAG = 1, IC_OFF = 2 };
+// The integrand of sigma^2(8 Mpc/h) for A = 1 (transfer_fn.rs:146-184): k^(n_s+3)
+// T(k)^2 W(kR)^2 on 8193 log-spaced points of [1e-5, 5e2] h/Mpc.
+__host__ __device__ inline double sigma_integrand(double k, double r, double n_s, double om, double ob, double h) {
+  const double t = eh_transfer(k, om, ob, h);
+  const double x = k * r;
+  const double w = fabs(x) < 1e-4 ? 1.0 - x * x / 10.0 : 3.0 * (sin(x) - x * cos(x)) / (x * x * x);
+  return pow(k, n_s + 3.0) * t * t * w * w;
+}
 
-// delta(k) regenerated per call from the mode seeds (cheaper than keeping it).
-__global__ void k_ic_modes(int n, int nh, uint64_t seed, IcSpectrum sp, float2* __restrict__ spec3,
-                           int64_t comp_stride, int field) {
+constexpr int SIGMA_STEPS = 8192;
+
+// One block: the trapezoid of sigma^2(8) (weights 1/2 at both ends) and the
+// amplitude A = sigma_8 / sqrt(sigma^2) into amp_out (amplitude_for_sigma8,
+// transfer_fn.rs:222-228); the sum's order differs from the reference's
+// running sum only in rounding.
+__global__ void k_ic_sigma8(IcSpectrum sp, double sigma8, double* __restrict__ amp_out) {
+  __shared__ double part[32];
+  const double lk0 = log(1e-5), lk1 = log(5e2), dl = (lk1 - lk0) / SIGMA_STEPS;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i <= SIGMA_STEPS; i += blockDim.x) {
+    const double k = i == 0 ? 1e-5 : exp(lk0 + i * dl);
+    const double wgt = (i == 0 || i == SIGMA_STEPS) ? 0.5 : 1.0;
+    acc += wgt * sigma_integrand(k, 8.0, sp.n_s, sp.omega_m, sp.omega_b, sp.h);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += part[w];
+    v = v * dl / (2.0 * M_PI * M_PI);
+    *amp_out = v > 0.0 ? sigma8 / sqrt(v) : sigma8;
+  }
+}
+
+// sigma(sqrt(n2)) for every integer n2 <= n2_max; the amplitude from amp_dev
+// when given (sigma_8 normalisation), else the configured one.
+__global__ void k_ic_sigma_table(IcSpectrum sp, const double* __restrict__ amp_dev, int64_t n2_max,
+                                 double* __restrict__ table) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i > n2_max) return;
+  if (amp_dev) sp.amp = *amp_dev;
+  table[i] = ic_sigma(sp, sqrt((double)i));
+}
+
+// delta(k) of every half-spectrum mode from the mode seeds, written as the
+// three Psi1 components i n_a / |n|^2 delta (ic_zeldovich.rs:541-585) and,
+// when `delta_out` is given, as delta itself for the second-order fields.
+__global__ void k_ic_modes(int n, int nh, uint64_t seed, const double* __restrict__ sigma_of_n2,
+                           float2* __restrict__ spec3, int64_t comp_stride, float2* __restrict__ delta_out) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t total = (int64_t)n * n * nh;
   if (i >= total) return;
@@ -109,6 +150,7 @@ __global__ void k_ic_modes(int n, int nh, uint64_t seed, IcSpectrum sp, float2* 
   const int nx = kx, ny = mode_int(y, n), nz = mode_int(z, n), half = n / 2;
   const double n2 = (double)nx * nx + (double)ny * ny + (double)nz * nz;
   float2 out[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  float2 dk = make_float2(0.f, 0.f);
   if (n2 > 0.0 && nx != half && abs(ny) != half && abs(nz) != half) {
     // representative of the pair {k, -k} and whether this mode is its twin
     const int64_t self = ((int64_t)kx * n + y) * n + z;
@@ -122,26 +164,39 @@ __global__ void k_ic_modes(int n, int nh, uint64_t seed, IcSpectrum sp, float2* 
         twin = true;
       }
     }
-    const double sig = ic_sigma(sp, sqrt(n2));
+    const double sig = sigma_of_n2[(int64_t)n2];
     const uint64_t ms = fmix64(seed ^ fmix64((uint64_t)rep));
     double re = sig * gaussian_std(ms), im = sig * gaussian_std(fmix64(ms ^ 0x9E3779B97F4A7C15ull));
     if (twin) im = -im;
     const double inv_n2 = 1.0 / n2;
     const double na[3] = {(double)nx, (double)ny, (double)nz};
-    if (field == IC_PSI1) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c)  // i n_a / |n|^2 (re + i im)
-        out[c] = make_float2((float)(-na[c] * im * inv_n2), (float)(na[c] * re * inv_n2));
-    } else {
-      const int a0[3] = {0, 0, 1}, b0[3] = {1, 2, 2};
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const double f = field == IC_DIAG ? -na[c] * na[c] * inv_n2 : -na[a0[c]] * na[b0[c]] * inv_n2;
-        out[c] = make_float2((float)(f * re), (float)(f * im));
-      }
-    }
+    for (int c = 0; c < 3; ++c)  // i n_a / |n|^2 (re + i im)
+      out[c] = make_float2((float)(-na[c] * im * inv_n2), (float)(na[c] * re * inv_n2));
+    dk = make_float2((float)re, (float)im);
   }
   for (int c = 0; c < 3; ++c) spec3[c * comp_stride + i] = out[c];
+  if (delta_out) delta_out[i] = dk;
+}
+
+// Second derivatives of phi from the stored delta (ic_2lpt.rs:86-140):
+// -n_a^2 / |n|^2 delta for a = x, y, z (off_diagonal 0) or -n_a n_b / |n|^2
+// delta for ab = xy, xz, yz (off_diagonal 1).
+__global__ void k_ic_phi_ab(const float2* __restrict__ delta, int n, int nh, float2* __restrict__ spec3,
+                            int64_t comp_stride, int off_diagonal) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)n * n * nh;
+  if (i >= total) return;
+  const int kx = (int)(i % nh), y = (int)((i / nh) % n), z = (int)(i / ((int64_t)n * nh));
+  const float na[3] = {(float)kx, (float)mode_int(y, n), (float)mode_int(z, n)};
+  const float n2 = na[0] * na[0] + na[1] * na[1] + na[2] * na[2];
+  const float2 dk = delta[i];
+  const int a0[3] = {0, 0, 1}, b0[3] = {1, 2, 2};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float f = n2 > 0.f ? (off_diagonal ? -na[a0[c]] * na[b0[c]] : -na[c] * na[c]) / n2 : 0.f;
+    spec3[c * comp_stride + i] = make_float2(f * dk.x, f * dk.y);
+  }
 }
 
 // The 2LPT source (ic_2lpt.rs:146-165) from unnormalised inverse transforms of
@@ -178,73 +233,72 @@ __global__ void k_ic_psi2_modes(const float2* __restrict__ src, int n, int nh, f
   for (int c = 0; c < 3; ++c) spec3[c * comp_stride + i] = out[c];
 }
 
-__device__ __forceinline__ void lattice_of(int64_t gid, int n, int64_t* node, int ii[3]) {
-  ii[0] = (int)(gid / ((int64_t)n * n));
-  ii[1] = (int)((gid / n) % n);
-  ii[2] = (int)(gid % n);
-  *node = ((int64_t)ii[2] * n + ii[1]) * n + ii[0];  // the mesh's [z][y][x] layout
+// Particles are stored in the mesh's [z][y][x] order (slot = mesh node, so
+// reads of the displacement fields and writes of the state coalesce); each
+// carries its reference global id gid = ix n^2 + iy n + iz, through which every
+// host view of the state is ordered.
+__device__ __forceinline__ uint32_t lattice_of(int64_t slot, int n, int ii[3]) {
+  ii[0] = (int)(slot % n);
+  ii[1] = (int)((slot / n) % n);
+  ii[2] = (int)(slot / ((int64_t)n * n));
+  return (uint32_t)(((int64_t)ii[0] * n + ii[1]) * n + ii[2]);
 }
 
-// Keep the scaled Psi2 of each particle in its velocity slots until the
-// Psi1 pass writes the final state.
-__global__ void k_ic_stash_psi2(int n, double psi2_scale, const float* __restrict__ psi2, int64_t n3, Particles p) {
-  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (gid >= n3) return;
-  int64_t node;
+// Lattice position at the cell centre + Psi1, wrapped; momentum vel1 Psi1
+// (ic_zeldovich.rs:726-757).
+__global__ void k_ic_particles(int n, double box, double psi_scale, double vel1, const float* __restrict__ psi,
+                               int64_t n3, Particles p) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n3) return;
   int ii[3];
-  lattice_of(gid, n, &node, ii);
-  p.vx[gid] = (float)(psi2[node] * psi2_scale);
-  p.vy[gid] = (float)(psi2[n3 + node] * psi2_scale);
-  p.vz[gid] = (float)(psi2[2 * n3 + node] * psi2_scale);
-}
-
-// Lattice position at the cell centre + Psi1 (+ D2/D1^2 Psi2), wrapped;
-// momentum vel1 Psi1 (+ vel2 Psi2) (ic_zeldovich.rs:726-757, ic_2lpt.rs:520-548).
-__global__ void k_ic_particles(int n, double box, double psi_scale, double vel1, double d21, double vel2, int lpt2,
-                               const float* __restrict__ psi, int64_t n3, Particles p) {
-  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (gid >= n3) return;
-  int64_t node;
-  int ii[3];
-  lattice_of(gid, n, &node, ii);
+  const uint32_t gid = lattice_of(i, n, ii);
   const double d = box / n;
-  const float s2v[3] = {lpt2 ? p.vx[gid] : 0.f, lpt2 ? p.vy[gid] : 0.f, lpt2 ? p.vz[gid] : 0.f};
   uint32_t q[3];
   float v[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const double s1 = (double)psi[c * n3 + node] * psi_scale, s2 = (double)s2v[c];
-    double u = ((ii[c] + 0.5) * d + s1 + d21 * s2) / box;
+    const double s1 = (double)psi[c * n3 + i] * psi_scale;
+    double u = ((ii[c] + 0.5) * d + s1) / box;
     u = u - floor(u);
     q[c] = (uint32_t)((unsigned long long)llrint(u * TWO32) & 0xFFFFFFFFull);
-    v[c] = (float)(s1 * vel1 + s2 * vel2);
+    v[c] = (float)(s1 * vel1);
   }
-  p.qx[gid] = q[0];
-  p.qy[gid] = q[1];
-  p.qz[gid] = q[2];
-  p.vx[gid] = v[0];
-  p.vy[gid] = v[1];
-  p.vz[gid] = v[2];
+  p.qx[i] = q[0];
+  p.qy[i] = q[1];
+  p.qz[i] = q[2];
+  p.vx[i] = v[0];
+  p.vy[i] = v[1];
+  p.vz[i] = v[2];
   const double m = 1.0 / (double)n3;
-  p.mass[gid] = m;
-  p.massf[gid] = (float)m;
-  p.id[gid] = (uint32_t)gid;
+  p.mass[i] = m;
+  p.massf[i] = (float)m;
+  p.id[i] = gid;
 }
 
-// transfer_fn.rs:146-184, :190-199, :222-228
+// Second order on top of the first (ic_2lpt.rs:520-548): x += D2/D1^2 Psi2
+// as a fixed-point offset (the uint32 sum wraps periodically, as rem_euclid
+// does), p += vel2 Psi2.
+__global__ void k_ic_add_psi2(int n, double box, double psi2_scale, double d21, double vel2,
+                              const float* __restrict__ psi2, int64_t n3, Particles p) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  uint32_t* q[3] = {p.qx, p.qy, p.qz};
+  float* v[3] = {p.vx, p.vy, p.vz};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double s2 = (double)psi2[c * n3 + i] * psi2_scale;
+    q[c][i] += (uint32_t)llrint(d21 * s2 / box * TWO32);
+    v[c][i] = (float)((double)v[c][i] + s2 * vel2);
+  }
+}
+
+// transfer_fn.rs:146-184, :190-199, :222-228 (host, the reference's running sum)
 double sigma_sq_unit(double r, double n_s, double om, double ob, double h) {
   const double lk0 = std::log(1e-5), lk1 = std::log(5e2);
-  const int steps = 8192;
-  const double dl = (lk1 - lk0) / steps;
-  auto integrand = [&](double k) {
-    const double t = eh_transfer(k, om, ob, h);
-    const double x = k * r;
-    const double w = std::fabs(x) < 1e-4 ? 1.0 - x * x / 10.0 : 3.0 * (std::sin(x) - x * std::cos(x)) / (x * x * x);
-    return std::pow(k, n_s + 3.0) * t * t * w * w;
-  };
-  double sum = 0.0, fprev = integrand(1e-5);
-  for (int i = 1; i <= steps; ++i) {
-    const double f = integrand(std::exp(lk0 + i * dl));
+  const double dl = (lk1 - lk0) / SIGMA_STEPS;
+  double sum = 0.0, fprev = sigma_integrand(1e-5, r, n_s, om, ob, h);
+  for (int i = 1; i <= SIGMA_STEPS; ++i) {
+    const double f = sigma_integrand(std::exp(lk0 + i * dl), r, n_s, om, ob, h);
     sum += 0.5 * (fprev + f) * dl;
     fprev = f;
   }
@@ -262,7 +316,7 @@ struct IcFactors {
 };
 
 // Spectrum and factors of a configuration (host); false when it is invalid.
-bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, IcFactors* fa) {
+bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, IcFactors* fa, bool host_sigma8 = true) {
   if (!c || c->n_side < 4 || c->n_side > 1024 || (c->n_side & (c->n_side - 1)) != 0) return false;
   if (c->transfer != 0 && c->transfer != 1) return false;
   if (c->use_2lpt != 0 && c->use_2lpt != 1) return false;
@@ -277,7 +331,7 @@ bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, IcFactors* fa) {
   sp->two_pi_h_over_bsm = c->transfer == 1 ? 2.0 * M_PI * c->h / c->box_size_mpc_h : 0.0;
   sp->inv_sqrt_n3 = 1.0 / std::sqrt(n3);
   sp->amp = c->amplitude;
-  if (c->transfer == 1 && c->sigma8 > 0.0) {
+  if (host_sigma8 && c->transfer == 1 && c->sigma8 > 0.0) {
     const double v = sigma_sq_unit(8.0, c->spectral_index, c->omega_m, c->omega_b, c->h);
     sp->amp = v > 0.0 ? c->sigma8 / std::sqrt(v) : c->sigma8;
   }
@@ -315,12 +369,13 @@ bool zeldovich_factors(const tpm_zeldovich* c, IcSpectrum* sp, IcFactors* fa) {
 
 // `mesh` is a plan of the solver whose buffers may be overwritten; it is used
 // when its mesh is the IC lattice (no allocation), otherwise a temporary plan
-// of n_side^3 is made and freed.  Sequence: [2LPT: phi_aa -> source, phi_ab ->
-// source, forward transform, Psi2 -> velocity slots], then Psi1 -> particles.
+// of n_side^3 is made and freed.  Sequence: delta -> Psi1 -> particles; for
+// 2LPT then phi_aa -> source, phi_ab -> source, forward transform -> Psi2,
+// added to the particles.
 void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cudaStream_t s, PmPlan* mesh) {
   IcSpectrum sp{};
   IcFactors fa{};
-  if (!zeldovich_factors(c, &sp, &fa)) throw Error(TPM_ERR_INVALID_ARGUMENT, "bad Zel'dovich configuration");
+  if (!zeldovich_factors(c, &sp, &fa, false)) throw Error(TPM_ERR_INVALID_ARGUMENT, "bad Zel'dovich configuration");
   const int n = c->n_side;
   const bool reuse = mesh && mesh->nm == n && mesh->ncomp >= 3 && mesh->spec3 && mesh->force && mesh->rho &&
                      mesh->spec;
@@ -335,28 +390,41 @@ void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cu
     const int64_t nh = n / 2 + 1, plane = (int64_t)n * n * nh, n3 = (int64_t)n * n * n;
     const unsigned gm = grid_for(plane, 256, 1ll << 30), gp = grid_for(n3, 256, 1ll << 30);
     const double cell_over_n3 = (box / n) / (double)n3;  // rustfft's inverse is unnormalised
+    // sigma(|n|) tabulated by |n|^2 in the density buffer (6 n^2 + 16 bytes of
+    // its 4 n^3), the sigma_8 amplitude first when asked for
+    double* table = reinterpret_cast<double*>(plan.rho);
+    const int64_t n2_max = 3ll * (n / 2) * (n / 2);
+    double* amp_dev = nullptr;
+    if (c->transfer == 1 && c->sigma8 > 0.0) {
+      amp_dev = table + n2_max + 1;
+      k_ic_sigma8<<<1, 256, 0, s>>>(sp, c->sigma8, amp_dev);
+      TPM_LAUNCH_CHECK();
+    }
+    k_ic_sigma_table<<<grid_for(n2_max + 1, 256, 1ll << 30), 256, 0, s>>>(sp, amp_dev, n2_max, table);
+    TPM_LAUNCH_CHECK();
+    // first order; delta kept in the spectrum work array for the second
+    k_ic_modes<<<gm, 256, 0, s>>>(n, (int)nh, c->seed, table, plan.spec3, plane, c->use_2lpt ? plan.spec : nullptr);
+    TPM_LAUNCH_CHECK();
+    pm_inverse_components(plan, 3, s);
+    k_ic_particles<<<gp, 256, 0, s>>>(n, box, cell_over_n3 * fa.scale, fa.vel1, plan.force, n3, out);
+    TPM_LAUNCH_CHECK();
     if (c->use_2lpt) {
       const float inv_n3 = (float)(1.0 / (double)n3);
       for (int off = 0; off < 2; ++off) {
-        k_ic_modes<<<gm, 256, 0, s>>>(n, (int)nh, c->seed, sp, plan.spec3, plane, off ? IC_OFF : IC_DIAG);
+        k_ic_phi_ab<<<gm, 256, 0, s>>>(plan.spec, n, (int)nh, plan.spec3, plane, off);
         TPM_LAUNCH_CHECK();
         pm_inverse_components(plan, 3, s);
         k_ic_source<<<gp, 256, 0, s>>>(plan.force, plan.rho, n3, inv_n3, off);
         TPM_LAUNCH_CHECK();
       }
-      pm_forward_real(plan, s);
+      pm_forward_real(plan, s);  // S(k) replaces delta in the work array
       k_ic_psi2_modes<<<gm, 256, 0, s>>>(plan.spec, n, (int)nh, plan.spec3, plane);
       TPM_LAUNCH_CHECK();
       pm_inverse_components(plan, 3, s);
-      k_ic_stash_psi2<<<gp, 256, 0, s>>>(n, cell_over_n3 * fa.scale * fa.scale, plan.force, n3, out);
+      k_ic_add_psi2<<<gp, 256, 0, s>>>(n, box, cell_over_n3 * fa.scale * fa.scale, fa.d21, fa.vel2, plan.force, n3,
+                                       out);
       TPM_LAUNCH_CHECK();
     }
-    k_ic_modes<<<gm, 256, 0, s>>>(n, (int)nh, c->seed, sp, plan.spec3, plane, IC_PSI1);
-    TPM_LAUNCH_CHECK();
-    pm_inverse_components(plan, 3, s);
-    k_ic_particles<<<gp, 256, 0, s>>>(n, box, cell_over_n3 * fa.scale, fa.vel1, fa.d21, fa.vel2, c->use_2lpt,
-                                      plan.force, n3, out);
-    TPM_LAUNCH_CHECK();
     TPM_CUDA(cudaStreamSynchronize(s));
   } catch (...) {
     if (!reuse) pm_plan_free(temp);
