@@ -320,6 +320,62 @@ def zeldovich_cpu_sample(n_side=64):
             "sample": f"oracle/ic_oracle.py (numpy float64, single thread) at {n_side}^3"}
 
 
+def snapshot_report(device, n_side=128, reps=3):
+    """Time tpm_write_snapshot (JSONL and bincode) of n_side^3 Zel'dovich
+    particles into a temporary directory on the local disk: wall time of the
+    synchronous call (device decode, chunked copies, host formatting, file
+    writes), median of `reps`; the files are removed."""
+    import shutil
+    import tempfile
+    import treepm
+    solver = treepm.TreePmSolver(n_side, 100.0, r_split=2.5 * 100.0 / n_side, device=device)
+    solver.set_particles_zeldovich(n_side, 3, **IC_CFG)
+    out = {"particles": n_side ** 3, "threads": os.cpu_count()}
+    root = tempfile.mkdtemp(prefix="tpm_snapshot_")
+    try:
+        for fmt, name in (("bincode", "particles.bin"), ("jsonl", "particles.jsonl")):
+            ts, size = [], 0
+            for r in range(reps):
+                d = os.path.join(root, f"{fmt}{r}")
+                c0 = time.perf_counter()
+                solver.write_snapshot(d, fmt, time=0.02, redshift=49.0)
+                ts.append(time.perf_counter() - c0)
+                size = os.path.getsize(os.path.join(d, name))
+                shutil.rmtree(d)
+            sec = float(np.median(ts))
+            out[fmt] = {"ms": 1e3 * sec, "bytes": size, "gb_per_s": size / sec / 1e9,
+                        "records_per_s": n_side ** 3 / sec}
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+        solver.close()
+    return out
+
+
+def snapshot_cpu_sample(records=1 << 15):
+    """The pure-Python restatement of both writers on a bounded sample."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import snapshot_oracle as so
+    rng = np.random.default_rng(1)
+    pos, vel = rng.uniform(0, 100, (records, 3)), rng.normal(0, 1e-3, (records, 3))
+    m, ids = np.full(records, 1.0 / records), np.arange(records)
+    t0 = time.perf_counter()
+    so.jsonl(ids, m, pos, vel)
+    t1 = time.perf_counter()
+    so.bincode(ids, m, pos, vel)
+    t2 = time.perf_counter()
+    return {"jsonl_records_per_s": records / (t1 - t0), "bincode_records_per_s": records / (t2 - t1),
+            "kind": "port", "cores": 1, "sample": f"oracle/snapshot_oracle.py (pure Python) on {records} records"}
+
+
+def run_snapshot_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    rep = snapshot_report(0, n_side=args.snapshot_side, reps=max(1, args.steps))
+    rep["cpu_baseline"] = None if args.no_cpu_baseline else snapshot_cpu_sample()
+    print(json.dumps({"metric": "snapshot records/s", "snapshot": rep}), flush=True)
+    return 0
+
+
 def run_ics_only(args):
     """One JSON line for the IC generator alone (profiling and the IC row)."""
     import torch
@@ -514,6 +570,8 @@ def main():
     ap.add_argument("--no-ics", action="store_true", help="skip the Zel'dovich IC timing")
     ap.add_argument("--ics-only", action="store_true", help="time only the Zel'dovich IC generator")
     ap.add_argument("--ics-side", type=int, default=256, help="particles per side for the IC timing")
+    ap.add_argument("--snapshot-only", action="store_true", help="time only the snapshot writers")
+    ap.add_argument("--snapshot-side", type=int, default=128, help="particles per side for the snapshot timing")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak measurement (profiling runs)")
     ap.add_argument("--no-ewald", action="store_true", help="skip the FP64 Ewald error report")
     ap.add_argument("--no-accurate", action="store_true", help="skip the accurate-mode report")
@@ -525,6 +583,8 @@ def main():
         return run_reference(args)
     if args.ics_only:
         return run_ics_only(args)
+    if args.snapshot_only:
+        return run_snapshot_only(args)
     return run_b200(args)
 
 

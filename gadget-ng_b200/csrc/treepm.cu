@@ -17,6 +17,7 @@
 #include "learned.cuh"
 #include "pm.cuh"
 #include "scan.cuh"
+#include "snapshot.cuh"
 #include "sort.cuh"
 #include "tree.cuh"
 #include "walk.cuh"
@@ -1033,6 +1034,89 @@ int tpm_set_particles_zeldovich(tpm_handle* h, const tpm_zeldovich* cfg) {
     zeldovich_fill(cfg, h->cfg.box_size, h->P[0], h->stream, &h->pm);
   } catch (const Error& e) {
     return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_write_snapshot(tpm_handle* h, const char* out_dir, int32_t format, const tpm_snapshot_env* env,
+                       const tpm_provenance* prov) {
+  if (!h || !out_dir || !env || !prov) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    snapshot_write(out_dir, format, env, prov, DeviceState{h->P[h->cur], h->n, h->cfg.box_size, h->staging, h->stream});
+  } catch (const Error& e) {
+    return fail(h, e);
+  } catch (const std::exception& e) {
+    return fail(h, Error(TPM_ERR_IO, e.what()));
+  }
+  return TPM_OK;
+}
+
+int tpm_read_snapshot(tpm_handle* h, const char* dir, int32_t format, tpm_snapshot_env* env_out) {
+  if (!h || !dir) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    std::vector<double> pos, vel, mass;
+    std::vector<uint64_t> ids;
+    snapshot_read(dir, format, env_out, pos, vel, mass, ids);
+    order_by_id(pos, vel, mass, ids);
+    const int rc = tpm_set_particles(h, pos.data(), vel.data(), mass.data(), (int64_t)ids.size());
+    if (rc != TPM_OK) return rc;
+  } catch (const Error& e) {
+    return fail(h, e);
+  } catch (const std::exception& e) {
+    return fail(h, Error(TPM_ERR_IO, e.what()));
+  }
+  return TPM_OK;
+}
+
+// save_checkpoint (checkpoint.rs:47-105): the JSONL writer with the default
+// SnapshotEnv (time 0, redshift 0, box 1) and the provenance ("checkpoint",
+// no commit, "release", no features, no command line, config hash).
+int tpm_write_checkpoint(tpm_handle* h, const char* out_dir, uint64_t completed_step, double a_current,
+                         const char* config_hash) {
+  if (!h || !out_dir || !config_hash) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    const std::string ck = std::string(out_dir) + "/checkpoint";
+    tpm_snapshot_env env{};
+    env.box_size = 1.0;
+    const tpm_provenance prov{"checkpoint", nullptr, "release", nullptr, 0, 0, nullptr, config_hash};
+    snapshot_write(ck, TPM_SNAPSHOT_JSONL, &env, &prov,
+                   DeviceState{h->P[h->cur], h->n, h->cfg.box_size, h->staging, h->stream});
+    checkpoint_write_meta(ck, completed_step, a_current, config_hash, h->n);
+  } catch (const Error& e) {
+    return fail(h, e);
+  } catch (const std::exception& e) {
+    return fail(h, Error(TPM_ERR_IO, e.what()));
+  }
+  return TPM_OK;
+}
+
+// load_checkpoint (checkpoint.rs:112-178) for one rank holding every particle.
+int tpm_read_checkpoint(tpm_handle* h, const char* resume_dir, uint64_t* completed_step, double* a_current,
+                        char* config_hash, int64_t config_hash_capacity) {
+  if (!h || !resume_dir || !completed_step || !a_current) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    const std::string ck = std::string(resume_dir) + "/checkpoint";
+    std::string hash;
+    int64_t total = 0;
+    checkpoint_read_meta(ck, completed_step, a_current, &hash, &total);
+    if (config_hash) {
+      if (config_hash_capacity < (int64_t)hash.size() + 1)
+        throw Error(TPM_ERR_INVALID_ARGUMENT, "config_hash buffer too small");
+      std::memcpy(config_hash, hash.c_str(), hash.size() + 1);
+    }
+    std::vector<double> pos, vel, mass;
+    std::vector<uint64_t> ids;
+    snapshot_read(ck, TPM_SNAPSHOT_JSONL, nullptr, pos, vel, mass, ids);
+    if ((int64_t)ids.size() != total) throw Error(TPM_ERR_IO, "checkpoint particle count differs from checkpoint.json");
+    order_by_id(pos, vel, mass, ids);
+    const int rc = tpm_set_particles(h, pos.data(), vel.data(), mass.data(), total);
+    if (rc != TPM_OK) return rc;
+  } catch (const Error& e) {
+    return fail(h, e);
+  } catch (const std::exception& e) {
+    return fail(h, Error(TPM_ERR_IO, e.what()));
   }
   return TPM_OK;
 }

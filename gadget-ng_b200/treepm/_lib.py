@@ -23,7 +23,9 @@ ERRORS = {
     8: "TPM_ERR_NO_DEVICE",
     9: "TPM_ERR_NONFINITE",
     10: "TPM_ERR_TOO_LARGE",
+    11: "TPM_ERR_IO",
 }
+SNAPSHOT_FORMATS = {"jsonl": 0, "bincode": 1}
 
 FLAG_APERIODIC_WALK = 1 << 0
 FLAG_DECONVOLVE_CIC = 1 << 1
@@ -70,6 +72,36 @@ class TpmZeldovich(C.Structure):
         ("rescale_to_a_init", C.c_int32),
         ("use_2lpt", C.c_int32),
         ("reserved", C.c_int32),
+    ]
+
+
+class TpmProvenance(C.Structure):
+    """tpm_provenance (crates/gadget-ng-io/src/provenance.rs:4-12)."""
+    _fields_ = [
+        ("crate_version", C.c_char_p),
+        ("git_commit", C.c_char_p),
+        ("build_profile", C.c_char_p),
+        ("enabled_features", C.POINTER(C.c_char_p)),
+        ("n_enabled_features", C.c_int32),
+        ("n_command_line", C.c_int32),
+        ("command_line", C.POINTER(C.c_char_p)),
+        ("config_hash", C.c_char_p),
+    ]
+
+
+class TpmSnapshotEnv(C.Structure):
+    """tpm_snapshot_env (crates/gadget-ng-io/src/writer.rs:10-37)."""
+    _fields_ = [
+        ("time", C.c_double),
+        ("redshift", C.c_double),
+        ("box_size", C.c_double),
+        ("has_units", C.c_int32),
+        ("reserved", C.c_int32),
+        ("length_in_kpc", C.c_double),
+        ("mass_in_msun", C.c_double),
+        ("velocity_in_km_s", C.c_double),
+        ("time_in_gyr", C.c_double),
+        ("g_internal", C.c_double),
     ]
 
 
@@ -157,6 +189,13 @@ SIGNATURES = {
     "tpm_power_spectrum": ([_P, _P, _I64, _D, C.c_int32, C.c_int32, _P, _P, _P], _I),
     "tpm_get_power_spectrum": ([_P, _P, _P, _P], _I),
     "tpm_set_particles_zeldovich": ([_P, _P], _I),
+    "tpm_write_snapshot": ([_P, C.c_char_p, C.c_int32, _P, _P], _I),
+    "tpm_read_snapshot": ([_P, C.c_char_p, C.c_int32, _P], _I),
+    "tpm_write_snapshot_host": ([C.c_char_p, C.c_int32, _P, _P, _P, _P, _I64, _P, _P], _I),
+    "tpm_read_snapshot_host": ([C.c_char_p, C.c_int32, _P, _P, _P, _P, _P, _I64, _P], _I),
+    "tpm_snapshot_last_error": ([], C.c_char_p),
+    "tpm_write_checkpoint": ([_P, C.c_char_p, C.c_uint64, _D, C.c_char_p], _I),
+    "tpm_read_checkpoint": ([_P, C.c_char_p, _P, _P, C.c_char_p, _I64], _I),
     "tpm_zeldovich_sigma": ([_P, _P, _I64, _P, _P], _I),
 }
 NOALLOC_MAX_PARTICLES = 1 << 18

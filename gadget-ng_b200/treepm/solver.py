@@ -133,6 +133,28 @@ class TreePmSolver:
         check(self._h.h, self._h._lib.tpm_set_particles_zeldovich(self._h.h, C.byref(c)))
         return int(n_side) ** 3
 
+    # ---- snapshots and checkpoints (crates/gadget-ng-io, engine/checkpoint.rs) --
+    def write_snapshot(self, out_dir, fmt="jsonl", time=0.0, redshift=0.0, box_size=None, units=None,
+                       provenance=None):
+        """The resident particles as a gadget-ng snapshot ("jsonl" or "bincode")."""
+        from . import snapshot
+        snapshot.solver_write_snapshot(self._h, out_dir, fmt, time, redshift,
+                                       self.box_size if box_size is None else box_size, units, provenance)
+
+    def read_snapshot(self, path, fmt="jsonl") -> dict:
+        """Load a snapshot's particles (global ids 0..n-1); returns meta.json's fields."""
+        from . import snapshot
+        return snapshot.solver_read_snapshot(self._h, path, fmt)
+
+    def write_checkpoint(self, out_dir, completed_step, a_current, config_hash=""):
+        from . import snapshot
+        snapshot.solver_write_checkpoint(self._h, out_dir, completed_step, a_current, config_hash)
+
+    def read_checkpoint(self, resume_dir):
+        """(completed_step, a_current, config_hash); the particles become the state."""
+        from . import snapshot
+        return snapshot.solver_read_checkpoint(self._h, resume_dir)
+
     def set_particles_fixed(self, q, mass, vel=None):
         q = np.ascontiguousarray(q, dtype=np.uint32).reshape(-1, 3)
         mass = np.ascontiguousarray(mass, dtype=np.float64).reshape(-1)

@@ -47,7 +47,8 @@ enum {
   TPM_ERR_NOT_READY = 7,       /* call needs particles / forces that are not set */
   TPM_ERR_NO_DEVICE = 8,       /* no CUDA device, or the device is not sm_100 */
   TPM_ERR_NONFINITE = 9,       /* non-finite input position or mass */
-  TPM_ERR_TOO_LARGE = 10       /* more particles than tpm_hilbert_sort_noalloc's fixed scratch holds */
+  TPM_ERR_TOO_LARGE = 10,      /* more particles than tpm_hilbert_sort_noalloc's fixed scratch holds */
+  TPM_ERR_IO = 11              /* a snapshot or checkpoint file could not be written, read or parsed */
 };
 
 /* ---- configuration flags -------------------------------------------------- */
@@ -292,6 +293,66 @@ int tpm_power_spectrum(const double* pos, const double* mass, int64_t n, double 
 /* The same estimator on a handle's resident particles (mesh = its pm_grid_size);
  * overwrites the density mesh that tpm_get_mesh returns. */
 int tpm_get_power_spectrum(tpm_handle* h, double* k, double* pk, uint64_t* n_modes);
+
+/* ---- snapshots and checkpoints ---------------------------------------------------
+ * The files of gadget-ng's SnapshotWriter implementations: <dir>/meta.json,
+ * <dir>/provenance.json and <dir>/particles.jsonl (JsonlWriter,
+ * crates/gadget-ng-io/src/snapshot.rs:124-146) or <dir>/particles.bin
+ * (BincodeWriter, bincode_writer.rs:16-31), records in global-id order with
+ * the current ParticleRecord fields (dark matter: internal_energy and
+ * smoothing_length 0, ptype DarkMatter).  Checkpoints are
+ * <dir>/checkpoint/{particles.jsonl, meta.json, provenance.json,
+ * checkpoint.json} (crates/gadget-ng-cli/src/engine/checkpoint.rs:47-110). */
+#define TPM_SNAPSHOT_JSONL 0
+#define TPM_SNAPSHOT_BINCODE 1
+
+/* Provenance (crates/gadget-ng-io/src/provenance.rs:4-12); git_commit NULL
+ * is written as null. */
+typedef struct tpm_provenance {
+  const char* crate_version;
+  const char* git_commit;
+  const char* build_profile;
+  const char* const* enabled_features;
+  int32_t n_enabled_features;
+  int32_t n_command_line;
+  const char* const* command_line;
+  const char* config_hash;
+} tpm_provenance;
+
+/* SnapshotEnv (crates/gadget-ng-io/src/writer.rs:10-37): time, redshift and
+ * box size of meta.json, units when has_units != 0. */
+typedef struct tpm_snapshot_env {
+  double time;
+  double redshift;
+  double box_size;
+  int32_t has_units;
+  int32_t reserved;
+  double length_in_kpc, mass_in_msun, velocity_in_km_s, time_in_gyr, g_internal;
+} tpm_snapshot_env;
+
+/* The resident state (decoded on the device; JSONL formatted by host threads
+ * from double-buffered chunk copies; bincode records built on the device). */
+int tpm_write_snapshot(tpm_handle* h, const char* out_dir, int32_t format, const tpm_snapshot_env* env,
+                       const tpm_provenance* prov);
+/* Load a snapshot's particles into the handle (global ids must be 0..n-1);
+ * env_out (may be NULL) receives meta.json's time, redshift, box size, units. */
+int tpm_read_snapshot(tpm_handle* h, const char* dir, int32_t format, tpm_snapshot_env* env_out);
+/* Host arrays (the reference's write_snapshot on a particle slice):
+ * positions and velocities n x 3, masses n, global ids n (NULL: 0..n-1). */
+int tpm_write_snapshot_host(const char* out_dir, int32_t format, const double* pos, const double* vel,
+                            const double* mass, const uint64_t* global_ids, int64_t n,
+                            const tpm_snapshot_env* env, const tpm_provenance* prov);
+/* Read a snapshot in file order into host arrays of `capacity` records
+ * (all four may be NULL to query *n_out only). */
+int tpm_read_snapshot_host(const char* dir, int32_t format, int64_t* n_out, double* pos, double* vel,
+                           double* mass, uint64_t* global_ids, int64_t capacity, tpm_snapshot_env* env_out);
+const char* tpm_snapshot_last_error(void);  /* message of the last failed *_host call on this thread */
+/* save_checkpoint / load_checkpoint of the serial engine: the JSONL state and
+ * checkpoint.json (completed step, a, config hash, particle count). */
+int tpm_write_checkpoint(tpm_handle* h, const char* out_dir, uint64_t completed_step, double a_current,
+                         const char* config_hash);
+int tpm_read_checkpoint(tpm_handle* h, const char* resume_dir, uint64_t* completed_step, double* a_current,
+                        char* config_hash, int64_t config_hash_capacity);
 
 /* ---- learned short-range network (extension) --------------------------------
  * No counterpart in the reference.  A small 3D CNN reads the long-range mesh
