@@ -456,20 +456,23 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     const uint32_t take = __ballot_sync(0xffffffffu, lane < avail && incl <= 32u);
     const int k = __popc(take);
     sp -= k;
-    // per-target refinement of undecided open nodes
+    // per-target refinement of undecided open nodes; the node records of all
+    // of them are loaded at once (one per lane) and broadcast in turn
     uint32_t amb = __ballot_sync(0xffffffffu, lane < k && (e.y & INFO_AMB));
+    uint4 wrec = make_uint4(0u, 0u, 0u, 0u);
+    if (ACC ? (lane < k && (e.y & (INFO_AMB | INFO_MAC))) : ((amb >> lane) & 1u)) wrec = __ldg(&a.walk[e.w]);
     while (amb) {
       const int src = __ffs(amb) - 1;
       amb &= amb - 1;
       const uint32_t node = __shfl_sync(0xffffffffu, e.w, src);
       const uint32_t me = __shfl_sync(0xffffffffu, e.z, src);
       const int dep = wn_depth(__shfl_sync(0xffffffffu, e.y, src));
+      const uint32_t wq[3] = {__shfl_sync(0xffffffffu, wrec.x, src), __shfl_sync(0xffffffffu, wrec.y, src),
+                              __shfl_sync(0xffffffffu, wrec.z, src)};
       bool pass = false;
       if (has && lane < TPW && ((me >> tgt) & 1u)) {
-        const uint4 w = __ldg(&a.walk[node]);
         const float h = ldexpf(a.h0_u, (ACC ? 1 : 0) - dep);
         float s = 0.f;
-        const uint32_t wq[3] = {w.x, w.y, w.z};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
           float dd = (float)rel32(wq[d], tq[d], a.periodic) * a.u_inv;
@@ -495,7 +498,8 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const uint32_t node = __shfl_sync(0xffffffffu, e.w, src);
       const uint32_t me = __shfl_sync(0xffffffffu, e.z, src);
       const int dep = wn_depth(__shfl_sync(0xffffffffu, e.y, src));
-      const uint4 w = __ldg(&a.walk[node]);
+      const uint4 w = make_uint4(__shfl_sync(0xffffffffu, wrec.x, src), __shfl_sync(0xffffffffu, wrec.y, src),
+                                 __shfl_sync(0xffffffffu, wrec.z, src), __shfl_sync(0xffffffffu, wrec.w, src));
       const float hnode = ldexpf(a.h0_u, -dep);
       bool accept = false;
       if (has && lane < TPW && ((me >> tgt) & 1u)) {
