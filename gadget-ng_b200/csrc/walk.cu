@@ -71,6 +71,12 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
   return v;
 }
 
+// h0 * 2^-dep by exponent arithmetic: h0 (the root half side in walk units,
+// O(r_cut / cell)) stays a normal float for every tree depth (-1 <= dep < 64).
+__device__ __forceinline__ float half_side(float h0, int dep) {
+  return __int_as_float(__float_as_int(h0) - dep * (1 << 23));
+}
+
 // ---- float64 decisions with the reference's expressions -------------------
 __device__ __forceinline__ double aabb_axis(double dc, double h) {
   double e = dsub(fabs(dc), h);
@@ -277,21 +283,20 @@ __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nl
 }
 
 // Stack entry of an open node: its children's record range, mask of the
-// targets that still see it, and the octree id for the per-target test.
+// targets that see it (refined per target before the push), and the octree id.
 struct __align__(16) StackEntry {
   uint32_t first;  // record index of the first child
-  uint32_t info;   // the node's record info | INFO_AMB / INFO_MAC when undecided for the group
+  uint32_t info;   // the node's record info | INFO_MAC when its opening angle is undecided for the group
   uint32_t mask;
   uint32_t ref;    // octree node id
 };
 constexpr int STACK_ENTRIES = 1024;  // global, per warp
-constexpr uint32_t INFO_AMB = 0x80000000u;
 constexpr uint32_t INFO_MAC = 0x40000000u;  // opening angle undecided for the group
 
 // Walk the tree for targets [first, first + count) (count <= TPW) with one warp.
 template <int TPW, bool ACC>
 __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, Entry* Ll, Entry* Lm, uint8_t* owner,
-                             StackEntry* stk) {
+                             StackEntry* stk, float4* rpos, uint4* rmask) {
   const int lane = threadIdx.x & 31;
   const int tgt = lane & (TPW - 1);  // this lane's target within the group
   const uint32_t p = first + ((uint32_t)tgt < count ? (uint32_t)tgt : 0u);
@@ -337,13 +342,15 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     bool emit = false, push = false, ambig = false, is_leaf = false;
     Entry ent;
     StackEntry se;
+    float sx = 0.f, sy = 0.f, sz = 0.f, sh = 0.f;  // an undecided open node: group-relative COM, cull half side
+    uint32_t simg = 0u;
     if (have && imask != 0u) {
       const uint4 r0 = __ldg(reinterpret_cast<const uint4*>(&a.recs[item]));
       const uint4 r1 = __ldg(reinterpret_cast<const uint4*>(&a.recs[item]) + 1);
       const uint32_t info = r1.y;
       const bool leaf = (info & WN_LEAF) != 0;
       const int dep = wn_depth(info);
-      const float hnode = ldexpf(a.h0_u, -dep);
+      const float hnode = half_side(a.h0_u, dep);
       // cull half side: the COM-centred AABB of the reference, or (accurate
       // mode) twice that, which holds the whole cell
       const float h = (leaf && a.periodic) ? 0.f : (ACC && !leaf ? 2.f * hnode : hnode);
@@ -353,10 +360,12 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       // (images at 0 and +-L), then the AABB gap.
       float emin2 = 0.f, emax2 = 0.f, dmin2 = 0.f, dmax2 = 0.f;
       int32_t S[3];
+      float SF[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         S[d] = rel32(cq[d], oq[d], a.periodic);
         const float sf = (float)S[d] * a.u_inv;
+        SF[d] = sf;
         const float lo = sf - bmax[d], hi = sf - bmin[d];
         float dmin = lo > 0.f ? lo : (hi < 0.f ? -hi : 0.f);
         float dmax = fmaxf(fabsf(lo), fabsf(hi));
@@ -393,9 +402,16 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
           push = true;
           ambig = !(emax2 < a.grc2_lo);
           se.first = r1.x;
-          se.info = info | (ambig ? INFO_AMB : 0u) | (macmix ? INFO_MAC : 0u);
+          se.info = info | (macmix ? INFO_MAC : 0u);
           se.mask = imask;
           se.ref = r1.z;
+          if (ambig) {
+            sx = SF[0];
+            sy = SF[1];
+            sz = SF[2];
+            sh = h;
+            simg = (a.periodic && dep < a.img_depth) ? 1u : 0u;
+          }
         } else {
           emit = true;
           ent.x = (float)S[0] * a.u_inv;
@@ -423,6 +439,49 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     }
     nll += __popc(eml);
     nlm += __popc(emm);
+    // ---- per-target refinement of open nodes undecided for the group, before
+    // they are pushed: each node is staged once (group-relative COM, cull half
+    // side) in shared memory, then tested against all targets (one per lane)
+    // from a broadcast load.  dd = COM - target in float differs from the exact
+    // minimum-image difference by ~1e-7 of r_cut, far inside the band that goes
+    // to the float64 test.  A node no target sees is not pushed.
+    const uint32_t below = (1u << lane) - 1u;
+    const uint32_t amb = __ballot_sync(0xffffffffu, push && ambig);
+    if (push && ambig) {
+      const int j = __popc(amb & below);
+      rpos[j] = make_float4(sx, sy, sz, sh);
+      rmask[j] = make_uint4(se.mask, se.ref, simg, 0u);
+    }
+    __syncwarp();
+    const int namb = __popc(amb);
+    for (int j = 0; j < namb; ++j) {
+      const float4 R = rpos[j];
+      const uint4 M = rmask[j];
+      bool pass = false;
+      if (has && lane < TPW && ((M.x >> tgt) & 1u)) {
+        const float rc[3] = {R.x, R.y, R.z};
+        float s = 0.f;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          float dd = rc[d] - tf[d];
+          if (M.z) dd -= a.box_u * rintf(dd / a.box_u);  // top levels: the nearest periodic image
+          const float ee = fmaxf(fabsf(dd) - R.w, 0.f);
+          s = fmaf(ee, ee, s);
+        }
+        if (s <= a.rc2_lo) pass = true;
+        else if (!ACC && s <= a.rc2_hi) {
+          pass = exact_open_pass(a, p, M.y);
+          ++nexact;
+        }
+      }
+      const uint32_t nm = __ballot_sync(0xffffffffu, pass);  // lanes < TPW hold the targets
+      if (lane == 0) rmask[j].x = nm;
+    }
+    __syncwarp();
+    if (push && ambig) {
+      se.mask = rmask[__popc(amb & below)].x;
+      push = se.mask != 0u;
+    }
     // ---- push open nodes
     const uint32_t pm = __ballot_sync(0xffffffffu, push);
     if (sp + __popc(pm) > STACK_ENTRIES) {
@@ -456,38 +515,8 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     const uint32_t take = __ballot_sync(0xffffffffu, lane < avail && incl <= 32u);
     const int k = __popc(take);
     sp -= k;
-    // per-target refinement of undecided open nodes; the node records of all
-    // of them are loaded at once (one per lane) and broadcast in turn
-    uint32_t amb = __ballot_sync(0xffffffffu, lane < k && (e.y & INFO_AMB));
     uint4 wrec = make_uint4(0u, 0u, 0u, 0u);
-    if (ACC ? (lane < k && (e.y & (INFO_AMB | INFO_MAC))) : ((amb >> lane) & 1u)) wrec = __ldg(&a.walk[e.w]);
-    while (amb) {
-      const int src = __ffs(amb) - 1;
-      amb &= amb - 1;
-      const uint32_t node = __shfl_sync(0xffffffffu, e.w, src);
-      const uint32_t me = __shfl_sync(0xffffffffu, e.z, src);
-      const int dep = wn_depth(__shfl_sync(0xffffffffu, e.y, src));
-      const uint32_t wq[3] = {__shfl_sync(0xffffffffu, wrec.x, src), __shfl_sync(0xffffffffu, wrec.y, src),
-                              __shfl_sync(0xffffffffu, wrec.z, src)};
-      bool pass = false;
-      if (has && lane < TPW && ((me >> tgt) & 1u)) {
-        const float h = ldexpf(a.h0_u, (ACC ? 1 : 0) - dep);
-        float s = 0.f;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          float dd = (float)rel32(wq[d], tq[d], a.periodic) * a.u_inv;
-          float ee = fmaxf(fabsf(dd) - h, 0.f);
-          s = fmaf(ee, ee, s);
-        }
-        if (s <= a.rc2_lo) pass = true;
-        else if (!ACC && s <= a.rc2_hi) {
-          pass = exact_open_pass(a, p, node);
-          ++nexact;
-        }
-      }
-      const uint32_t nm = __ballot_sync(0xffffffffu, pass);  // lanes < TPW hold the targets
-      if (lane == src) e.z = nm;
-    }
+    if (ACC && lane < k && (e.y & INFO_MAC)) wrec = __ldg(&a.walk[e.w]);
     // accurate mode: per-target opening angle for nodes undecided for the
     // group; targets that accept take the node as a monopole now, the rest
     // open it
@@ -500,7 +529,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const int dep = wn_depth(__shfl_sync(0xffffffffu, e.y, src));
       const uint4 w = make_uint4(__shfl_sync(0xffffffffu, wrec.x, src), __shfl_sync(0xffffffffu, wrec.y, src),
                                  __shfl_sync(0xffffffffu, wrec.z, src), __shfl_sync(0xffffffffu, wrec.w, src));
-      const float hnode = ldexpf(a.h0_u, -dep);
+      const float hnode = half_side(a.h0_u, dep);
       bool accept = false;
       if (has && lane < TPW && ((me >> tgt) & 1u)) {
         float d2 = 0.f;
@@ -579,7 +608,11 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
   }
 }
 
-template <bool ACC> constexpr size_t walk_smem_per_warp() { return sizeof(Entry) * (CHUNK_L + chunk_m<ACC>()) + 32; }
+// per warp: the leaf and monopole lists, 32 staged undecided nodes (float4
+// position + uint4 mask / node / image flag), the child-owner bytes
+template <bool ACC> constexpr size_t walk_smem_per_warp() {
+  return sizeof(Entry) * (CHUNK_L + chunk_m<ACC>()) + 32 * (sizeof(float4) + sizeof(uint4)) + 32;
+}
 
 template <int MIN_BLOCKS, int TPW, bool ACC>
 __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
@@ -588,7 +621,9 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
   unsigned char* mine = s_walk + wid * walk_smem_per_warp<ACC>();
   Entry* list_l = reinterpret_cast<Entry*>(mine);
   Entry* list_m = list_l + CHUNK_L;
-  uint8_t* owner = reinterpret_cast<uint8_t*>(list_m + chunk_m<ACC>());
+  float4* rpos = reinterpret_cast<float4*>(list_m + chunk_m<ACC>());
+  uint4* rmask = reinterpret_cast<uint4*>(rpos + 32);
+  uint8_t* owner = reinterpret_cast<uint8_t*>(rmask + 32);
   const int64_t gw = (int64_t)blockIdx.x * WALK_WARPS + wid;
   StackEntry* stk = reinterpret_cast<StackEntry*>(a.stack) + gw * STACK_ENTRIES;
   for (;;) {
@@ -613,9 +648,10 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
     }
     wide = wide || a.single_target;
     if (!wide) {
-      walk_targets<TPW, ACC>(a, first, count, list_l, list_m, owner, stk);
+      walk_targets<TPW, ACC>(a, first, count, list_l, list_m, owner, stk, rpos, rmask);
     } else {
-      for (uint32_t t = 0; t < count; ++t) walk_targets<TPW, ACC>(a, first + t, 1u, list_l, list_m, owner, stk);
+      for (uint32_t t = 0; t < count; ++t)
+        walk_targets<TPW, ACC>(a, first + t, 1u, list_l, list_m, owner, stk, rpos, rmask);
     }
   }
 }
