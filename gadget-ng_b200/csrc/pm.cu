@@ -449,8 +449,10 @@ inline int ilog2(int n) {
 // CIC assignment of power_spectrum.rs:146-166: fx = x / cell, floor, weights
 // (1 - t, t), indices rem_euclid(n), m * wx * wy * wz; stored z-major like the
 // PM mesh (the binned spectrum does not depend on the axis order).
-__device__ __forceinline__ void pk_deposit_one(double x, double y, double z, double m, double cell, int nm,
-                                               float* __restrict__ rho) {
+// CIC cells and weights of power_spectrum.rs:146-166 (float64, division by
+// the cell size), the eight corners in (dx, dy, dz) order.
+__device__ __forceinline__ void pk_cic(double x, double y, double z, double m, double cell, int nm, int64_t idx[8],
+                                       float w[8]) {
   const double f[3] = {ddiv(x, cell), ddiv(y, cell), ddiv(z, cell)};
   int i0[3];
   double t[3];
@@ -460,6 +462,7 @@ __device__ __forceinline__ void pk_deposit_one(double x, double y, double z, dou
     i0[d] = (int)fl;
     t[d] = dsub(f[d], fl);
   }
+  const int msk = nm - 1;  // nm is a power of two: & wraps negative indices too (rem_euclid)
 #pragma unroll
   for (int dx = 0; dx < 2; ++dx)
 #pragma unroll
@@ -468,25 +471,65 @@ __device__ __forceinline__ void pk_deposit_one(double x, double y, double z, dou
       for (int dz = 0; dz < 2; ++dz) {
         const double wx = dx ? t[0] : dsub(1.0, t[0]), wy = dy ? t[1] : dsub(1.0, t[1]);
         const double wz = dz ? t[2] : dsub(1.0, t[2]);
-        const int jx = ((i0[0] + dx) % nm + nm) % nm, jy = ((i0[1] + dy) % nm + nm) % nm,
-                  jz = ((i0[2] + dz) % nm + nm) % nm;
-        atomicAdd(&rho[((int64_t)jz * nm + jy) * nm + jx], (float)dmul(dmul(dmul(m, wx), wy), wz));
+        const int jx = (i0[0] + dx) & msk, jy = (i0[1] + dy) & msk, jz = (i0[2] + dz) & msk;
+        const int k = dx * 4 + dy * 2 + dz;
+        idx[k] = ((int64_t)jz * nm + jy) * nm + jx;
+        w[k] = (float)dmul(dmul(dmul(m, wx), wy), wz);
       }
+}
+
+// Add the eight corner weights of each live lane; lanes whose particles share
+// a base cell sum their weights in registers first (warp match), so one lane
+// per cell issues the eight atomics.
+__device__ __forceinline__ void pk_add_aggregated(bool live, const int64_t idx[8], const float w[8], float* rho) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t key = live ? (uint32_t)idx[0] : 0xFFFFFFFFu;
+  const uint32_t peers = __match_any_sync(0xffffffffu, key);
+  const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
+  if (rounds == 1) {
+    if (!live) return;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) atomicAdd(&rho[idx[k]], w[k]);
+    return;
+  }
+  float sum[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) sum[k] = 0.f;
+  uint32_t rest = peers;
+  for (int r = 0; r < rounds; ++r) {  // the same count on every lane: full-warp shuffles
+    const int src = rest ? __ffs(rest) - 1 : lane;
+    const bool take = rest != 0u;
+    rest &= rest - 1u;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float v = __shfl_sync(0xffffffffu, w[k], src);
+      if (take) sum[k] += v;
+    }
+  }
+  if (!live || lane != __ffs(peers) - 1) return;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) atomicAdd(&rho[idx[k]], sum[k]);
 }
 
 __global__ void k_pk_deposit_pos(const double* __restrict__ pos, const double* __restrict__ m, int64_t n,
                                  double cell, int nm, float* __restrict__ rho) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  pk_deposit_one(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], m[i], cell, nm, rho);
+  const bool live = i < n;
+  int64_t idx[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  float w[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (live) pk_cic(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], m[i], cell, nm, idx, w);
+  pk_add_aggregated(live, idx, w, rho);
 }
 
 __global__ void k_pk_deposit_q(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
                                const uint32_t* __restrict__ qz, const double* __restrict__ m, int64_t n,
                                double scale, double cell, int nm, float* __restrict__ rho) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  pk_deposit_one(decode(qx[i], scale), decode(qy[i], scale), decode(qz[i], scale), m[i], cell, nm, rho);
+  const bool live = i < n;
+  int64_t idx[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  float w[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (live) pk_cic(decode(qx[i], scale), decode(qy[i], scale), decode(qz[i], scale), m[i], cell, nm, idx, w);
+  pk_add_aggregated(live, idx, w, rho);
 }
 
 __device__ __forceinline__ double pk_sinc(int k, int nm) {
