@@ -137,14 +137,15 @@ def measured_peaks():
         return {}
 
 
+# DRAM bytes (read + write) of one k_walk launch, from single-pass ncu captures of
+# dram__bytes_read.sum / dram__bytes_write.sum (profiles/k_walk_dram_clustered256.md,
+# profiles/k_walk_treepm128.md).
+WALK_DRAM_BYTES = {"clustered256_L200": 963312384 + 368289792, "treepm128_L100": 144405760 + 69206272}
+
+
 def profile_traffic(workload):
-    """DRAM bytes per walk launch from the committed ncu summary, if any."""
-    try:
-        with open(os.path.join(REPO, "profiles", "walk_traffic.json")) as f:
-            d = json.load(f)
-        return d.get(workload, {}).get("dram_bytes_per_launch")
-    except (OSError, ValueError):
-        return None
+    """DRAM bytes per walk launch measured by ncu for this workload, if captured."""
+    return WALK_DRAM_BYTES.get(workload)
 
 
 def cpu_sample(box, mesh, phys, n_targets, threads):
