@@ -148,6 +148,25 @@ def profile_traffic(workload):
     return WALK_DRAM_BYTES.get(workload)
 
 
+def stage_rooflines(stage_ms, n, mesh):
+    """HBM rooflines of the memory-bound stages from their algorithmic bytes per
+    evaluation (keys + radix sort 68 B per particle; PM deposit + forward +
+    three inverse transforms 12 N + 36 N_c with the spectral step fused; gather
+    + kick 12 N_c + 36 N) against the measured copy bandwidth."""
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    nc = mesh ** 3
+    out = {}
+    for name, key, nbytes in (("keys_sort", ("ms_bbox_keys", "ms_sort"), 68 * n),
+                              ("pm", ("ms_pm",), 12 * n + 36 * nc),
+                              ("gather_kick", ("ms_gather_kick",), 12 * nc + 36 * n)):
+        ms = sum(stage_ms.get(k, 0.0) for k in key)
+        if ms > 0:
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            out[name] = {"bytes": nbytes, "ms": ms, "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak}
+    out["peak_source"] = "MEASURED_PEAKS.json hbm_gbs (measured)" if measured_peaks().get("hbm_gbs") else "fallback"
+    return out
+
+
 def cpu_sample(box, mesh, phys, n_targets, threads):
     """The oracle restatement on a bounded sample: full PM + full tree build +
     the walk of n_targets seeded targets, extrapolated to all particles."""
@@ -506,6 +525,8 @@ def run_b200(args):
     achieved = inter * FLOP_PER_INTERACTION / (wms * 1e-3) / 1e12
     peak = None if args.no_peak else fp32_peak_tflops(solver)
     st = stats[-1]
+    stage_ms = {k: float(np.mean([s[k] for s in stats])) for k in
+                ("ms_bbox_keys", "ms_sort", "ms_build", "ms_walk", "ms_pm", "ms_gather_kick", "ms_total")}
     line = {
         "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -517,8 +538,8 @@ def run_b200(args):
                    "l2": "inputs larger than L2 (>= 0.8 GB touched per step)"},
         "per_force_evaluation": {"value": value, "note": "one force evaluation per fused step; the reference "
                                                          "evaluates twice per step"},
-        "stage_ms": {k: float(np.mean([s[k] for s in stats])) for k in
-                     ("ms_bbox_keys", "ms_sort", "ms_build", "ms_walk", "ms_pm", "ms_gather_kick", "ms_total")},
+        "stage_ms": stage_ms,
+        "stage_roofline": stage_rooflines(stage_ms, n, mesh),
         "walk": {"interactions_per_step": inter, "evaluated_pairs_per_step": evaluated,
                  "interactions_per_particle": inter / n, "exact_fallbacks": st["exact_fallbacks"],
                  "tree_nodes": st["n_tree_nodes"], "groups": st["n_groups"], "max_depth": st["max_tree_depth"]},
