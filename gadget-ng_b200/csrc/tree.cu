@@ -320,79 +320,118 @@ __device__ __forceinline__ void child_moments(uint32_t c, double scale, const ui
   }
 }
 
-__global__ void k_aggregate(int64_t n, double scale, const uint32_t* __restrict__ qx,
-                            const uint32_t* __restrict__ qy, const uint32_t* __restrict__ qz,
-                            const double* __restrict__ pmass, const int32_t* __restrict__ leaf_oparent,
-                            const int32_t* __restrict__ o_parent, const uint32_t* __restrict__ slots,
-                            const uint32_t* __restrict__ nchild, uint32_t* __restrict__ cnt, double* o_mass,
-                            double* o_com, double* o_quad) {
-  int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  int32_t P = leaf_oparent[p];
-  for (int guard = 0; P >= 0; ++guard) {
-    if (guard > 2 * KEY_LEVELS + 4) return;  // deeper than any key can describe: malformed tree
-    // release this thread's node before counting it in (a leaf wrote nothing)
-    if (guard > 0) __threadfence();
-    const uint32_t arrived = atomicAdd(&cnt[P], 1u);
-    if (arrived + 1 != nchild[P]) return;  // another child finishes this node
-    __threadfence();
-    // pass 1: mass and centre of mass over the children in octant order
-    uint32_t cs[8];
-    double mt = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      const uint32_t c = slots[(int64_t)P * 8 + s];
-      cs[s] = c;
-      if (c == EMPTY_SLOT) continue;
-      double m, x, y, z;
-      child_moments(c, scale, qx, qy, qz, pmass, o_mass, o_com, &m, &x, &y, &z);
-      mt = dadd(mt, m);
-      ax = dadd(ax, dmul(x, m));
-      ay = dadd(ay, dmul(y, m));
-      az = dadd(az, dmul(z, m));
+// Internal nodes by depth: per-block histograms, then one reserved range per
+// (block, depth) into the depth buckets (the order inside a bucket is free).
+__global__ void k_depth_count(int64_t n_int, const uint8_t* __restrict__ o_depth, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t sh[DEPTH_BINS];
+  if (threadIdx.x < DEPTH_BINS) sh[threadIdx.x] = 0u;
+  __syncthreads();
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n_int) atomicAdd(&sh[o_depth[i] & (DEPTH_BINS - 1)], 1u);
+  __syncthreads();
+  if (threadIdx.x < DEPTH_BINS && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+}
+
+// hist -> exclusive offsets (DEPTH_BINS + 1) and cursors; one warp
+__global__ void k_depth_offsets(uint32_t* tab) {
+  uint32_t* hist = tab;
+  uint32_t* off = tab + DEPTH_BINS;
+  uint32_t* cur = tab + 2 * DEPTH_BINS + 1;
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int d = 0; d < DEPTH_BINS; ++d) {
+      off[d] = acc;
+      cur[d] = acc;
+      acc += hist[d];
     }
-    double comx = 0.0, comy = 0.0, comz = 0.0;
-    if (mt > 0.0) {
-      comx = ddiv(ax, mt);
-      comy = ddiv(ay, mt);
-      comz = ddiv(az, mt);
-    }
-    // pass 2: quadrupole by the parallel-axis theorem (outer_traceless :197-207);
-    // the children are read again (cache hits) rather than held in registers
-    double qd[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll 1
-    for (int s = 0; s < 8; ++s) {
-      const uint32_t c = cs[s];
-      if (c == EMPTY_SLOT) continue;
-      double m, x, y, z;
-      child_moments(c, scale, qx, qy, qz, pmass, o_mass, o_com, &m, &x, &y, &z);
-      if (m == 0.0) continue;
-      const double sx = dsub(x, comx), sy = dsub(y, comy), sz = dsub(z, comz);
-      const double s2 = dadd(dadd(dmul(sx, sx), dmul(sy, sy)), dmul(sz, sz));
-      const double m3 = dmul(m, 3.0);
-      double oq[6];
-      oq[0] = dmul(m, dsub(dmul(dmul(3.0, sx), sx), s2));
-      oq[1] = dmul(dmul(m3, sx), sy);
-      oq[2] = dmul(dmul(m3, sx), sz);
-      oq[3] = dmul(m, dsub(dmul(dmul(3.0, sy), sy), s2));
-      oq[4] = dmul(dmul(m3, sy), sz);
-      oq[5] = dmul(m, dsub(dmul(dmul(3.0, sz), sz), s2));
-      if (c & LEAF_BIT) {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) qd[k] = dadd(qd[k], dadd(0.0, oq[k]));
-      } else {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) qd[k] = dadd(qd[k], dadd(__ldcg(&o_quad[6 * (int64_t)c + k]), oq[k]));
-      }
-    }
-    __stcg(&o_mass[P], mt);
-    __stcg(&o_com[3 * (int64_t)P], comx);
-    __stcg(&o_com[3 * (int64_t)P + 1], comy);
-    __stcg(&o_com[3 * (int64_t)P + 2], comz);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) __stcg(&o_quad[6 * (int64_t)P + k], qd[k]);
-    P = o_parent[P];
+    off[DEPTH_BINS] = acc;
   }
+}
+
+__global__ void k_depth_scatter(int64_t n_int, const uint8_t* __restrict__ o_depth, uint32_t* __restrict__ cur,
+                                uint32_t* __restrict__ by_depth) {
+  __shared__ uint32_t cnt[DEPTH_BINS], base[DEPTH_BINS];
+  if (threadIdx.x < DEPTH_BINS) cnt[threadIdx.x] = 0u;
+  __syncthreads();
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int d = 0;
+  uint32_t r = 0;
+  if (i < n_int) {
+    d = o_depth[i] & (DEPTH_BINS - 1);
+    r = atomicAdd(&cnt[d], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < DEPTH_BINS && cnt[threadIdx.x]) base[threadIdx.x] = atomicAdd(&cur[threadIdx.x], cnt[threadIdx.x]);
+  __syncthreads();
+  if (i < n_int) by_depth[base[d] + r] = (uint32_t)i;
+}
+
+// Moments of the internal nodes at one depth (octree.rs:547-629) from their
+// children, which are leaves or nodes one level deeper (finished by the
+// previous launch): mass and centre of mass summed over the children in
+// octant order, then the quadrupole by the parallel-axis theorem
+// (outer_traceless :197-207), all float64 in the reference's operation order.
+__global__ void k_aggregate_level(const uint32_t* __restrict__ nodes, int64_t count, double scale,
+                                  const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                                  const uint32_t* __restrict__ qz, const double* __restrict__ pmass,
+                                  const uint32_t* __restrict__ slots, double* o_mass, double* o_com, double* o_quad) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint32_t P = nodes[i];
+  // pass 1: mass and centre of mass over the children in octant order
+  uint32_t cs[8];
+  double mt = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const uint32_t c = slots[(int64_t)P * 8 + s];
+    cs[s] = c;
+    if (c == EMPTY_SLOT) continue;
+    double m, x, y, z;
+    child_moments(c, scale, qx, qy, qz, pmass, o_mass, o_com, &m, &x, &y, &z);
+    mt = dadd(mt, m);
+    ax = dadd(ax, dmul(x, m));
+    ay = dadd(ay, dmul(y, m));
+    az = dadd(az, dmul(z, m));
+  }
+  double comx = 0.0, comy = 0.0, comz = 0.0;
+  if (mt > 0.0) {
+    comx = ddiv(ax, mt);
+    comy = ddiv(ay, mt);
+    comz = ddiv(az, mt);
+  }
+  // pass 2: the children are read again (cache hits) rather than held in registers
+  double qd[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+  for (int s = 0; s < 8; ++s) {
+    const uint32_t c = cs[s];
+    if (c == EMPTY_SLOT) continue;
+    double m, x, y, z;
+    child_moments(c, scale, qx, qy, qz, pmass, o_mass, o_com, &m, &x, &y, &z);
+    if (m == 0.0) continue;
+    const double sx = dsub(x, comx), sy = dsub(y, comy), sz = dsub(z, comz);
+    const double s2 = dadd(dadd(dmul(sx, sx), dmul(sy, sy)), dmul(sz, sz));
+    const double m3 = dmul(m, 3.0);
+    double oq[6];
+    oq[0] = dmul(m, dsub(dmul(dmul(3.0, sx), sx), s2));
+    oq[1] = dmul(dmul(m3, sx), sy);
+    oq[2] = dmul(dmul(m3, sx), sz);
+    oq[3] = dmul(m, dsub(dmul(dmul(3.0, sy), sy), s2));
+    oq[4] = dmul(dmul(m3, sy), sz);
+    oq[5] = dmul(m, dsub(dmul(dmul(3.0, sz), sz), s2));
+    if (c & LEAF_BIT) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) qd[k] = dadd(qd[k], dadd(0.0, oq[k]));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) qd[k] = dadd(qd[k], dadd(__ldcg(&o_quad[6 * (int64_t)c + k]), oq[k]));
+    }
+  }
+  __stcg(&o_mass[P], mt);
+  __stcg(&o_com[3 * (int64_t)P], comx);
+  __stcg(&o_com[3 * (int64_t)P + 1], comy);
+  __stcg(&o_com[3 * (int64_t)P + 2], comz);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) __stcg(&o_quad[6 * (int64_t)P + k], qd[k]);
 }
 
 __global__ void k_walk_nodes(int64_t n_int, double inv_scale, const double* __restrict__ o_mass,
@@ -660,12 +699,35 @@ void launch_octree_links(int64_t n, int64_t n_int, TreeBuffers& t, void* scan_sc
   TPM_LAUNCH_CHECK();
 }
 
+// Level by level from the deepest internal nodes to the root: each launch
+// finishes one depth, so every node reads finished children without atomics
+// or fences.  One host synchronisation brings the per-depth counts back.
 void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, TreeBuffers& t, cudaStream_t s) {
-  TPM_CUDA(cudaMemsetAsync(t.o_cnt, 0, (size_t)n_int * sizeof(uint32_t), s));
-  k_aggregate<<<grid_for(n, 128, 1ll << 30), 128, 0, s>>>(n, box / TWO32, p.qx, p.qy, p.qz, p.mass, t.leaf_oparent,
-                                                          t.o_parent, t.o_slots, t.o_nchild, t.o_cnt, t.o_mass,
-                                                          t.o_com, t.o_quad);
+  (void)n;
+  if (n_int <= 0) return;
+  uint32_t* hist = t.depth_tab;
+  TPM_CUDA(cudaMemsetAsync(hist, 0, DEPTH_BINS * sizeof(uint32_t), s));
+  k_depth_count<<<grid_for(n_int, 256, 1ll << 30), 256, 0, s>>>(n_int, t.o_depth, hist);
   TPM_LAUNCH_CHECK();
+  k_depth_offsets<<<1, 32, 0, s>>>(t.depth_tab);
+  TPM_LAUNCH_CHECK();
+  uint32_t counts[DEPTH_BINS];
+  TPM_CUDA(cudaMemcpyAsync(counts, hist, sizeof(counts), cudaMemcpyDeviceToHost, s));
+  k_depth_scatter<<<grid_for(n_int, 256, 1ll << 30), 256, 0, s>>>(n_int, t.o_depth, t.depth_tab + 2 * DEPTH_BINS + 1,
+                                                                   t.o_cnt);
+  TPM_LAUNCH_CHECK();
+  TPM_CUDA(cudaStreamSynchronize(s));
+  int64_t offset[DEPTH_BINS + 1];
+  offset[0] = 0;
+  for (int d = 0; d < DEPTH_BINS; ++d) offset[d + 1] = offset[d] + counts[d];
+  if (offset[DEPTH_BINS] != n_int) throw Error(2, "octree depth buckets do not add up to the node count");
+  for (int d = DEPTH_BINS - 1; d >= 0; --d) {
+    if (counts[d] == 0) continue;
+    k_aggregate_level<<<grid_for(counts[d], 128, 1ll << 30), 128, 0, s>>>(
+        t.o_cnt + offset[d], counts[d], box / TWO32, p.qx, p.qy, p.qz, p.mass, t.o_slots, t.o_mass, t.o_com,
+        t.o_quad);
+    TPM_LAUNCH_CHECK();
+  }
   k_walk_nodes<<<grid_for(n_int, 256, 1ll << 30), 256, 0, s>>>(n_int, TWO32 / box, t.o_mass, t.o_com, t.o_walk);
   TPM_LAUNCH_CHECK();
 }

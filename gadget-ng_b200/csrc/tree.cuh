@@ -74,7 +74,7 @@ struct TreeBuffers {
   uint32_t* o_slots;  // 8 per node, EMPTY_SLOT or child id (LEAF_BIT | particle)
   uint32_t* o_nchild;
   uint32_t* o_child_first;
-  uint32_t* o_cnt;
+  uint32_t* o_cnt;      // internal node ids bucketed by depth (aggregation order)
   uint32_t* child_ids;  // compacted, same encoding as o_slots
   double* o_mass;
   double* o_com;   // 3 per node
@@ -94,8 +94,11 @@ struct TreeBuffers {
   TreeParams* params;
   uint32_t* bbox;       // 6 words
   uint32_t* scalars;    // [0] octree internal count, [1] groups, [2] max depth, [3] child total
+  uint32_t* depth_tab;  // DEPTH_BINS counts, offsets, cursors of internal nodes per depth
   uint32_t* err;
 };
+
+constexpr int DEPTH_BINS = 64;  // octree depths are at most KEY_LEVELS
 
 void launch_bbox_root(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s);
 void launch_tree_keys(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s);

@@ -776,6 +776,7 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
     h->T.params = h->alloc<TreeParams>(1, 0);
     h->T.bbox = h->alloc<uint32_t>(6, 0);
     h->T.scalars = h->alloc<uint32_t>(8, 0);
+    h->T.depth_tab = h->alloc<uint32_t>(3 * DEPTH_BINS + 1, 0);
     h->T.err = h->alloc<uint32_t>(1, 0);
     h->stats_dev = h->alloc<unsigned long long>(8, 0);
     h->work = h->alloc<uint32_t>(1, 0);
