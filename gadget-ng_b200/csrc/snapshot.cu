@@ -26,6 +26,7 @@
 #include <charconv>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <string>
 #include <thread>
 #include <vector>
@@ -318,16 +319,39 @@ void format_jsonl(const HostRecords& r, int64_t lo, int64_t hi, std::string& out
   }
 }
 
-// Format n records with every host thread and append them to f in order.
-void write_jsonl_block(File& f, const HostRecords& r, int64_t n, std::vector<std::string>& bufs) {
-  const unsigned t = host_threads();
-  bufs.resize(t);
-  std::vector<std::thread> pool;
-  for (unsigned k = 0; k < t; ++k)
-    pool.emplace_back([&, k] { format_jsonl(r, n * k / t, n * (k + 1) / t, bufs[k]); });
-  for (auto& th : pool) th.join();
-  for (unsigned k = 0; k < t; ++k) f.write(bufs[k].data(), bufs[k].size());
-}
+// JSONL blocks appended in order: each block is formatted by every host
+// thread, then written by a background task while the next block is
+// formatted (two sets of buffers).
+class JsonlStream {
+ public:
+  explicit JsonlStream(File& f) : f_(f) {}
+  ~JsonlStream() {
+    if (pending_.valid()) pending_.wait();
+  }
+  void push(const HostRecords& r, int64_t n) {
+    std::vector<std::string>& bufs = bufs_[slot_];
+    const unsigned t = host_threads();
+    bufs.resize(t);
+    std::vector<std::thread> pool;
+    for (unsigned k = 0; k < t; ++k)
+      pool.emplace_back([&, k] { format_jsonl(r, n * k / t, n * (k + 1) / t, bufs[k]); });
+    for (auto& th : pool) th.join();
+    if (pending_.valid()) pending_.get();  // the previous block is on disk; rethrows its error
+    pending_ = std::async(std::launch::async, [this, &bufs] {
+      for (const std::string& b : bufs) f_.write(b.data(), b.size());
+    });
+    slot_ ^= 1;
+  }
+  void finish() {
+    if (pending_.valid()) pending_.get();
+  }
+
+ private:
+  File& f_;
+  std::vector<std::string> bufs_[2];
+  int slot_ = 0;
+  std::future<void> pending_;
+};
 
 // ---- bincode ----------------------------------------------------------------------
 __host__ __device__ inline int varint_size(uint64_t u) {
@@ -632,7 +656,7 @@ void snapshot_write(const std::string& dir, int32_t format, const tpm_snapshot_e
     // per buffer: chunk x (3 + 3 + 1) doubles; copy chunk c + 1 while chunk c is formatted
     Pinned host(2 * (size_t)chunk * 7 * sizeof(double));
     Event ev[2];
-    std::vector<std::string> bufs;
+    JsonlStream js(f);
     auto issue = [&](int64_t lo, int slot) {
       const int64_t m = std::min(chunk, n - lo);
       double* h = (double*)host.p + (size_t)slot * chunk * 7;
@@ -648,8 +672,9 @@ void snapshot_write(const std::string& dir, int32_t format, const tpm_snapshot_e
       if (lo + chunk < n) issue(lo + chunk, slot ^ 1);
       const double* h = (const double*)host.p + (size_t)slot * chunk * 7;
       const HostRecords r{h, h + 3 * chunk, h + 6 * chunk, nullptr, (uint64_t)lo};
-      write_jsonl_block(f, r, std::min(chunk, n - lo), bufs);
+      js.push(r, std::min(chunk, n - lo));
     }
+    js.finish();
     f.close();
   } else {
     File f(dir + "/particles.bin", "wb");
@@ -692,12 +717,13 @@ void snapshot_write_host(const std::string& dir, int32_t format, const double* p
   const HostRecords r{pos, vel, mass, ids, 0};
   if (format == TPM_SNAPSHOT_JSONL) {
     File f(dir + "/particles.jsonl", "wb");
-    std::vector<std::string> bufs;
+    JsonlStream js(f);
     const int64_t chunk = 1 << 20;
     for (int64_t lo = 0; lo < n; lo += chunk) {
       const HostRecords c{pos + 3 * lo, vel + 3 * lo, mass + lo, ids ? ids + lo : nullptr, (uint64_t)lo};
-      write_jsonl_block(f, c, std::min(chunk, n - lo), bufs);
+      js.push(c, std::min(chunk, n - lo));
     }
+    js.finish();
     f.close();
   } else {
     File f(dir + "/particles.bin", "wb");
