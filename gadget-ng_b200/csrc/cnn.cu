@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv_tc(const __nv_bfloat16* _
                                                           __nv_bfloat16* __restrict__ zout,
                                                           const __nv_bfloat16* __restrict__ zprev,
                                                           const uint4* __restrict__ wpack,
-                                                          const float* __restrict__ bias, uint32_t* err) {
+                                                          const float* __restrict__ bias, uint32_t* err, int issue) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint4* s_in = reinterpret_cast<uint4*>(smem);
   uint4* s_w = reinterpret_cast<uint4*>(smem + SIN_BYTES);
@@ -194,7 +194,9 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv_tc(const __nv_bfloat16* _
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *s_tmem;
 
-  if (tid == 0) {
+  // issue == 0 (the bounded-wait self-test): no MMA and no commit, so the
+  // mbarrier never completes and the wait below must give up and report
+  if (tid == 0 && issue) {
     const uint32_t a0 = smem_u32(s_in), w0 = smem_u32(s_w);
     for (int zz = 0; zz < TZ; ++zz) {
 #pragma unroll 1
@@ -515,11 +517,59 @@ static void conv_launch(bool bwd, const __nv_bfloat16* in, Vol vin, int pad, __n
                   (unsigned)vout.b);
   if (bwd)
     k_conv_tc<true><<<grid, CONV_THREADS, CONV_SMEM, s>>>(in, vin, pad, out, vout.z, vout.y, vout.x, zout, zprev, w,
-                                                           bias, err);
+                                                           bias, err, 1);
   else
     k_conv_tc<false><<<grid, CONV_THREADS, CONV_SMEM, s>>>(in, vin, pad, out, vout.z, vout.y, vout.x, zout, zprev,
-                                                            w, bias, err);
+                                                            w, bias, err, 1);
   TPM_LAUNCH_CHECK();
+}
+
+// One conv tile whose tensor-core work is never issued, then one normal tile:
+// the first must end by its wait's time limit with DEV_ERR_MMA_TIMEOUT set
+// (TMEM freed, nothing in flight), the second must run cleanly on the same
+// context.  Returns the seconds the first launch took; throws on a failure.
+double conv_wait_selftest(cudaStream_t s) {
+  conv_launch(false, nullptr, Vol{0, 0, 0, 0}, 0, nullptr, Vol{0, 0, 0, 0}, nullptr, nullptr, nullptr, nullptr,
+              nullptr, s);  // sets the shared-memory attribute only
+  const Vol vin{1, TZ + 2, TY + 2, TX + 2};
+  const int64_t in_bytes = vin.nodes() * CH * 2, out_bytes = (int64_t)TZ * TY * TX * CH * 2;
+  char* buf = nullptr;
+  const size_t total = (size_t)(in_bytes + out_bytes) + WPACK_U4 * 16 + CH * 4 + 16;
+  TPM_CUDA(cudaMalloc(&buf, total));
+  struct Free {
+    char* p;
+    ~Free() { cudaFree(p); }
+  } guard{buf};
+  TPM_CUDA(cudaMemsetAsync(buf, 0, total, s));
+  auto* in = reinterpret_cast<__nv_bfloat16*>(buf);
+  auto* out = reinterpret_cast<__nv_bfloat16*>(buf + in_bytes);
+  auto* w = reinterpret_cast<uint4*>(buf + in_bytes + out_bytes);
+  auto* bias = reinterpret_cast<float*>(buf + in_bytes + out_bytes + WPACK_U4 * 16);
+  auto* err = reinterpret_cast<uint32_t*>(buf + in_bytes + out_bytes + WPACK_U4 * 16 + CH * 4);
+  cudaEvent_t e0, e1;
+  TPM_CUDA(cudaEventCreate(&e0));
+  TPM_CUDA(cudaEventCreate(&e1));
+  TPM_CUDA(cudaEventRecord(e0, s));
+  k_conv_tc<false><<<dim3(1, 1, 1), CONV_THREADS, CONV_SMEM, s>>>(in, vin, 0, out, TZ, TY, TX, nullptr, nullptr, w,
+                                                                   bias, err, 0);
+  TPM_LAUNCH_CHECK();
+  TPM_CUDA(cudaEventRecord(e1, s));
+  uint32_t flag = 0;
+  TPM_CUDA(cudaMemcpyAsync(&flag, err, 4, cudaMemcpyDeviceToHost, s));
+  TPM_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  TPM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!(flag & DEV_ERR_MMA_TIMEOUT)) throw Error(2, "the unissued tensor-core wait was not reported");
+  TPM_CUDA(cudaMemsetAsync(err, 0, 4, s));
+  k_conv_tc<false><<<dim3(1, 1, 1), CONV_THREADS, CONV_SMEM, s>>>(in, vin, 0, out, TZ, TY, TX, nullptr, nullptr, w,
+                                                                   bias, err, 1);
+  TPM_LAUNCH_CHECK();
+  TPM_CUDA(cudaMemcpyAsync(&flag, err, 4, cudaMemcpyDeviceToHost, s));
+  TPM_CUDA(cudaStreamSynchronize(s));
+  if (flag != 0) throw Error(2, "a normal tensor-core tile failed after the timed-out one");
+  return ms * 1e-3;
 }
 
 void conv_forward(const __nv_bfloat16* in, Vol vin, __nv_bfloat16* out, __nv_bfloat16* zout, const uint4* wpack,

@@ -50,6 +50,9 @@ void conv_forward(const __nv_bfloat16* in, Vol vin, __nv_bfloat16* out, __nv_bfl
 // GELU'(zprev[i]) * sum_t W[t]^T dz[i - t] (a full convolution, dims + 2).
 void conv_backward_data(const __nv_bfloat16* dz, Vol vdz, __nv_bfloat16* dzprev, const __nv_bfloat16* zprev,
                         const uint4* wpack_bwd, uint32_t* err, cudaStream_t s);
+// Self-test of the tensor-core wait's time limit (one tile with no MMA issued,
+// then a normal tile); returns the seconds the timed-out launch took.
+double conv_wait_selftest(cudaStream_t s);
 // Weight and bias gradients of a valid convolution (accumulated, FP32).
 void conv_backward_weights(const __nv_bfloat16* x, Vol vin, const __nv_bfloat16* dz, int cin, float* dw, float* db,
                            cudaStream_t s);

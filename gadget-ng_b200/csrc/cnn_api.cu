@@ -802,4 +802,24 @@ int tpm_cnn_evaluate(tpm_cnn* c, int32_t held_out, int32_t batch, float* loss) {
   return TPM_OK;
 }
 
+int tpm_selftest_bounded_wait(int32_t device, double* waited_seconds) {
+  try {
+    TPM_CUDA(cudaSetDevice(device));
+    cudaStream_t s;
+    TPM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    double t = 0.0;
+    try {
+      t = cn::conv_wait_selftest(s);
+    } catch (...) {
+      cudaStreamDestroy(s);
+      throw;
+    }
+    cudaStreamDestroy(s);
+    if (waited_seconds) *waited_seconds = t;
+  } catch (const Error& e) {
+    return e.code;
+  }
+  return TPM_OK;
+}
+
 }  // extern "C"

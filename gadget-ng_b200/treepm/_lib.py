@@ -189,6 +189,7 @@ SIGNATURES = {
     "tpm_power_spectrum": ([_P, _P, _I64, _D, C.c_int32, C.c_int32, _P, _P, _P], _I),
     "tpm_get_power_spectrum": ([_P, _P, _P, _P], _I),
     "tpm_set_particles_zeldovich": ([_P, _P], _I),
+    "tpm_selftest_bounded_wait": ([C.c_int32, _P], _I),
     "tpm_write_snapshot": ([_P, C.c_char_p, C.c_int32, _P, _P], _I),
     "tpm_read_snapshot": ([_P, C.c_char_p, C.c_int32, _P], _I),
     "tpm_write_snapshot_host": ([C.c_char_p, C.c_int32, _P, _P, _P, _P, _I64, _P, _P], _I),

@@ -367,6 +367,11 @@ int tpm_read_checkpoint(tpm_handle* h, const char* resume_dir, uint64_t* complet
  * Wh (3,16), bh (3)]; tap t = (dz*3 + dy)*3 + dx reads node o + (dx,dy,dz).
  * Host arrays are copied synchronously. */
 typedef struct tpm_cnn tpm_cnn;
+/* Failure-detection self-test of the tensor-core kernels' bounded waits: one
+ * tile whose MMAs are never issued must end by its wait's 2 s limit with the
+ * timeout flag set and its TMEM freed, and a normal tile must then run on the
+ * same context.  TPM_OK with the seconds the first tile took, else an error. */
+int tpm_selftest_bounded_wait(int32_t device, double* waited_seconds);
 int64_t tpm_cnn_param_count(int32_t c_in);
 int tpm_cnn_create(int32_t c_in, int32_t device, tpm_cnn** out);
 int tpm_cnn_destroy(tpm_cnn* c);

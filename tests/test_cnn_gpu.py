@@ -202,3 +202,21 @@ def test_near_field_sum_matches_direct_pairs():
         ref[k] = phys["g"] * np.sum((box.mass[m] * w / (r2 * r))[:, None] * d[m], 0)
     err = np.linalg.norm(sr[t] - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1e-30)
     assert np.sqrt(np.mean(err ** 2)) < 1e-4, float(np.sqrt(np.mean(err ** 2)))
+
+
+@pytest.mark.gpu
+def test_tensor_core_wait_times_out_and_reports():
+    """Failure detection without a fault: a conv tile whose MMAs are never
+    issued waits on an mbarrier nothing completes; the wait must give up at
+    its 2 s limit, flag the timeout and free its TMEM, and a normal tile must
+    then run on the same context (checked inside the self-test).  A network
+    forward afterwards still matches the oracle."""
+    import ctypes as C
+    from treepm import load
+    t = C.c_double(0.0)
+    assert load().tpm_selftest_bounded_wait(0, C.byref(t)) == 0
+    assert 1.9 < t.value < 10.0
+    net = _net(0)
+    x0, pb, ps, tg, w = _batch(7, n=10)
+    loss, grads = net.loss_grad(x0, pb, ps, tg, w)
+    assert np.isfinite(loss)
