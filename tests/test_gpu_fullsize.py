@@ -4,7 +4,7 @@ At these sizes the oracle builds the full insertion octree and PM mesh but
 walks a seeded subsample of targets: the device's accelerations at those
 targets must be within 1e-5 rms relative error, and the device's per-particle
 interaction counts must equal the oracle's exactly.  Size-independent checks
-cover every particle: finite forces, the mass deposit's total, and momentum.
+cover every particle: finite forces and the mass deposit's total.
 """
 import numpy as np
 import pytest
