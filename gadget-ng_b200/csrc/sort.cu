@@ -14,7 +14,7 @@ namespace tpm {
 namespace {
 
 constexpr int SORT_BLOCK = 256;
-constexpr int SORT_ITEMS = 16;
+constexpr int SORT_ITEMS = 8;  // 8 keys per thread: 2048-key tiles (sort 2.84 -> 2.30 ms at 256^3 against 16)
 constexpr int SORT_TILE = SORT_BLOCK * SORT_ITEMS;
 constexpr int SORT_WARPS = SORT_BLOCK / 32;
 
