@@ -575,6 +575,24 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
         a.rc2_lo_bits = lo_bits;
         a.band_bits = hi_bits - lo_bits;
       }
+      // The pair loop's band: near r_cut its FP32 distance carries a relative
+      // error below 2.4e-7 (1 + E / r_cut) + 2e-7, E = the widest group the
+      // walk accepts (1/16 of the box; coordinates are group-relative floats),
+      // since periodic leaves have no half side and monopoles h < 0.1 r_cut;
+      // 8 times that (at least 1e-5) leaves every pair the FP32 path could
+      // misjudge to the float64 test.  The aperiodic walk's leaves carry their
+      // cell's half side (cancellation against it): the node band of 1e-4.
+      {
+        const double e_over_rc = (box / 16.0) / h->r_cut;
+        const double pband = h->periodic ? std::max(1e-5, 8.0 * (2.4e-7 * (1.0 + e_over_rc) + 2e-7)) : 1e-4;
+        a.prc2_lo = (float)(rc2_u * (1.0 - pband));
+        a.prc2_hi = (float)(rc2_u * (1.0 + pband));
+        uint32_t lo_bits, hi_bits;
+        std::memcpy(&lo_bits, &a.prc2_lo, 4);
+        std::memcpy(&hi_bits, &a.prc2_hi, 4);
+        a.prc2_lo_bits = lo_bits;
+        a.pband_bits = hi_bits - lo_bits;
+      }
       a.grc2_lo = (float)(rc2_u * (1.0 - 4e-4));
       a.grc2_hi = (float)(rc2_u * (1.0 + 4e-4));
       a.eps2_u = (float)(eps2 / (u * u));
@@ -594,6 +612,9 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
         a.rc2_lo = a.rc2_hi = (float)rc2_u;
         std::memcpy(&a.rc2_lo_bits, &a.rc2_lo, 4);
         a.band_bits = 0u;
+        a.prc2_lo = a.prc2_hi = a.rc2_lo;
+        a.prc2_lo_bits = a.rc2_lo_bits;
+        a.pband_bits = 0u;
         a.tiny_u = -1.f;
       }
       a.ax = h->srx; a.ay = h->sry; a.az = h->srz;

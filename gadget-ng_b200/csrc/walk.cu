@@ -210,10 +210,10 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
       s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     }
     const bool in = (mask >> t) & 1u;
-    const bool ok = in && s <= a.rc2_lo;
+    const bool ok = in && s <= a.prc2_lo;
     if (!ACC) {  // accurate mode reproduces no float64 decisions
-      // s in (rc2_lo, rc2_hi]: positive floats order like their bit patterns
-      bool amb = in && (__float_as_uint(s) - a.rc2_lo_bits - 1u) < a.band_bits;
+      // s in (prc2_lo, prc2_hi]: positive floats order like their bit patterns
+      bool amb = in && (__float_as_uint(s) - a.prc2_lo_bits - 1u) < a.pband_bits;
       if (MONO) amb = amb || (in && r2b < a.tiny_u);
       amb_any = amb_any || amb;
     }
@@ -246,7 +246,7 @@ __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int
       s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     }
     const bool in = (mask >> t) & 1u;
-    bool amb = in && s > a.rc2_lo && s <= a.rc2_hi;
+    bool amb = in && s > a.prc2_lo && s <= a.prc2_hi;
     if (MONO) amb = amb || (in && r2b < a.tiny_u);
     if (!amb) continue;
     ++*nexact;
