@@ -568,13 +568,6 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       const double rc2_u = h->rc2 / (u * u);
       a.rc2_lo = (float)(rc2_u * (1.0 - 1e-4));
       a.rc2_hi = (float)(rc2_u * (1.0 + 1e-4));
-      {
-        uint32_t lo_bits, hi_bits;
-        std::memcpy(&lo_bits, &a.rc2_lo, 4);
-        std::memcpy(&hi_bits, &a.rc2_hi, 4);
-        a.rc2_lo_bits = lo_bits;
-        a.band_bits = hi_bits - lo_bits;
-      }
       // The pair loop's band: near r_cut its FP32 distance carries a relative
       // error below 2.4e-7 (1 + E / r_cut) + 2e-7, E = the widest group the
       // walk accepts (1/16 of the box; coordinates are group-relative floats),
@@ -610,10 +603,8 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       }
       if (a.accurate) {  // no reference decisions to reproduce: no float64 band, no COM-on-target opening
         a.rc2_lo = a.rc2_hi = (float)rc2_u;
-        std::memcpy(&a.rc2_lo_bits, &a.rc2_lo, 4);
-        a.band_bits = 0u;
         a.prc2_lo = a.prc2_hi = a.rc2_lo;
-        a.prc2_lo_bits = a.rc2_lo_bits;
+        std::memcpy(&a.prc2_lo_bits, &a.prc2_lo, 4);
         a.pband_bits = 0u;
         a.tiny_u = -1.f;
       }

@@ -35,9 +35,8 @@ struct WalkArgs {
   float box_u;    // box side in walk units (2^32 quanta)
   float h0_u;     // root half side in u
   float rc2_lo, rc2_hi;    // per-target ambiguity band around r_cut^2 (u^2): node refinement
-  uint32_t rc2_lo_bits, band_bits;  // the band as float bit patterns: (lo, lo + band]
   float prc2_lo, prc2_hi;  // the pair loop's (narrower) band: leaf pairs and monopoles
-  uint32_t prc2_lo_bits, pband_bits;
+  uint32_t prc2_lo_bits, pband_bits;  // the pair band as float bit patterns: (lo, lo + band]
   float grc2_lo, grc2_hi;  // group-level band
   float eps2_u;
   float pcx;      // 0.3275911 * scale*2^U / (sqrt(2) r_s)
