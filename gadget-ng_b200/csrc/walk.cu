@@ -743,7 +743,7 @@ static int env_choice(const char* name, int dflt, int a, int b, int c) {
   return (v == a || v == b || v == c) ? v : dflt;
 }
 static int walk_blocks_variant() {
-  static int v = env_choice("TPM_WALK_BLOCKS", 5, 4, 5, 6);
+  static int v = env_choice("TPM_WALK_BLOCKS", 6, 4, 5, 6);
   return v;
 }
 int walk_targets_per_warp() {
