@@ -234,24 +234,82 @@ __global__ void k_cells(const uint32_t* __restrict__ qx, const uint32_t* __restr
   out[o + 2] = c.iz[0];
 }
 
-// ---- x pass: real rows -> half spectrum ----------------------------------------
+// ---- x passes: a real row of nm samples as one complex row of h = nm/2 -------
+// (x[2j], x[2j+1]) is packed as z[j] = x[2j] + i x[2j+1] and transformed at
+// half length.  Forward: X[k] = E[k] + e^{-2 pi i k/nm} O[k] with
+// E = (Z[k] + conj Z[h-k]) / 2 and O = (Z[k] - conj Z[h-k]) / 2i, k = 0..h.
+// Inverse: Z[k] = X[k] (1 + i W_k) + conj(X[h-k]) (1 - i W_k), W_k =
+// e^{2 pi i k/nm}, k < h; the unnormalised inverse of Z gives x[2j] and
+// x[2j+1] as its real and imaginary parts (the row spectrum is Hermitian, so
+// X[0] and X[h] are real up to rounding).  Shared memory: the nm/2 twiddles of
+// length nm, the h/2 of length h, two work rows of h per row.
+__device__ __forceinline__ void load_x_twiddles(float2* s_tw, float2* s_th, const float2* tw, int nm) {
+  const int h = nm >> 1;
+  for (int i = threadIdx.x; i < h; i += blockDim.x) s_tw[i] = tw[i];
+  for (int i = threadIdx.x; i < (h >> 1); i += blockDim.x) s_th[i] = tw[2 * i];
+}
+
 __global__ void k_fft_x_r2c(const float* __restrict__ rho, float2* __restrict__ spec, int nm, int logn, int nh,
                             int rows, int64_t nrows, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
+  const int h = nm >> 1;
   float2* s_tw = sm;
-  float2* a = sm + (nm >> 1);
-  float2* b = a + rows * nm;
-  load_twiddles(s_tw, tw, nm);
+  float2* s_th = sm + h;
+  float2* a = s_th + (h >> 1 > 0 ? h >> 1 : 1);
+  float2* b = a + rows * h;
+  load_x_twiddles(s_tw, s_th, tw, nm);
   const int64_t row0 = (int64_t)blockIdx.x * rows;
-  for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
-    const int r = idx / nm, j = idx % nm;
-    a[idx] = make_float2(row0 + r < nrows ? rho[(row0 + r) * nm + j] : 0.f, 0.f);
+  const float2* src = reinterpret_cast<const float2*>(rho);
+  for (int idx = threadIdx.x; idx < rows * h; idx += blockDim.x) {
+    const int r = idx / h, j = idx % h;
+    a[idx] = row0 + r < nrows ? src[(row0 + r) * h + j] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  const float2* res = fft_smem<true>(a, b, nm, logn, rows, s_tw, false);
+  const float2* res = fft_smem<true>(a, b, h, logn - 1, rows, s_th, false);
   for (int idx = threadIdx.x; idx < rows * nh; idx += blockDim.x) {
     const int r = idx / nh, k = idx % nh;
-    if (row0 + r < nrows) spec[(row0 + r) * nh + k] = res[r * nm + k];
+    if (row0 + r >= nrows) continue;
+    const float2 zk = res[r * h + (k == h ? 0 : k)];
+    const float2 zm = res[r * h + (k == 0 || k == h ? 0 : h - k)];
+    const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));  // (Zk - conj Zm) / 2i
+    spec[(row0 + r) * nh + k] = cadd(e, cmul(twiddle(s_tw, k, nm, false), o));
+  }
+}
+
+__global__ void k_fft_x_c2r(const float2* __restrict__ spec3, float* __restrict__ force, int nm, int logn, int nh,
+                            int rows, int64_t nrows, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  const int h = nm >> 1;
+  float2* s_tw = sm;
+  float2* s_th = sm + h;
+  float2* a = s_th + (h >> 1 > 0 ? h >> 1 : 1);
+  float2* b = a + rows * h;
+  load_x_twiddles(s_tw, s_th, tw, nm);
+  __syncthreads();  // the unpacking below reads s_tw
+  const int comp = blockIdx.y;
+  const float2* in = spec3 + comp * nrows * nh;
+  float2* out = reinterpret_cast<float2*>(force + comp * nrows * nm);
+  const int64_t row0 = (int64_t)blockIdx.x * rows;
+  for (int idx = threadIdx.x; idx < rows * h; idx += blockDim.x) {
+    const int r = idx / h, k = idx % h;
+    float2 z = make_float2(0.f, 0.f);
+    if (row0 + r < nrows) {
+      float2 xk = in[(row0 + r) * nh + k];
+      float2 xm = in[(row0 + r) * nh + (h - k)];
+      if (k == 0) xk.y = xm.y = 0.f;  // the real part of the full inverse: Im X[0], Im X[h] drop out
+      const float2 w = twiddle(s_tw, k, nm, true);  // e^{+2 pi i k / nm}
+      // X[k] (1 + i W) + conj(X[h - k]) (1 - i W)
+      const float2 p = make_float2(1.f - w.y, w.x), q = make_float2(1.f + w.y, -w.x);
+      z = cadd(cmul(xk, p), cmul(make_float2(xm.x, -xm.y), q));
+    }
+    a[idx] = z;
+  }
+  __syncthreads();
+  const float2* res = fft_smem<true>(a, b, h, logn - 1, rows, s_th, true);
+  for (int idx = threadIdx.x; idx < rows * h; idx += blockDim.x) {
+    const int r = idx / h, j = idx % h;
+    if (row0 + r < nrows) out[(row0 + r) * h + j] = res[idx];
   }
 }
 
@@ -360,38 +418,6 @@ __global__ void k_fft_z_poisson(const float2* __restrict__ spec, float2* __restr
       spare = c3;
       c3 = t;
     }
-  }
-}
-
-// ---- inverse x pass: half spectrum rows -> real rows -------------------------------
-__global__ void k_fft_x_c2r(const float2* __restrict__ spec3, float* __restrict__ force, int nm, int logn, int nh,
-                            int rows, int64_t nrows, const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  float2* s_tw = sm;
-  float2* a = sm + (nm >> 1);
-  float2* b = a + rows * nm;
-  load_twiddles(s_tw, tw, nm);
-  const int comp = blockIdx.y;
-  const float2* in = spec3 + comp * nrows * nh;
-  float* out = force + comp * nrows * nm;
-  const int64_t row0 = (int64_t)blockIdx.x * rows;
-  for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
-    const int r = idx / nm, k = idx % nm;
-    float2 v = make_float2(0.f, 0.f);
-    if (row0 + r < nrows) {
-      if (k < nh) v = in[(row0 + r) * nh + k];
-      else {
-        v = in[(row0 + r) * nh + (nm - k)];
-        v.y = -v.y;
-      }
-    }
-    a[idx] = v;
-  }
-  __syncthreads();
-  const float2* res = fft_smem<true>(a, b, nm, logn, rows, s_tw, true);
-  for (int idx = threadIdx.x; idx < rows * nm; idx += blockDim.x) {
-    const int r = idx / nm, j = idx % nm;
-    if (row0 + r < nrows) out[(row0 + r) * nm + j] = res[idx].x;
   }
 }
 
@@ -595,7 +621,7 @@ __global__ void k_fft_z_pk(const float2* __restrict__ spec, int nm, int logn, in
 // resident blocks per SM better than 256 (PM 2.04 -> 1.67 ms at 256^3) or 1024.
 constexpr int FFT_THREADS = 512;
 
-// Rows (x pass) and columns (y, z passes) per block: 2048 elements per block
+// Full-length rows and columns (y, z passes) per block: 2048 elements per block
 // (8 x 8 at nm = 256: PM 1.67 -> 1.61 ms against 16 x 16; 32-wide tiles are
 // slower), at least 8 columns so a block still reads 64-byte runs.
 inline int rows_for(int nm) {
@@ -605,6 +631,21 @@ inline int rows_for(int nm) {
 inline int tx_for(int nm) {
   int t = 2048 / nm;
   return t < 8 ? 8 : (t > 16 ? 16 : t);
+}
+
+// The x passes: rows per block (the half-length rows of 2048 / nm complex
+// elements each make the same 2048-element tile), shared memory, blocks.
+struct XPass {
+  int rows;
+  size_t smem;
+  int blocks;
+};
+inline XPass x_pass(int nm, int64_t nrows) {
+  const int h = nm >> 1;
+  int rows = rows_for(nm) * 2;
+  if ((int64_t)rows > nrows) rows = (int)nrows;
+  const size_t smem = sizeof(float2) * ((size_t)h + (size_t)(h >> 1 > 0 ? h >> 1 : 1) + 2 * (size_t)rows * h);
+  return XPass{rows, smem, (int)((nrows + rows - 1) / rows)};
 }
 
 }  // namespace
@@ -689,14 +730,13 @@ void pm_deposit(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const u
 
 void pm_solve(const PmPlan& p, cudaStream_t s) {
   const int nm = p.nm, nh = p.nh, logn = p.logn;
-  const int rows = rows_for(nm), tx = tx_for(nm);
+  const int tx = tx_for(nm);
   const int64_t nrows = (int64_t)nm * nm;
-  const size_t sm_x = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)rows * nm);
+  const XPass xp = x_pass(nm, nrows);
   const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
   const size_t sm_z = sizeof(float2) * ((size_t)(nm / 2) + 3 * (size_t)nm * tx);
-  const int nblk_x = (int)((nrows + rows - 1) / rows);
   const int ntx = (nh + tx - 1) / tx;
-  k_fft_x_r2c<<<nblk_x, FFT_THREADS, sm_x, s>>>(p.rho, p.spec, nm, logn, nh, rows, nrows, p.twiddle);
+  k_fft_x_r2c<<<xp.blocks, FFT_THREADS, xp.smem, s>>>(p.rho, p.spec, nm, logn, nh, xp.rows, nrows, p.twiddle);
   TPM_LAUNCH_CHECK();
   k_fft_y<<<dim3(ntx, nm, 1), FFT_THREADS, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
   TPM_LAUNCH_CHECK();
@@ -705,7 +745,8 @@ void pm_solve(const PmPlan& p, cudaStream_t s) {
   TPM_LAUNCH_CHECK();
   k_fft_y<<<dim3(ntx, nm, p.ncomp), FFT_THREADS, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
   TPM_LAUNCH_CHECK();
-  k_fft_x_c2r<<<dim3(nblk_x, p.ncomp), FFT_THREADS, sm_x, s>>>(p.spec3, p.force, nm, logn, nh, rows, nrows, p.twiddle);
+  k_fft_x_c2r<<<dim3(xp.blocks, p.ncomp), FFT_THREADS, xp.smem, s>>>(p.spec3, p.force, nm, logn, nh, xp.rows, nrows,
+                                                                      p.twiddle);
   TPM_LAUNCH_CHECK();
 }
 
@@ -727,14 +768,13 @@ void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uin
 
 void pm_forward_real(const PmPlan& p, cudaStream_t s) {
   const int nm = p.nm, nh = p.nh, logn = p.logn;
-  const int rows = rows_for(nm), tx = tx_for(nm);
+  const int tx = tx_for(nm);
   const int64_t nrows = (int64_t)nm * nm;
-  const size_t sm_x = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)rows * nm);
+  const XPass xp = x_pass(nm, nrows);
   const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
   TPM_CUDA(cudaFuncSetAttribute(k_fft_z_c2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-  const int nblk_x = (int)((nrows + rows - 1) / rows);
   const int ntx = (nh + tx - 1) / tx;
-  k_fft_x_r2c<<<nblk_x, FFT_THREADS, sm_x, s>>>(p.rho, p.spec, nm, logn, nh, rows, nrows, p.twiddle);
+  k_fft_x_r2c<<<xp.blocks, FFT_THREADS, xp.smem, s>>>(p.rho, p.spec, nm, logn, nh, xp.rows, nrows, p.twiddle);
   TPM_LAUNCH_CHECK();
   k_fft_y<<<dim3(ntx, nm, 1), FFT_THREADS, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
   TPM_LAUNCH_CHECK();
@@ -744,18 +784,18 @@ void pm_forward_real(const PmPlan& p, cudaStream_t s) {
 
 void pm_inverse_components(const PmPlan& p, int ncomp, cudaStream_t s) {
   const int nm = p.nm, nh = p.nh, logn = p.logn;
-  const int rows = rows_for(nm), tx = tx_for(nm);
+  const int tx = tx_for(nm);
   const int64_t nrows = (int64_t)nm * nm;
-  const size_t sm_x = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)rows * nm);
+  const XPass xp = x_pass(nm, nrows);
   const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
   TPM_CUDA(cudaFuncSetAttribute(k_fft_z_c2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-  const int nblk_x = (int)((nrows + rows - 1) / rows);
   const int ntx = (nh + tx - 1) / tx;
   k_fft_z_c2c<<<dim3(ntx, nm, ncomp), FFT_THREADS, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
   TPM_LAUNCH_CHECK();
   k_fft_y<<<dim3(ntx, nm, ncomp), FFT_THREADS, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
   TPM_LAUNCH_CHECK();
-  k_fft_x_c2r<<<dim3(nblk_x, ncomp), FFT_THREADS, sm_x, s>>>(p.spec3, p.force, nm, logn, nh, rows, nrows, p.twiddle);
+  k_fft_x_c2r<<<dim3(xp.blocks, ncomp), FFT_THREADS, xp.smem, s>>>(p.spec3, p.force, nm, logn, nh, xp.rows, nrows,
+                                                                    p.twiddle);
   TPM_LAUNCH_CHECK();
 }
 
@@ -777,15 +817,14 @@ void pm_power_spectrum(const PmPlan& p, const double* pos, const uint32_t* qx, c
                                                                  p.rho);
     TPM_LAUNCH_CHECK();
   }
-  const int rows = rows_for(nm), tx = tx_for(nm);
+  const int tx = tx_for(nm);
   const int64_t nrows = (int64_t)nm * nm;
-  const size_t sm_x = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)rows * nm);
+  const XPass xp = x_pass(nm, nrows);
   const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
   const size_t sm_pk = sm_y + (sizeof(double) + sizeof(unsigned long long)) * (size_t)nb;
   TPM_CUDA(cudaFuncSetAttribute(k_fft_z_pk, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-  const int nblk_x = (int)((nrows + rows - 1) / rows);
   const int ntx = (nh + tx - 1) / tx;
-  k_fft_x_r2c<<<nblk_x, FFT_THREADS, sm_x, s>>>(p.rho, p.spec, nm, logn, nh, rows, nrows, p.twiddle);
+  k_fft_x_r2c<<<xp.blocks, FFT_THREADS, xp.smem, s>>>(p.rho, p.spec, nm, logn, nh, xp.rows, nrows, p.twiddle);
   TPM_LAUNCH_CHECK();
   k_fft_y<<<dim3(ntx, nm, 1), FFT_THREADS, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
   TPM_LAUNCH_CHECK();

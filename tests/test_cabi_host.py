@@ -108,6 +108,55 @@ def test_stockham_indexing_is_a_dft(n):
     assert np.max(np.abs(_stockham_mirror(x, True) - n * np.fft.ifft(x))) < 1e-12 * n
 
 
+def _packed_forward_mirror(x):
+    """pm.cu k_fft_x_r2c: the real row as h = n/2 complex samples, a length-h
+    transform, then the split into even and odd halves."""
+    n = len(x)
+    h = n // 2
+    z = _stockham_mirror(x[0::2] + 1j * x[1::2])
+    tw = np.exp(-2j * np.pi * np.arange(h) / n)
+    out = np.empty(h + 1, dtype=complex)
+    for k in range(h + 1):
+        zk, zm = z[k % h], z[(h - k) % h]
+        e = 0.5 * (zk + np.conj(zm))
+        o = (zk - np.conj(zm)) / 2j
+        w = tw[k] if k < h else -tw[0]
+        out[k] = e + w * o
+    return out
+
+
+def _packed_inverse_mirror(spec):
+    """pm.cu k_fft_x_c2r: the half spectrum (h + 1 values) to the real row of
+    the unnormalised inverse, through one length-h transform."""
+    h = len(spec) - 1
+    n = 2 * h
+    X = spec.astype(complex).copy()
+    X[0], X[h] = X[0].real, X[h].real
+    z = np.empty(h, dtype=complex)
+    for k in range(h):
+        w = np.exp(2j * np.pi * k / n)
+        z[k] = X[k] * (1 + 1j * w) + np.conj(X[h - k]) * (1 - 1j * w)
+    r = _stockham_mirror(z, inverse=True)
+    out = np.empty(n)
+    out[0::2], out[1::2] = r.real, r.imag
+    return out
+
+
+@pytest.mark.parametrize("n", [4, 8, 16, 64, 256])
+def test_packed_real_row_transforms(n):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n)
+    assert np.max(np.abs(_packed_forward_mirror(x) - np.fft.rfft(x))) < 1e-12 * n
+    spec = np.fft.rfft(rng.standard_normal(n))
+    assert np.max(np.abs(_packed_inverse_mirror(spec) - n * np.fft.irfft(spec, n))) < 1e-12 * n
+    # a row whose DC and Nyquist entries carry imaginary parts: the real part of
+    # the full inverse, as the full-length transform gave it
+    spec[0] += 0.7j
+    spec[-1] -= 0.3j
+    full = np.concatenate([spec, np.conj(spec[1:-1][::-1])])
+    assert np.max(np.abs(_packed_inverse_mirror(spec) - np.real(n * np.fft.ifft(full)))) < 1e-12 * n
+
+
 def test_half_spectrum_gradient_equals_real_part_of_full():
     """Zeroing the derivative's Nyquist plane reproduces Re(ifft(-i k phi)) of the
     reference's full complex transform (fft_poisson.rs:542-548, :466-473)."""
