@@ -164,10 +164,11 @@ __device__ __forceinline__ Cic cic_of(uint32_t qx, uint32_t qy, uint32_t qz, dou
 // reference's (float64 position arithmetic, product m wx wy wz).
 __global__ void k_deposit(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
                           const uint32_t* __restrict__ qz, const float* __restrict__ m, int64_t n, double scale,
-                          double inv_cell, int nm, float* __restrict__ rho) {
+                          double inv_cell, int nm, float* __restrict__ rho, const uint32_t* __restrict__ id,
+                          uint32_t id_limit) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  const bool live = i < n;
+  const bool live = i < n && (!id || id[i] < id_limit);  // halo copies deposit nothing
   Cic c{};
   float mi = 0.f;
   uint32_t key = 0xFFFFFFFFu;
@@ -719,12 +720,12 @@ void pm_plan_free(PmPlan& p) {
 }
 
 void pm_deposit(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const float* massf,
-                int64_t n, cudaStream_t s) {
+                int64_t n, cudaStream_t s, const uint32_t* id, uint32_t id_limit) {
   const int64_t nm3 = (int64_t)p.nm * p.nm * p.nm;
   TPM_CUDA(cudaMemsetAsync(p.rho, 0, sizeof(float) * nm3, s));
   if (n == 0) return;
   k_deposit<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, massf, n, p.box / TWO32, (double)p.nm / p.box,
-                                                        p.nm, p.rho);
+                                                        p.nm, p.rho, id, id_limit);
   TPM_LAUNCH_CHECK();
 }
 

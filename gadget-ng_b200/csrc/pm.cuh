@@ -47,8 +47,10 @@ struct GatherArgs {
   double kick;
 };
 
+// CIC deposit of particles [0, n) into p.rho (cleared first); with `id`,
+// only the particles whose id is below id_limit (the owned ones) deposit.
 void pm_deposit(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const float* massf,
-                int64_t n, cudaStream_t s);
+                int64_t n, cudaStream_t s, const uint32_t* id = nullptr, uint32_t id_limit = 0xFFFFFFFFu);
 void pm_solve(const PmPlan& p, cudaStream_t s);
 void pm_gather_kick(const PmPlan& p, const GatherArgs& a, cudaStream_t s);
 void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uint32_t* qz, const uint32_t* id,

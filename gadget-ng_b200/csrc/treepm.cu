@@ -4,7 +4,10 @@
 // device and one stream, with device-resident particle state.  A force
 // evaluation runs: bounding box -> octant-path keys -> radix sort -> particle
 // permutation -> radix tree -> octree -> bit-exact moments -> walk groups ->
-// short-range walk -> CIC deposit -> FFT Poisson -> gather (+ kick).
+// short-range walk -> CIC deposit -> FFT Poisson -> gather (+ kick).  A
+// domain-decomposed step runs the same stages in three calls around the
+// caller's density all-reduce, with halo copies of other ranks' particles
+// resident for one evaluation.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -14,6 +17,7 @@
 #include "../../include/treepm_b200.h"
 #include "cnn_api.h"
 #include "common.cuh"
+#include "domain.cuh"
 #include "learned.cuh"
 #include "pm.cuh"
 #include "scan.cuh"
@@ -110,10 +114,11 @@ __global__ void k_decode_state(Particles p, int64_t n, double scale, const float
   }
 }
 
+// out[id] = (x, y, z) * mul for the particles with id < limit (halo copies have none)
 __global__ void k_scatter_xyz(const uint32_t* __restrict__ id, int64_t n, const float* x, const float* y,
-                              const float* z, double mul, double* out) {
+                              const float* z, double mul, double* out, uint32_t limit = 0xFFFFFFFFu) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || id[i] >= limit) return;
   const int64_t o = 3 * (int64_t)id[i];
   out[o] = x[i] * mul;
   out[o + 1] = y[i] * mul;
@@ -209,6 +214,9 @@ struct tpm_handle {
   bool periodic = true, pm_only = false;
   std::string err;
   int64_t n = 0, cap = 0;
+  // particles with id < n_owned are this rank's; the rest (n - n_owned) are
+  // halo copies of other ranks' particles for one domain-decomposed evaluation
+  int64_t n_owned = 0;
   Particles P[2]{};
   int cur = 0;
   float *ax = nullptr, *ay = nullptr, *az = nullptr;
@@ -229,6 +237,7 @@ struct tpm_handle {
   double* staging = nullptr;  // float64 host-exchange buffer (n x 3 + n)
   size_t staging_elems = 0;
   bool forces_valid = false;
+  bool parts_valid = false;  // lr / sr parts and interaction counts match the particle order
   double g_acc = 0, eps2_acc = -1;
   int64_t n_int = 0, n_groups = 0;
   TreeParams params_host{};
@@ -265,6 +274,20 @@ struct tpm_handle {
   };
   std::vector<Alloc> allocs;
   bool tree_valid = false;
+  // domain decomposition scratch (sized by the particle capacity)
+  uint8_t* owned_mask = nullptr;
+  uint64_t* dom_flags = nullptr;
+  uint32_t* dom_a = nullptr;
+  uint32_t* dom_b = nullptr;
+  unsigned long long* dom_counts = nullptr;  // MAX_RANKS, persistent
+  // state carried between the stages of one force evaluation
+  struct Stage {
+    int phase = 0;  // 0 idle, 1 sorted + deposited, 2 short range done (domain-decomposed calls)
+    unsigned long long launches0 = 0;
+    bool use_net = false;
+    int64_t walk_groups = 0;
+    double eps2 = 0.0;
+  } fe;
 
   template <class T_>
   T_* alloc(size_t count, int group) {
@@ -371,6 +394,10 @@ void ensure_capacity(tpm_handle* h, int64_t n) {
     h->lgrp_first = h->alloc<uint32_t>(c + 1, 1);
     h->lgrp_size = h->alloc<uint32_t>(c + 1, 1);
   }
+  h->owned_mask = h->alloc<uint8_t>(c, 1);
+  h->dom_flags = h->alloc<uint64_t>(c, 1);
+  h->dom_a = h->alloc<uint32_t>(c, 1);
+  h->dom_b = h->alloc<uint32_t>(c, 1);
   h->staging_elems = (size_t)9 * c + 1;  // positions, velocities, accelerations (n x 3 float64 each), a scratch word
   h->staging = h->alloc<double>(h->staging_elems, 1);
   h->cap = n;
@@ -466,23 +493,22 @@ void near_of(tpm_handle* h, double eps2, const uint8_t* skip, float* nx, float* 
   near_field(f, h->stream);
 }
 
-// One force evaluation of all resident particles.  kick != 0 applies
-// v += a * kick in the gather.
-void force_eval(tpm_handle* h, double eps2, double g, double kick) {
+// The stages of one force evaluation of the resident particles.
+// fe_sort: events, keys and sort (tree solvers).
+void fe_sort(tpm_handle* h) {
   cudaStream_t s = h->stream;
   const int64_t n = h->n;
   if (n == 0) throw Error(TPM_ERR_NOT_READY, "no particles set");
   TreeBuffers& T = h->T;
   const double box = h->cfg.box_size;
-  const unsigned long long launches0 = g_kernel_launches;
+  h->fe.launches0 = g_kernel_launches;
   TPM_CUDA(cudaEventRecord(h->ev[0], s));
   TPM_CUDA(cudaMemsetAsync(h->stats_dev, 0, 8 * sizeof(unsigned long long), s));
   const bool need_tree = !h->pm_only;
-  const bool use_net = need_tree && h->learned && h->net_attached;
-  int64_t walk_groups = 0;
+  h->fe.use_net = need_tree && h->learned && h->net_attached;
+  h->fe.walk_groups = 0;
   h->tree_valid = false;
   if (need_tree) {
-    // ---- keys and sort
     launch_bbox_root(h->P[h->cur], n, box, T, s);
     launch_tree_keys(h->P[h->cur], n, box, T, s);
     TPM_CUDA(cudaEventRecord(h->ev[1], s));
@@ -491,6 +517,25 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
     launch_permute(h->P[h->cur], h->P[1 - h->cur], n, T.perm, s);
     h->cur = 1 - h->cur;
     TPM_CUDA(cudaEventRecord(h->ev[2], s));
+  } else {
+    TPM_CUDA(cudaEventRecord(h->ev[1], s));
+    TPM_CUDA(cudaEventRecord(h->ev[2], s));
+  }
+}
+
+// fe_tree_walk: octree, moments, walk groups and the short-range walk (the
+// learned path also runs its mesh stages here).  only: per sorted particle,
+// 1 = a walk target (null: all).
+void fe_tree_walk(tpm_handle* h, double eps2, const uint8_t* only) {
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  TreeBuffers& T = h->T;
+  const double box = h->cfg.box_size;
+  const bool need_tree = !h->pm_only;
+  const bool use_net = h->fe.use_net;
+  int64_t walk_groups = 0;
+  h->fe.eps2 = eps2;
+  if (need_tree) {
     // ---- tree
     h->n_int = 0;
     if (n >= 2) {
@@ -614,7 +659,7 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       a.stack = h->stack; a.stack_cap = STACK_CAP;
       a.single_target = h->r_cut > 0.2 * box ? 1 : 0;
       a.pcounts = h->pcounts;
-      a.only = use_net ? h->fallback : nullptr;
+      a.only = use_net ? h->fallback : only;
       {
         // a group spans at most L/16 (wider ones are walked target by target),
         // so for a node of cull half side hc the +-L images lie at least
@@ -647,15 +692,23 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
       learned_apply(P.qx, P.qy, P.qz, n, h->net, learned_mesh_of(h), h->fallback, h->srx, h->sry, h->srz, s);
     }
   } else {
-    TPM_CUDA(cudaEventRecord(h->ev[1], s));
-    TPM_CUDA(cudaEventRecord(h->ev[2], s));
     TPM_CUDA(cudaEventRecord(h->ev[3], s));
   }
   TPM_CUDA(cudaEventRecord(h->ev[4], s));
-  // ---- long range
+  h->fe.walk_groups = walk_groups;
+}
+
+// fe_long_range: CIC deposit (unless the caller deposited already), FFT
+// Poisson solve, gather fused with the short-range sum and the kick, stats.
+void fe_long_range(tpm_handle* h, double g, double kick, bool deposit) {
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  const bool use_net = h->fe.use_net;
+  const int64_t walk_groups = h->fe.walk_groups;
+  const double eps2 = h->fe.eps2;
   const Particles& P = h->P[h->cur];
   if (!use_net) {
-    pm_deposit(h->pm, P.qx, P.qy, P.qz, P.massf, n, s);
+    if (deposit) pm_deposit(h->pm, P.qx, P.qy, P.qz, P.massf, n, s);
     pm_solve(h->pm, s);
   }
   TPM_CUDA(cudaEventRecord(h->ev[5], s));
@@ -705,11 +758,83 @@ void force_eval(tpm_handle* h, double eps2, double g, double kick) {
   }
   h->stats.ms_gather_kick = ms_between(h->ev[5], h->ev[6]);
   h->stats.ms_total = ms_between(h->ev[0], h->ev[6]);
-  h->stats.kernel_launches = (int64_t)(g_kernel_launches - launches0);
+  h->stats.kernel_launches = (int64_t)(g_kernel_launches - h->fe.launches0);
   h->stats.force_evaluations += 1;
   h->forces_valid = true;
+  h->parts_valid = true;
   h->g_acc = g;
   h->eps2_acc = eps2;
+  h->fe.phase = 0;
+}
+
+// Drop the halo copies: the owned particles (id < n_owned) move, in their
+// current order and with their accelerations, to the front.  The force parts
+// and interaction counts of the last evaluation are not carried.
+void drop_halos(tpm_handle* h) {
+  if (h->n <= h->n_owned) return;
+  cudaStream_t s = h->stream;
+  const Particles& src = h->P[h->cur];
+  const Particles& dst = h->P[1 - h->cur];
+  compact_owned(src, dst, h->n, (uint32_t)h->n_owned, h->ax, h->ay, h->az, h->srx, h->sry, h->srz, h->dom_a,
+                h->dom_b, h->scan_scratch, s);
+  const size_t b = sizeof(float) * (size_t)h->n_owned;
+  TPM_CUDA(cudaMemcpyAsync(h->ax, h->srx, b, cudaMemcpyDeviceToDevice, s));
+  TPM_CUDA(cudaMemcpyAsync(h->ay, h->sry, b, cudaMemcpyDeviceToDevice, s));
+  TPM_CUDA(cudaMemcpyAsync(h->az, h->srz, b, cudaMemcpyDeviceToDevice, s));
+  h->cur = 1 - h->cur;
+  h->n = h->n_owned;
+  h->tree_valid = false;
+  h->parts_valid = false;
+  h->fe.phase = 0;
+}
+
+// Grow the particle capacity to at least `need` keeping the resident
+// particles [0, n) and their accelerations (through one temporary buffer).
+void grow_keeping_state(tpm_handle* h, int64_t need) {
+  if (need <= h->cap) return;
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  const Particles& P = h->P[h->cur];
+  const void* src[12] = {P.qx, P.qy, P.qz, P.vx, P.vy, P.vz, P.mass, P.massf, P.id, h->ax, h->ay, h->az};
+  const size_t esz[12] = {4, 4, 4, 4, 4, 4, 8, 4, 4, 4, 4, 4};
+  size_t total = 0;
+  for (int k = 0; k < 12; ++k) total += esz[k] * (size_t)n;
+  char* tmp = nullptr;
+  if (n > 0) {
+    TPM_CUDA(cudaMalloc(&tmp, total));
+    size_t off = 0;
+    for (int k = 0; k < 12; ++k) {
+      TPM_CUDA(cudaMemcpyAsync(tmp + off, src[k], esz[k] * n, cudaMemcpyDeviceToDevice, s));
+      off += esz[k] * (size_t)n;
+    }
+    TPM_CUDA(cudaStreamSynchronize(s));
+  }
+  try {
+    ensure_capacity(h, need + need / 4);
+  } catch (...) {
+    cudaFree(tmp);
+    throw;
+  }
+  h->cur = 0;
+  const Particles& Q = h->P[0];
+  void* dst[12] = {Q.qx, Q.qy, Q.qz, Q.vx, Q.vy, Q.vz, Q.mass, Q.massf, Q.id, h->ax, h->ay, h->az};
+  size_t off = 0;
+  for (int k = 0; k < 12 && n > 0; ++k) {
+    TPM_CUDA(cudaMemcpyAsync(dst[k], tmp + off, esz[k] * n, cudaMemcpyDeviceToDevice, s));
+    off += esz[k] * (size_t)n;
+  }
+  TPM_CUDA(cudaStreamSynchronize(s));
+  cudaFree(tmp);
+  h->tree_valid = false;
+}
+
+// One force evaluation of all resident particles (halo copies dropped
+// first).  kick != 0 applies v += a * kick in the gather.
+void force_eval(tpm_handle* h, double eps2, double g, double kick) {
+  drop_halos(h);
+  fe_sort(h);
+  fe_tree_walk(h, eps2, nullptr);
+  fe_long_range(h, g, kick, true);
 }
 
 void upload(tpm_handle* h, const double* pos, const double* vel, const double* mass, int64_t n) {
@@ -717,6 +842,7 @@ void upload(tpm_handle* h, const double* pos, const double* vel, const double* m
   if (n > 0 && (!pos || !mass)) throw Error(TPM_ERR_INVALID_ARGUMENT, "positions and masses are required");
   ensure_capacity(h, std::max<int64_t>(n, 1));
   h->n = n;
+  h->n_owned = n;
   h->cur = 0;
   h->forces_valid = false;
   h->m_total_valid = false;
@@ -792,6 +918,7 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
     h->T.err = h->alloc<uint32_t>(1, 0);
     h->stats_dev = h->alloc<unsigned long long>(8, 0);
     h->work = h->alloc<uint32_t>(1, 0);
+    h->dom_counts = h->alloc<unsigned long long>(MAX_RANKS + 8, 0);
     h->lgrp_count = h->alloc<uint32_t>(1, 0);
     if (h->learned) {
       const int64_t nm3 = (int64_t)nm * nm * nm;
@@ -848,6 +975,189 @@ int tpm_set_stream(tpm_handle* h, void* stream) {
 
 void* tpm_get_stream(const tpm_handle* h) { return h ? (void*)h->stream : nullptr; }
 
+// ---- domain-decomposed TreePM ----------------------------------------------
+static_assert(sizeof(tpm_halo_record) == sizeof(HaloRecord), "halo record layout");
+static_assert(sizeof(tpm_halo_record) == 24, "halo record size");
+
+int tpm_owned_aabb(tpm_handle* h, double aabb6[6]) {
+  if (!h || !aabb6) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
+    if (h->n_owned == 0) {  // Aabb3::empty
+      for (int d = 0; d < 3; ++d) {
+        aabb6[2 * d] = INFINITY;
+        aabb6[2 * d + 1] = -INFINITY;
+      }
+      return TPM_OK;
+    }
+    uint32_t b[6];
+    owned_bounds(h->P[h->cur], h->n_owned, reinterpret_cast<uint32_t*>(h->dom_counts), b, h->stream);
+    // decode is monotone, so the bounds of the decoded positions are the
+    // decoded bounds (compute_aabb_3d, halo3d.rs)
+    const double scale = h->cfg.box_size / TWO32;
+    for (int k = 0; k < 6; ++k) aabb6[k] = decode(b[k], scale);
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_halo_select(tpm_handle* h, const double* aabbs, int32_t n_ranks, int32_t rank, double width,
+                    int64_t* counts, tpm_halo_record* send, int64_t cap) {
+  if (!h || !aabbs || !counts || n_ranks < 1 || n_ranks > MAX_RANKS || rank < 0 || rank >= n_ranks ||
+      !(width >= 0.0) || cap < 0)
+    return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
+    cudaStream_t s = h->stream;
+    AabbTable t{};
+    std::memcpy(t.v, aabbs, sizeof(double) * 6 * (size_t)n_ranks);
+    const int64_t n = h->n_owned;
+    const Particles& P = h->P[h->cur];
+    halo_flags(P, n, h->cfg.box_size / TWO32, h->cfg.box_size, t, n_ranks, rank, width * width, h->dom_flags,
+               h->dom_counts, s);
+    unsigned long long c[MAX_RANKS];
+    TPM_CUDA(cudaMemcpyAsync(c, h->dom_counts, sizeof(c), cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaStreamSynchronize(s));
+    int64_t total = 0;
+    for (int r = 0; r < n_ranks; ++r) {
+      counts[r] = (int64_t)c[r];
+      total += (int64_t)c[r];
+    }
+    if (!send) return TPM_OK;
+    if (total > cap) throw Error(TPM_ERR_INVALID_ARGUMENT, "halo send buffer holds " + std::to_string(cap) +
+                                                               " records, " + std::to_string(total) + " selected");
+    int64_t off = 0;
+    for (int r = 0; r < n_ranks; ++r) {
+      if (c[r] == 0) continue;
+      halo_pack(P, n, h->dom_flags, r, h->dom_a, h->dom_b, h->scan_scratch,
+                reinterpret_cast<HaloRecord*>(send) + off, s);
+      off += (int64_t)c[r];
+    }
+    TPM_CUDA(cudaStreamSynchronize(s));
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_set_halos(tpm_handle* h, const tpm_halo_record* recv, int64_t n) {
+  if (!h || n < 0 || (n > 0 && !recv)) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
+    if (h->n_owned + n >= ((int64_t)1 << 31)) throw Error(TPM_ERR_INVALID_ARGUMENT, "particle count out of range");
+    grow_keeping_state(h, std::max<int64_t>(h->n_owned + n, 1));
+    append_halos(h->P[h->cur], h->n_owned, reinterpret_cast<const HaloRecord*>(recv), n, h->stream);
+    h->n = h->n_owned + n;
+    h->tree_valid = false;
+    h->parts_valid = false;
+    h->m_total_valid = false;
+    TPM_CUDA(cudaStreamSynchronize(h->stream));  // the receive buffer is free on return
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_force_begin(tpm_handle* h) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (h->learned) throw Error(TPM_ERR_INVALID_ARGUMENT, "the learned short range runs on one domain only");
+    h->fe.phase = 0;
+    if (h->n == 0) {  // an empty rank still contributes its (empty) density to the sum
+      h->fe.launches0 = g_kernel_launches;
+      h->fe.use_net = false;
+      TPM_CUDA(cudaMemsetAsync(h->pm.rho, 0, sizeof(float) * (size_t)h->pm.nm * h->pm.nm * h->pm.nm, h->stream));
+    } else {
+      fe_sort(h);
+      const Particles& P = h->P[h->cur];
+      pm_deposit(h->pm, P.qx, P.qy, P.qz, P.massf, h->n, h->stream, P.id, (uint32_t)h->n_owned);
+    }
+    h->fe.phase = 1;
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_mesh_density(tpm_handle* h, float** density, int64_t* cells) {
+  if (!h || !density || !cells) return TPM_ERR_INVALID_ARGUMENT;
+  *density = h->pm.rho;
+  *cells = (int64_t)h->pm.nm * h->pm.nm * h->pm.nm;
+  return TPM_OK;
+}
+
+int tpm_force_short_range(tpm_handle* h, double eps2) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (h->fe.phase != 1) throw Error(TPM_ERR_NOT_READY, "tpm_force_begin first");
+    if (h->n > 0) {
+      const uint8_t* only = nullptr;
+      if (h->n_owned < h->n) {
+        owned_mask(h->P[h->cur].id, h->n, (uint32_t)h->n_owned, h->owned_mask, h->stream);
+        only = h->owned_mask;
+      }
+      fe_tree_walk(h, eps2, only);
+    } else {
+      h->fe.eps2 = eps2;
+    }
+    h->fe.phase = 2;
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_force_end(tpm_handle* h, double g, double kick) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (h->fe.phase != 2) throw Error(TPM_ERR_NOT_READY, "tpm_force_short_range first");
+    if (h->n > 0) {
+      fe_long_range(h, g, kick, false);
+    } else {
+      h->fe.phase = 0;
+      h->forces_valid = true;
+      h->parts_valid = true;
+      h->g_acc = g;
+      h->eps2_acc = h->fe.eps2;
+    }
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_kick_drift(tpm_handle* h, double kick_half, double drift, double g) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
+    if (h->n == 0) return TPM_OK;
+    if (!h->forces_valid || h->g_acc == 0.0) throw Error(TPM_ERR_NOT_READY, "no forces computed");
+    const double k1 = kick_half * (g / h->g_acc);
+    const Particles& P = h->P[h->cur];
+    k_kick_drift<<<grid_for(h->n, 256, 1ll << 30), 256, 0, h->stream>>>(P, h->n, h->ax, h->ay, h->az, (float)k1,
+                                                                        drift * TWO32 / h->cfg.box_size);
+    TPM_LAUNCH_CHECK();
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_particle_counts(const tpm_handle* h, int64_t* n_owned, int64_t* n_resident) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  if (n_owned) *n_owned = h->n_owned;
+  if (n_resident) *n_resident = h->n;
+  return TPM_OK;
+}
+
 int tpm_accelerations_for_indices(tpm_handle* h, const double* pos, const double* mass, int64_t n, double eps2,
                                   double g, const uint64_t* idx, int64_t n_idx, double* out) {
   if (!h) return TPM_ERR_INVALID_ARGUMENT;
@@ -897,6 +1207,7 @@ int tpm_set_particles_fixed(tpm_handle* h, const uint32_t* q, const float* vel, 
     if (n <= 0 || !q || !mass) throw Error(TPM_ERR_INVALID_ARGUMENT, "positions and masses are required");
     ensure_capacity(h, n);
     h->n = n;
+    h->n_owned = n;
     h->cur = 0;
     h->forces_valid = false;
     h->m_total_valid = false;
@@ -944,6 +1255,7 @@ int tpm_kdk_step(tpm_handle* h, double kick_half, double drift, double kick_half
   if (!h) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
     if (h->n == 0) throw Error(TPM_ERR_NOT_READY, "no particles set");
     if (!h->forces_valid || h->eps2_acc != eps2 || h->g_acc == 0.0) force_eval(h, eps2, g, 0.0);
     // opening half kick with the cached acceleration, rescaled to this step's coupling
@@ -964,7 +1276,9 @@ int tpm_get_state(tpm_handle* h, double* pos, double* vel, double* acc) {
   if (!h) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
-    const int64_t n = h->n;
+    // owned particles only (ids below n_owned), read in place: halo copies
+    // land past the owned block of each staging area and are not copied
+    const int64_t n = h->n, no = h->n_owned;
     if (n == 0) return TPM_OK;
     if (acc && !h->forces_valid) throw Error(TPM_ERR_NOT_READY, "no forces computed");
     cudaStream_t s = h->stream;
@@ -975,14 +1289,15 @@ int tpm_get_state(tpm_handle* h, double* pos, double* vel, double* acc) {
                                                                nullptr, nullptr, pos ? dp : nullptr,
                                                                vel ? dv : nullptr, nullptr);
     TPM_LAUNCH_CHECK();
-    if (pos) TPM_CUDA(cudaMemcpyAsync(pos, dp, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
-    if (vel) TPM_CUDA(cudaMemcpyAsync(vel, dv, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+    if (pos) TPM_CUDA(cudaMemcpyAsync(pos, dp, sizeof(double) * 3 * no, cudaMemcpyDeviceToHost, s));
+    if (vel) TPM_CUDA(cudaMemcpyAsync(vel, dv, sizeof(double) * 3 * no, cudaMemcpyDeviceToHost, s));
     TPM_CUDA(cudaStreamSynchronize(s));
     if (acc) {
       double* buf = da;
-      k_scatter_xyz<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, h->ax, h->ay, h->az, 1.0, buf);
+      k_scatter_xyz<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, h->ax, h->ay, h->az, 1.0, buf,
+                                                                (uint32_t)no);
       TPM_LAUNCH_CHECK();
-      TPM_CUDA(cudaMemcpyAsync(acc, buf, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaMemcpyAsync(acc, buf, sizeof(double) * 3 * no, cudaMemcpyDeviceToHost, s));
       TPM_CUDA(cudaStreamSynchronize(s));
     }
   } catch (const Error& e) {
@@ -1041,6 +1356,7 @@ int tpm_set_particles_zeldovich(tpm_handle* h, const tpm_zeldovich* cfg) {
     if (n >= ((int64_t)1 << 31)) throw Error(TPM_ERR_INVALID_ARGUMENT, "too many particles");
     ensure_capacity(h, n);
     h->n = n;
+    h->n_owned = n;
     h->cur = 0;
     h->forces_valid = false;
     h->m_total_valid = false;
@@ -1056,6 +1372,7 @@ int tpm_write_snapshot(tpm_handle* h, const char* out_dir, int32_t format, const
   if (!h || !out_dir || !env || !prov) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
     snapshot_write(out_dir, format, env, prov, DeviceState{h->P[h->cur], h->n, h->cfg.box_size, h->staging, h->stream});
   } catch (const Error& e) {
     return fail(h, e);
@@ -1090,6 +1407,7 @@ int tpm_write_checkpoint(tpm_handle* h, const char* out_dir, uint64_t completed_
   if (!h || !out_dir || !config_hash) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
     const std::string ck = std::string(out_dir) + "/checkpoint";
     tpm_snapshot_env env{};
     env.box_size = 1.0;
@@ -1179,6 +1497,7 @@ int tpm_get_power_spectrum(tpm_handle* h, double* k, double* pk, uint64_t* n_mod
   if (!h || !k || !pk || !n_modes) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
     if (h->n == 0) throw Error(TPM_ERR_NOT_READY, "no particles set");
     const int nb = h->pm.nm / 2;
     if (!h->pk_sum) {
@@ -1301,24 +1620,25 @@ int tpm_get_force_parts(tpm_handle* h, double* acc_lr, double* acc_sr) {
   if (!h) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
-    if (!h->forces_valid) throw Error(TPM_ERR_NOT_READY, "no forces computed");
-    const int64_t n = h->n;
+    if (!h->forces_valid || !h->parts_valid) throw Error(TPM_ERR_NOT_READY, "no forces computed");
+    const int64_t n = h->n, no = h->n_owned;  // owned particles only
+    const uint32_t lim = (uint32_t)no;
     cudaStream_t s = h->stream;
     if (acc_lr) {
       k_scatter_xyz<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, h->lrx, h->lry, h->lrz, 1.0,
-                                                                h->staging);
+                                                                h->staging, lim);
       TPM_LAUNCH_CHECK();
-      TPM_CUDA(cudaMemcpyAsync(acc_lr, h->staging, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+      TPM_CUDA(cudaMemcpyAsync(acc_lr, h->staging, sizeof(double) * 3 * no, cudaMemcpyDeviceToHost, s));
       TPM_CUDA(cudaStreamSynchronize(s));
     }
     if (acc_sr) {
       if (h->pm_only) {
-        std::memset(acc_sr, 0, sizeof(double) * 3 * n);
+        std::memset(acc_sr, 0, sizeof(double) * 3 * no);
       } else {
         k_scatter_xyz<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, h->srx, h->sry, h->srz,
-                                                                  h->g_acc, h->staging);
+                                                                  h->g_acc, h->staging, lim);
         TPM_LAUNCH_CHECK();
-        TPM_CUDA(cudaMemcpyAsync(acc_sr, h->staging, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+        TPM_CUDA(cudaMemcpyAsync(acc_sr, h->staging, sizeof(double) * 3 * no, cudaMemcpyDeviceToHost, s));
         TPM_CUDA(cudaStreamSynchronize(s));
       }
     }
@@ -1332,13 +1652,15 @@ int tpm_get_interaction_counts(tpm_handle* h, int64_t* counts) {
   if (!h || !counts) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
-    if (!h->forces_valid || h->pm_only || h->n < 2) throw Error(TPM_ERR_NOT_READY, "no short-range walk computed");
+    if (!h->forces_valid || !h->parts_valid || h->pm_only || h->n < 2)
+      throw Error(TPM_ERR_NOT_READY, "no short-range walk computed");
     const int64_t n = h->n;
     std::vector<uint32_t> c((size_t)2 * n), id((size_t)n);
     TPM_CUDA(cudaMemcpyAsync(c.data(), h->pcounts, sizeof(uint32_t) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
     TPM_CUDA(cudaMemcpyAsync(id.data(), h->P[h->cur].id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, h->stream));
     TPM_CUDA(cudaStreamSynchronize(h->stream));
     for (int64_t i = 0; i < n; ++i) {
+      if ((int64_t)id[i] >= h->n_owned) continue;  // halo copies
       counts[2 * (int64_t)id[i]] = c[2 * i];
       counts[2 * (int64_t)id[i] + 1] = c[2 * i + 1];
     }
@@ -1381,6 +1703,7 @@ int tpm_hilbert_keys(tpm_handle* h, uint64_t* keys, int64_t* order) {
   if (!h || !keys) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
     const int64_t n = h->n;
     if (n == 0) return TPM_OK;
     cudaStream_t s = h->stream;
@@ -1407,10 +1730,42 @@ int tpm_hilbert_keys(tpm_handle* h, uint64_t* keys, int64_t* order) {
   return TPM_OK;
 }
 
+int tpm_sfc_keys(tpm_handle* h, const double bbox6[6], uint64_t* keys) {
+  if (!h || !bbox6 || !keys) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
+    const int64_t n = h->n;
+    if (n == 0) return TPM_OK;
+    cudaStream_t s = h->stream;
+    // particle_hilbert's normalisation (sfc.rs:187-204): origin lo, extent
+    // max(hi - lo, f64::EPSILON) per axis
+    TreeParams prm{};
+    for (int d = 0; d < 3; ++d) {
+      prm.hlo[d] = bbox6[2 * d];
+      prm.hlen[d] = std::max(bbox6[2 * d + 1] - bbox6[2 * d], 2.220446049250313e-16);
+    }
+    TPM_CUDA(cudaMemcpyAsync(h->T.params, &prm, sizeof(prm), cudaMemcpyHostToDevice, s));
+    uint64_t* k_store = h->T.key_lo_tmp;
+    uint64_t* k_by_id = h->T.key_hi;
+    uint32_t* vals = h->T.perm;
+    launch_hilbert_keys(h->P[h->cur], n, h->cfg.box_size, h->T.params, k_store, vals, s);
+    k_scatter_u64<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, k_store, k_by_id, vals);
+    TPM_LAUNCH_CHECK();
+    TPM_CUDA(cudaMemcpyAsync(keys, k_by_id, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaStreamSynchronize(s));
+    h->tree_valid = false;
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
 int tpm_cic_cells(tpm_handle* h, int32_t* cells) {
   if (!h || !cells) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
     const int64_t n = h->n;
     if (n == 0) return TPM_OK;
     int32_t* d = (int32_t*)h->staging;

@@ -198,7 +198,19 @@ SIGNATURES = {
     "tpm_write_checkpoint": ([_P, C.c_char_p, C.c_uint64, _D, C.c_char_p], _I),
     "tpm_read_checkpoint": ([_P, C.c_char_p, _P, _P, C.c_char_p, _I64], _I),
     "tpm_zeldovich_sigma": ([_P, _P, _I64, _P, _P], _I),
+    "tpm_owned_aabb": ([_P, _P], _I),
+    "tpm_halo_select": ([_P, _P, C.c_int32, C.c_int32, _D, _P, _P, _I64], _I),
+    "tpm_set_halos": ([_P, _P, _I64], _I),
+    "tpm_force_begin": ([_P], _I),
+    "tpm_mesh_density": ([_P, C.POINTER(_P), C.POINTER(_I64)], _I),
+    "tpm_force_short_range": ([_P, _D], _I),
+    "tpm_force_end": ([_P, _D, _D], _I),
+    "tpm_kick_drift": ([_P, _D, _D, _D], _I),
+    "tpm_particle_counts": ([_P, C.POINTER(_I64), C.POINTER(_I64)], _I),
+    "tpm_sfc_keys": ([_P, _P, _P], _I),
 }
+HALO_RECORD_BYTES = 24  # tpm_halo_record
+MAX_RANKS = 64
 NOALLOC_MAX_PARTICLES = 1 << 18
 
 _lib = None

@@ -180,6 +180,70 @@ int tpm_get_interaction_counts(tpm_handle* h, int64_t* counts);
 int tpm_set_stream(tpm_handle* h, void* cuda_stream);
 void* tpm_get_stream(const tpm_handle* h);
 
+/* ---- domain-decomposed TreePM (one handle per rank) -----------------------
+ * The reference's distributed TreePM with SFC domains: each rank owns its
+ * particles; for one force evaluation it also holds halo copies of the other
+ * ranks' particles within r_cut of its particle AABB
+ * (ParallelRuntime::exchange_halos_3d_periodic,
+ * crates/gadget-ng-parallel/src/lib.rs:168 and src/mpi_rt.rs:723-781); the
+ * short range walks a tree of owned + halo particles for the owned targets
+ * (short_range_accels_sfc, crates/gadget-ng-treepm/src/distributed.rs:119-145)
+ * and the long range solves the all-ranks density (the density all-reduce of
+ * ParallelRuntime::allreduce_sum_f64_slice, lib.rs:200-210).  The caller
+ * performs the three exchanges (AABB allgather, halo alltoallv, density
+ * all-reduce); the handle does the device work around them.  Results and
+ * state accessors report owned particles only (n_owned of them, original
+ * order); any other force call drops the halo copies first. */
+
+/* One halo particle on the wire: 32-bit fixed-point position (x = q L / 2^32),
+ * the owner's particle index, mass (24 bytes). */
+typedef struct tpm_halo_record {
+  uint32_t q[3];
+  uint32_t id;
+  double mass;
+} tpm_halo_record;
+
+/* AABB of the owned particles as the reference packs it (aabb_to_f64,
+ * crates/gadget-ng-parallel/src/halo3d.rs): {xlo, xhi, ylo, yhi, zlo, zhi};
+ * an empty rank gives lo = +inf, hi = -inf (an invalid box). */
+int tpm_owned_aabb(tpm_handle* h, double aabb6[6]);
+/* Halo selection for every rank r != rank: the owned particles whose periodic
+ * distance to rank r's AABB (aabbs + 6 r; invalid boxes skipped) is below
+ * `width` (min_dist2_to_aabb_3d_periodic < width^2, halo3d.rs:237-260).
+ * counts[r] (host, n_ranks) receives the number per rank; when `send` (device,
+ * cap records) is non-NULL the records follow grouped by destination rank in
+ * rank order, each group in the handle's particle order.  A particle can go to
+ * several ranks.  n_ranks <= 64.  A total above cap returns
+ * TPM_ERR_INVALID_ARGUMENT with counts filled and nothing written. */
+int tpm_halo_select(tpm_handle* h, const double* aabbs, int32_t n_ranks, int32_t rank, double width,
+                    int64_t* counts, tpm_halo_record* send, int64_t cap);
+/* Replace the halo copies by n records (device memory, e.g. the halo
+ * alltoallv's receive buffer); owned particles are kept. */
+int tpm_set_halos(tpm_handle* h, const tpm_halo_record* recv, int64_t n);
+/* The three stages of a domain-decomposed force evaluation, on the handle's
+ * stream.  tpm_force_begin: keys, sort, and the CIC deposit of the OWNED
+ * particles into the density mesh, whose device address and cell count
+ * tpm_mesh_density returns (float32, [z][y][x]); the caller then sums that mesh
+ * over all ranks in place (after the stream reaches this point) and may
+ * overlap the sum with tpm_force_short_range (tree over owned + halo
+ * particles, walk for the owned).  tpm_force_end (the summed density in place
+ * before the handle's stream reaches it): FFT Poisson solve, gather of long +
+ * short range and, kick != 0, v += a kick for the owned particles. */
+int tpm_force_begin(tpm_handle* h);
+int tpm_mesh_density(tpm_handle* h, float** density, int64_t* cells);
+int tpm_force_short_range(tpm_handle* h, double eps2);
+int tpm_force_end(tpm_handle* h, double g, double kick);
+/* The opening half of a domain-decomposed KDK step: halo copies dropped,
+ * then v += a kick_half (the cached acceleration rescaled by g / g_prev) and
+ * the drift with the periodic wrap, for the owned particles. */
+int tpm_kick_drift(tpm_handle* h, double kick_half, double drift, double g);
+/* particle_hilbert keys (crates/gadget-ng-parallel/src/sfc.rs:187-204) of the
+ * owned particles over a given box {xlo, xhi, ylo, yhi, zlo, zhi} (all ranks'
+ * bounding box for SfcDecomposition, sfc.rs:336-393), original order. */
+int tpm_sfc_keys(tpm_handle* h, const double bbox6[6], uint64_t* keys);
+/* Owned and resident (owned + halo) particle counts. */
+int tpm_particle_counts(const tpm_handle* h, int64_t* n_owned, int64_t* n_resident);
+
 /* ---- cosmology (FP64 host) ------------------------------------------------
  * CosmologyParams::drift_kick_factors (crates/gadget-ng-core/src/cosmology.rs:188-233)
  * for LambdaCDM: out3 = {drift, kick_half, kick_half2}. */
