@@ -607,6 +607,33 @@ __global__ void k_hilbert(const uint32_t* __restrict__ qx, const uint32_t* __res
   vals[i] = id ? id[i] : (uint32_t)i;
 }
 
+// spread_bits (crates/gadget-ng-parallel/src/sfc.rs:39-47): the 21 low bits of
+// x to every third bit position.
+__device__ __forceinline__ uint64_t spread3(uint64_t x) {
+  x &= 0x1FFFFFull;
+  x = (x | (x << 32)) & 0x1F00000000FFFFull;
+  x = (x | (x << 16)) & 0x1F0000FF0000FFull;
+  x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+  x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+  x = (x | (x << 2)) & 0x1249249249249249ull;
+  return x;
+}
+
+// particle_morton (sfc.rs:54-81): the coordinates normalised and quantised as
+// for the Hilbert keys, interleaved x | y << 1 | z << 2.
+__global__ void k_morton(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                         const uint32_t* __restrict__ qz, const uint32_t* __restrict__ id, int64_t n, double scale,
+                         const TreeParams* __restrict__ prm, uint64_t* __restrict__ keys,
+                         uint32_t* __restrict__ vals) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t ix = hilbert_coord(decode(qx[i], scale), prm->hlo[0], prm->hlen[0]);
+  const uint32_t iy = hilbert_coord(decode(qy[i], scale), prm->hlo[1], prm->hlen[1]);
+  const uint32_t iz = hilbert_coord(decode(qz[i], scale), prm->hlo[2], prm->hlen[2]);
+  keys[i] = spread3(ix) | (spread3(iy) << 1) | (spread3(iz) << 2);
+  vals[i] = id ? id[i] : (uint32_t)i;
+}
+
 __device__ __forceinline__ void mask_path(uint64_t hi, uint64_t lo, int depth, uint64_t* oh, uint64_t* ol) {
   if (depth <= 0) { *oh = 0; *ol = 0; return; }
   if (depth <= 21) {
@@ -754,6 +781,12 @@ void launch_groups(int64_t n, int64_t n_int, int group_max, TreeBuffers& t, void
 void launch_hilbert_keys(const Particles& p, int64_t n, double box, const TreeParams* prm, uint64_t* keys,
                          uint32_t* vals, cudaStream_t s) {
   k_hilbert<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(p.qx, p.qy, p.qz, p.id, n, box / TWO32, prm, keys, vals);
+  TPM_LAUNCH_CHECK();
+}
+
+void launch_morton_keys(const Particles& p, int64_t n, double box, const TreeParams* prm, uint64_t* keys,
+                        uint32_t* vals, cudaStream_t s) {
+  k_morton<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(p.qx, p.qy, p.qz, p.id, n, box / TWO32, prm, keys, vals);
   TPM_LAUNCH_CHECK();
 }
 

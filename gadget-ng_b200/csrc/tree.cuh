@@ -112,6 +112,10 @@ void launch_walk_records(const Particles& p, int64_t n, int64_t n_int, double th
 void launch_groups(int64_t n, int64_t n_int, int group_max, TreeBuffers& t, void* scan_scratch, cudaStream_t s);
 void launch_hilbert_keys(const Particles& p, int64_t n, double box, const TreeParams* prm, uint64_t* keys,
                          uint32_t* vals, cudaStream_t s);
+// Morton keys (particle_morton, sfc.rs:54-81) with the normalisation of prm's
+// hlo / hlen, like launch_hilbert_keys.
+void launch_morton_keys(const Particles& p, int64_t n, double box, const TreeParams* prm, uint64_t* keys,
+                        uint32_t* vals, cudaStream_t s);
 void launch_export_paths(int64_t n, int64_t n_int, const TreeBuffers& t, uint64_t* node_hi, uint64_t* node_lo,
                          uint64_t* leaf_hi, uint64_t* leaf_lo, cudaStream_t s);
 

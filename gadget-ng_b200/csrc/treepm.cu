@@ -1730,16 +1730,16 @@ int tpm_hilbert_keys(tpm_handle* h, uint64_t* keys, int64_t* order) {
   return TPM_OK;
 }
 
-int tpm_sfc_keys(tpm_handle* h, const double bbox6[6], uint64_t* keys) {
-  if (!h || !bbox6 || !keys) return TPM_ERR_INVALID_ARGUMENT;
+int tpm_sfc_keys(tpm_handle* h, const double bbox6[6], int32_t kind, uint64_t* keys) {
+  if (!h || !bbox6 || !keys || (kind != TPM_SFC_HILBERT && kind != TPM_SFC_MORTON)) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
     drop_halos(h);
     const int64_t n = h->n;
     if (n == 0) return TPM_OK;
     cudaStream_t s = h->stream;
-    // particle_hilbert's normalisation (sfc.rs:187-204): origin lo, extent
-    // max(hi - lo, f64::EPSILON) per axis
+    // the normalisation of particle_hilbert / particle_morton (sfc.rs:64-81,
+    // :187-204): origin lo, extent max(hi - lo, f64::EPSILON) per axis
     TreeParams prm{};
     for (int d = 0; d < 3; ++d) {
       prm.hlo[d] = bbox6[2 * d];
@@ -1749,7 +1749,10 @@ int tpm_sfc_keys(tpm_handle* h, const double bbox6[6], uint64_t* keys) {
     uint64_t* k_store = h->T.key_lo_tmp;
     uint64_t* k_by_id = h->T.key_hi;
     uint32_t* vals = h->T.perm;
-    launch_hilbert_keys(h->P[h->cur], n, h->cfg.box_size, h->T.params, k_store, vals, s);
+    if (kind == TPM_SFC_HILBERT)
+      launch_hilbert_keys(h->P[h->cur], n, h->cfg.box_size, h->T.params, k_store, vals, s);
+    else
+      launch_morton_keys(h->P[h->cur], n, h->cfg.box_size, h->T.params, k_store, vals, s);
     k_scatter_u64<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(h->P[h->cur].id, n, k_store, k_by_id, vals);
     TPM_LAUNCH_CHECK();
     TPM_CUDA(cudaMemcpyAsync(keys, k_by_id, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, s));

@@ -207,9 +207,10 @@ SIGNATURES = {
     "tpm_force_end": ([_P, _D, _D], _I),
     "tpm_kick_drift": ([_P, _D, _D, _D], _I),
     "tpm_particle_counts": ([_P, C.POINTER(_I64), C.POINTER(_I64)], _I),
-    "tpm_sfc_keys": ([_P, _P, _P], _I),
+    "tpm_sfc_keys": ([_P, _P, C.c_int32, _P], _I),
 }
 HALO_RECORD_BYTES = 24  # tpm_halo_record
+SFC_KINDS = {"hilbert": 0, "morton": 1}
 MAX_RANKS = 64
 NOALLOC_MAX_PARTICLES = 1 << 18
 

@@ -284,21 +284,25 @@ class DomainTreePm:
         self._force(eps2, g, kick_half2)
 
     # ---- SFC domains -----------------------------------------------------------
-    def sfc_keys(self, bbox6) -> np.ndarray:
+    def sfc_keys(self, bbox6, kind: str = "morton") -> np.ndarray:
+        """SfcKind keys of the owned particles over bbox6 (owned order)."""
         keys = np.empty(self.n_owned, dtype=np.uint64)
         check(self._h.h, self._L.tpm_sfc_keys(self._h.h, _ptr(np.ascontiguousarray(bbox6, dtype=np.float64)),
-                                              _ptr(keys)))
+                                              _lib.SFC_KINDS[kind], _ptr(keys)))
         return keys
 
-    def redistribute(self, sample: int = 4096) -> None:
-        """exchange_domain_sfc with a fresh SfcDecomposition: Hilbert keys over
-        the all-ranks bounding box; cut points at the count quantiles of a
-        regular sample of every rank's sorted keys (every key when a rank holds
-        at most `sample`); particles move to rank_for(key).  Accelerations are
-        recomputed by the next force evaluation."""
+    def redistribute(self, sample: int = 4096, kind: str = "morton") -> None:
+        """exchange_domain_sfc with a fresh SfcDecomposition: keys of `kind`
+        (the reference's SfcKind) over the all-ranks bounding box; cut points at
+        the count quantiles of a regular sample of every rank's sorted keys
+        (every key when a rank holds at most `sample`); particles move to
+        rank_for(key).  Morton by default: the reference's Hilbert keys pack the
+        finest coordinate bits first, so their domains span the whole box and
+        the AABB halo rule then sends every particle to every rank.
+        Accelerations are recomputed by the next force evaluation."""
         ex = self.ex
         bbox = union_bbox(ex.allgather_f64(self.owned_aabb()))
-        keys = self.sfc_keys(bbox)
+        keys = self.sfc_keys(bbox, kind)
         sk = np.sort(keys)
         m = sk.shape[0]
         take = sk if m <= sample else sk[(np.arange(sample, dtype=np.int64) * m) // sample]

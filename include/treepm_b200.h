@@ -237,10 +237,15 @@ int tpm_force_end(tpm_handle* h, double g, double kick);
  * then v += a kick_half (the cached acceleration rescaled by g / g_prev) and
  * the drift with the periodic wrap, for the owned particles. */
 int tpm_kick_drift(tpm_handle* h, double kick_half, double drift, double g);
-/* particle_hilbert keys (crates/gadget-ng-parallel/src/sfc.rs:187-204) of the
- * owned particles over a given box {xlo, xhi, ylo, yhi, zlo, zhi} (all ranks'
- * bounding box for SfcDecomposition, sfc.rs:336-393), original order. */
-int tpm_sfc_keys(tpm_handle* h, const double bbox6[6], uint64_t* keys);
+/* SFC keys of the owned particles over a given box {xlo, xhi, ylo, yhi, zlo,
+ * zhi} (all ranks' bounding box for SfcDecomposition, sfc.rs:336-393),
+ * original order.  kind (SfcKind): TPM_SFC_HILBERT = particle_hilbert
+ * (sfc.rs:187-204; its keys pack the coordinate bits lowest level first, so
+ * nearby keys need not be nearby in space), TPM_SFC_MORTON = particle_morton
+ * (sfc.rs:54-81, Z order). */
+#define TPM_SFC_HILBERT 0
+#define TPM_SFC_MORTON 1
+int tpm_sfc_keys(tpm_handle* h, const double bbox6[6], int32_t kind, uint64_t* keys);
 /* Owned and resident (owned + halo) particle counts. */
 int tpm_particle_counts(const tpm_handle* h, int64_t* n_owned, int64_t* n_resident);
 

@@ -142,3 +142,25 @@ def rank_for(key, cuts, n_ranks):
         else:
             return min(mid + 1, n_ranks - 1)
     return min(lo, n_ranks - 1)
+
+
+def spread_bits(x):
+    """sfc.rs:39-47: the 21 low bits of x to every third bit."""
+    x = np.asarray(x, dtype=np.uint64) & np.uint64(0x1FFFFF)
+    for sh, m in ((32, 0x1F00000000FFFF), (16, 0x1F0000FF0000FF), (8, 0x100F00F00F00F00F),
+                  (4, 0x10C30C30C30C30C3), (2, 0x1249249249249249)):
+        x = (x | (x << np.uint64(sh))) & np.uint64(m)
+    return x
+
+
+def morton_keys(pos, bbox6):
+    """particle_morton (sfc.rs:54-81) over the box {xlo, xhi, ylo, yhi, zlo, zhi}."""
+    pos = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    eps = np.finfo(np.float64).eps
+    c = []
+    for k in range(3):
+        lo, hi = bbox6[2 * k], bbox6[2 * k + 1]
+        ln = max(hi - lo, eps)
+        v = np.clip((pos[:, k] - lo) / ln, 0.0, 1.0 - eps)
+        c.append((v * 2097152.0).astype(np.uint64))
+    return spread_bits(c[0]) | (spread_bits(c[1]) << np.uint64(1)) | (spread_bits(c[2]) << np.uint64(2))

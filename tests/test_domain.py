@@ -209,3 +209,20 @@ def test_exchange_layer_two_gloo_ranks():
         np.testing.assert_array_equal(got, exp)
         np.testing.assert_array_equal(aabbs, np.stack([dom().compute_aabb_3d(p) for p in parts]))
         assert np.all(t == 3.0)
+
+
+def test_morton_keys_pins():
+    """morton_zero_maps_to_zero, morton_order_preserves_locality and
+    spread_bits_and_back of crates/gadget-ng-parallel/src/sfc.rs."""
+    d = dom()
+    unit = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]
+    k = d.morton_keys([[0.0, 0.0, 0.0], [0.1, 0.1, 0.1], [0.15, 0.12, 0.11], [0.9, 0.9, 0.9]], unit)
+    assert k[0] == 0 and k[1] < k[3] and k[2] < k[3]
+    for x in (0, 1, 42, 1048575, (1 << 21) - 1):
+        s = int(d.spread_bits(np.array([x], dtype=np.uint64))[0])
+        assert s & ~0x1249249249249249 == 0
+        # every third bit of s, gathered, is x again
+        assert sum(((s >> (3 * i)) & 1) << i for i in range(21)) == x
+    # Z order: the top three key bits are the octant (z, y, x)
+    k = d.morton_keys([[0.7, 0.2, 0.6]], unit)[0]
+    assert int(k) >> 60 == 0b101

@@ -20,7 +20,7 @@ from conftest import REPO, oracle
 
 pytestmark = pytest.mark.gpu
 
-NM, BOX, RCF = 32, 100.0, 4.5
+NM, BOX, RCF = 64, 100.0, 4.5  # r_cut = 8.8 % of the box: partial halos
 
 
 def dom():
@@ -103,7 +103,9 @@ def case():
     a0, a1 = 0.1, 0.102
     drift, kh, kh2 = treepm.drift_kick_factors(ics.OMEGA_M, ics.OMEGA_L, 1.0, a0, ics.time_between(a0, a1))
     phys.update(drift=drift, kh=kh, kh2=kh2)
-    keys, _ = oracle().hilbert_keys(pos)
+    # Morton domains (the reference's Hilbert keys give domains spanning the
+    # box, whose halos hold every particle)
+    keys = dom().morton_keys(pos, dom().compute_aabb_3d(pos))
     cuts = dom().cutpoints(np.sort(keys), 2)
     owner = np.array([dom().rank_for(k, cuts, 2) for k in keys])
     gids = [np.nonzero(owner == r)[0] for r in range(2)]
@@ -119,7 +121,7 @@ def test_domain_forces_and_interaction_sets_match_oracle(case):
                                                    ph["r_split"], RCF)
     for r in range(2):
         out, g = c["res"][r], c["gids"][r]
-        assert out["n_halo"] == halos[r].size
+        assert 0 < out["n_halo"] == halos[r].size < c["gids"][1 - r].size  # a partial halo
         np.testing.assert_array_equal(out["counts"], cnt[g])
         assert _rel(out["acc"], acc[g]) < 1e-5
         assert np.sqrt(np.sum((out["sr"] - sr[g]) ** 2) / np.sum(sr[g] ** 2)) < 1e-5
@@ -161,3 +163,26 @@ def test_redistribute_keeps_every_particle_once(case):
     acc = dom().distributed_treepm(p1, c["mass"], owner, ph["eps2"], ph["g"], NM, BOX, ph["r_split"], RCF)[0]
     for r in range(2):
         assert _rel(c["res"][r]["a2"], acc[c["res"][r]["g2"]]) < 1e-5
+
+
+def test_sfc_keys_bit_exact():
+    """tpm_sfc_keys: particle_hilbert over the positions' bounding box equals
+    the oracle's Hilbert keys; particle_morton equals the restatement for that
+    box and for a wider one."""
+    import ctypes as C
+    import treepm
+    from treepm import ics
+    b = ics.clustered_box(16, BOX, 0.3, 6, min_halo=20, max_halo=200, r_min=0.3, r_max=1.5, seed=31)
+    pos = b.positions()
+    s = treepm.TreePmSolver(NM, BOX, 1.25 * BOX / NM)
+    s.set_particles(pos, b.mass)
+    L = s._h._lib
+    for bbox in (dom().compute_aabb_3d(pos), np.array([0.0, BOX, -1.0, BOX + 3.0, 0.5, BOX])):
+        for kind in (0, 1):
+            keys = np.empty(pos.shape[0], dtype=np.uint64)
+            bb = np.ascontiguousarray(bbox, dtype=np.float64)
+            assert L.tpm_sfc_keys(s._h.h, bb.ctypes.data_as(C.c_void_p), kind, keys.ctypes.data_as(C.c_void_p)) == 0
+            if kind == 1:
+                np.testing.assert_array_equal(keys, dom().morton_keys(pos, bbox))
+            elif bbox[1] == pos[:, 0].max():
+                np.testing.assert_array_equal(keys, oracle().hilbert_keys(pos)[0])
