@@ -551,8 +551,9 @@ def run_b200(args):
         "e2e": {"value": e2e_value, "unit": "particle-updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
                 "path": "tpm_kdk_step_host: float64 positions, velocities and masses from pinned host memory, "
-                        "state back to host each step; the library reuses its resident closing acceleration when the inputs "
-                        "equal the state it returned (checked on the device), so one force evaluation per step"},
+                        "state back to host each step; the inputs are the state the previous call returned, so the "
+                        "step runs on the resident state (one force evaluation) while a copy stream uploads and checks "
+                        "the inputs and returns the drifted positions; the momenta are copied after the closing kick"},
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "force_error_vs_ewald": ewald,
         "accurate_mode": accurate,

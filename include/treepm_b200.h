@@ -158,11 +158,14 @@ int tpm_compute_forces(tpm_handle* h, double eps2, double g);
  * when eps2 changed or no acceleration is cached. */
 int tpm_kdk_step(tpm_handle* h, double kick_half, double drift, double kick_half2, double eps2, double g);
 /* Host KDK step: state in host buffers (n x 3 float64 pos / vel), copied to
- * the device, advanced by tpm_kdk_step, copied back (original order).  When
- * the inputs equal the resident state (the caller hands back what the
- * previous call returned; checked on the device after the copy), the
- * resident closing acceleration opens the step and one force evaluation is
- * made; otherwise the inputs are re-encoded and the step evaluates twice. */
+ * the device, advanced as tpm_kdk_step, copied back (original order).  When
+ * the caller hands back the state the previous call returned (and nothing
+ * changed the handle's state since), the step runs on the resident state at
+ * once with its closing acceleration (one force evaluation) while a second
+ * stream uploads the inputs, checks them bit for bit against the returned
+ * state and copies the new positions back; the momenta follow the closing
+ * kick.  Inputs that differ are re-encoded from the upload and stepped with
+ * two force evaluations (the speculative one is discarded). */
 int tpm_kdk_step_host(tpm_handle* h, double* pos, double* vel, const double* mass, int64_t n, double kick_half,
                       double drift, double kick_half2, double eps2, double g);
 /* Read back state in the original particle order (any pointer may be NULL). */
