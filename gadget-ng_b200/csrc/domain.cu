@@ -80,6 +80,66 @@ __global__ void k_halo_flags(const uint32_t* __restrict__ qx, const uint32_t* __
   }
 }
 
+__device__ __forceinline__ int cell_of(uint32_t q, int g) { return (int)(((uint64_t)q * (uint64_t)g) >> 32); }
+
+__global__ void k_occupancy(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                            const uint32_t* __restrict__ qz, int64_t n, int g, uint32_t* __restrict__ bits) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t c = ((int64_t)cell_of(qz[i], g) * g + cell_of(qy[i], g)) * g + cell_of(qx[i], g);
+  const uint32_t w = (uint32_t)(c >> 5), b = 1u << (c & 31);
+  // one atomic per word and warp
+  const uint32_t peers = __match_any_sync(__activemask(), w);
+  const uint32_t m = __reduce_or_sync(peers, b);
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicOr(&bits[w], m);
+}
+
+// the gap between coordinate x (in cell ci) and the neighbour cell at offset o
+__device__ __forceinline__ double face_gap(double x, int ci, int o, double cell) {
+  if (o == 0) return 0.0;
+  return o > 0 ? dsub(dmul((double)(ci + 1), cell), x) : dsub(x, dmul((double)ci, cell));
+}
+
+__global__ void k_halo_flags_cells(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                                   const uint32_t* __restrict__ qz, int64_t n, double scale, double cell, int g,
+                                   const uint32_t* __restrict__ bits, int64_t words, int n_ranks, int rank,
+                                   double w2, uint64_t* __restrict__ flags, unsigned long long* __restrict__ counts) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool live = i < n;
+  uint64_t f = 0;
+  if (live) {
+    const uint32_t q[3] = {qx[i], qy[i], qz[i]};
+    int ci[3];
+    double x[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      ci[k] = cell_of(q[k], g);
+      x[k] = decode(q[k], scale);
+    }
+    for (int oz = -1; oz <= 1; ++oz)
+      for (int oy = -1; oy <= 1; ++oy)
+        for (int ox = -1; ox <= 1; ++ox) {
+          const double gx = face_gap(x[0], ci[0], ox, cell), gy = face_gap(x[1], ci[1], oy, cell);
+          const double gz = face_gap(x[2], ci[2], oz, cell);
+          if (!(dadd(dadd(dmul(gx, gx), dmul(gy, gy)), dmul(gz, gz)) < w2)) continue;
+          const int cx = (ci[0] + ox + g) % g, cy = (ci[1] + oy + g) % g, cz = (ci[2] + oz + g) % g;
+          const int64_t c = ((int64_t)cz * g + cy) * g + cx;
+          for (int r = 0; r < n_ranks; ++r)
+            if (r != rank && ((__ldg(&bits[r * words + (c >> 5)]) >> (c & 31)) & 1u)) f |= 1ull << r;
+        }
+    flags[i] = f;
+  }
+  const uint64_t any = __reduce_or_sync(0xffffffffu, (uint32_t)f) |
+                       ((uint64_t)__reduce_or_sync(0xffffffffu, (uint32_t)(f >> 32)) << 32);
+  uint64_t rest = any;
+  while (rest) {
+    const int r = __ffsll((long long)rest) - 1;
+    rest &= rest - 1;
+    const unsigned cnt = __popc(__ballot_sync(0xffffffffu, (f >> r) & 1ull));
+    if ((threadIdx.x & 31) == 0) atomicAdd(&counts[r], (unsigned long long)cnt);
+  }
+}
+
 __global__ void k_bit(const uint64_t* __restrict__ flags, int64_t n, int r, uint32_t* __restrict__ bit) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) bit[i] = (uint32_t)((flags[i] >> r) & 1ull);
@@ -167,6 +227,24 @@ void halo_flags(const Particles& P, int64_t n, double scale, double box, const A
   TPM_CUDA(cudaMemsetAsync(counts_dev, 0, sizeof(unsigned long long) * MAX_RANKS, s));
   if (n == 0) return;
   k_halo_flags<<<blocks_of(n), 256, 0, s>>>(P.qx, P.qy, P.qz, n, scale, box, t, n_ranks, rank, w2, flags, counts_dev);
+  TPM_LAUNCH_CHECK();
+}
+
+void occupancy(const Particles& P, int64_t n, int grid, uint32_t* bits, cudaStream_t s) {
+  const int64_t words = ((int64_t)grid * grid * grid + 31) / 32;
+  TPM_CUDA(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * words, s));
+  if (n == 0) return;
+  k_occupancy<<<blocks_of(n), 256, 0, s>>>(P.qx, P.qy, P.qz, n, grid, bits);
+  TPM_LAUNCH_CHECK();
+}
+
+void halo_flags_cells(const Particles& P, int64_t n, double scale, double cell, int grid, const uint32_t* bits,
+                      int64_t words, int n_ranks, int rank, double w2, uint64_t* flags,
+                      unsigned long long* counts_dev, cudaStream_t s) {
+  TPM_CUDA(cudaMemsetAsync(counts_dev, 0, sizeof(unsigned long long) * MAX_RANKS, s));
+  if (n == 0) return;
+  k_halo_flags_cells<<<blocks_of(n), 256, 0, s>>>(P.qx, P.qy, P.qz, n, scale, cell, grid, bits, words, n_ranks, rank,
+                                                  w2, flags, counts_dev);
   TPM_LAUNCH_CHECK();
 }
 

@@ -40,6 +40,20 @@ void owned_bounds(const Particles& P, int64_t n, uint32_t* scratch6, uint32_t ou
 void halo_flags(const Particles& P, int64_t n, double scale, double box, const AabbTable& t, int n_ranks, int rank,
                 double w2, uint64_t* flags, unsigned long long* counts_dev, cudaStream_t s);
 
+// Occupancy of a coarse periodic grid of `grid`^3 cells (cell index
+// ((z g + y) g + x), x = (q g) >> 32) by particles [0, n): bit c of words
+// bits[c >> 5] (cleared first, (grid^3 + 31) / 32 words).
+void occupancy(const Particles& P, int64_t n, int grid, uint32_t* bits, cudaStream_t s);
+
+// flags[i]: bit r set when some cell that rank r occupies (bits + r * words)
+// among the 27 around particle i's cell lies within sqrt(w2) of it (periodic
+// gaps to the cell's faces, float64); cells are at least the halo width wide,
+// so every particle of r within that distance is in one of them.
+// counts_dev[r] (zeroed here) = bits r set.
+void halo_flags_cells(const Particles& P, int64_t n, double scale, double cell, int grid, const uint32_t* bits,
+                      int64_t words, int n_ranks, int rank, double w2, uint64_t* flags,
+                      unsigned long long* counts_dev, cudaStream_t s);
+
 // The particles with bit r of flags, in index order, as records at out.
 void halo_pack(const Particles& P, int64_t n, const uint64_t* flags, int r, uint32_t* bit, uint32_t* pos,
                void* scan_scratch, HaloRecord* out, cudaStream_t s);

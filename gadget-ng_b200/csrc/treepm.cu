@@ -284,6 +284,7 @@ struct tpm_handle {
   uint32_t* dom_a = nullptr;
   uint32_t* dom_b = nullptr;
   unsigned long long* dom_counts = nullptr;  // MAX_RANKS, persistent
+  uint32_t* dom_bits = nullptr;              // every rank's cell occupancy, MAX_RANKS x 64^3 bits, persistent
   // Host-buffer steps (tpm_kdk_step_host): the state the last call returned
   // (original order; positions then momenta, 6n float64) in two buffers, the
   // inputs of this call (7n) and a flag word; the state version that state
@@ -1060,6 +1061,75 @@ int tpm_halo_select(tpm_handle* h, const double* aabbs, int32_t n_ranks, int32_t
     const Particles& P = h->P[h->cur];
     halo_flags(P, n, h->cfg.box_size / TWO32, h->cfg.box_size, t, n_ranks, rank, width * width, h->dom_flags,
                h->dom_counts, s);
+    unsigned long long c[MAX_RANKS];
+    TPM_CUDA(cudaMemcpyAsync(c, h->dom_counts, sizeof(c), cudaMemcpyDeviceToHost, s));
+    TPM_CUDA(cudaStreamSynchronize(s));
+    int64_t total = 0;
+    for (int r = 0; r < n_ranks; ++r) {
+      counts[r] = (int64_t)c[r];
+      total += (int64_t)c[r];
+    }
+    if (!send) return TPM_OK;
+    if (total > cap) throw Error(TPM_ERR_INVALID_ARGUMENT, "halo send buffer holds " + std::to_string(cap) +
+                                                               " records, " + std::to_string(total) + " selected");
+    int64_t off = 0;
+    for (int r = 0; r < n_ranks; ++r) {
+      if (c[r] == 0) continue;
+      halo_pack(P, n, h->dom_flags, r, h->dom_a, h->dom_b, h->scan_scratch,
+                reinterpret_cast<HaloRecord*>(send) + off, s);
+      off += (int64_t)c[r];
+    }
+    TPM_CUDA(cudaStreamSynchronize(s));
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+// The occupancy grid for a halo width: cells at least `width` wide, at most
+// 64 per axis.
+static int occupancy_grid(double box, double width) {
+  const double g = width > 0.0 ? std::floor(box / width) : 64.0;
+  return (int)std::max(1.0, std::min(64.0, g));
+}
+
+int tpm_occupancy(tpm_handle* h, double width, int32_t* grid, uint32_t* bits) {
+  if (!h || !grid || !(width >= 0.0)) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
+    const int g = occupancy_grid(h->cfg.box_size, width);
+    *grid = g;
+    if (!bits) return TPM_OK;
+    if (!h->dom_bits) h->dom_bits = h->alloc<uint32_t>((size_t)MAX_RANKS * 8192, 0);
+    const int64_t words = ((int64_t)g * g * g + 31) / 32;
+    occupancy(h->P[h->cur], h->n_owned, g, h->dom_bits, h->stream);
+    TPM_CUDA(cudaMemcpyAsync(bits, h->dom_bits, sizeof(uint32_t) * words, cudaMemcpyDeviceToHost, h->stream));
+    TPM_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+int tpm_halo_select_cells(tpm_handle* h, const uint32_t* bits, int32_t grid, int32_t n_ranks, int32_t rank,
+                          double width, int64_t* counts, tpm_halo_record* send, int64_t cap) {
+  if (!h || !bits || !counts || n_ranks < 1 || n_ranks > MAX_RANKS || rank < 0 || rank >= n_ranks ||
+      !(width >= 0.0) || cap < 0 || grid != occupancy_grid(h->cfg.box_size, width))
+    return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    drop_halos(h);
+    cudaStream_t s = h->stream;
+    const int64_t words = ((int64_t)grid * grid * grid + 31) / 32;
+    if (!h->dom_bits) h->dom_bits = h->alloc<uint32_t>((size_t)MAX_RANKS * 8192, 0);
+    TPM_CUDA(cudaMemcpyAsync(h->dom_bits, bits, sizeof(uint32_t) * words * n_ranks, cudaMemcpyHostToDevice, s));
+    const int64_t n = h->n_owned;
+    const Particles& P = h->P[h->cur];
+    // the halo width with a relative margin of 1e-9 for the float64 face gaps
+    const double w2 = width * width * (1.0 + 1e-9);
+    halo_flags_cells(P, n, h->cfg.box_size / TWO32, h->cfg.box_size / grid, grid, h->dom_bits, words, n_ranks, rank,
+                     w2, h->dom_flags, h->dom_counts, s);
     unsigned long long c[MAX_RANKS];
     TPM_CUDA(cudaMemcpyAsync(c, h->dom_counts, sizeof(c), cudaMemcpyDeviceToHost, s));
     TPM_CUDA(cudaStreamSynchronize(s));

@@ -208,6 +208,8 @@ SIGNATURES = {
     "tpm_kick_drift": ([_P, _D, _D, _D], _I),
     "tpm_particle_counts": ([_P, C.POINTER(_I64), C.POINTER(_I64)], _I),
     "tpm_sfc_keys": ([_P, _P, C.c_int32, _P], _I),
+    "tpm_occupancy": ([_P, _D, C.POINTER(C.c_int32), _P], _I),
+    "tpm_halo_select_cells": ([_P, _P, C.c_int32, C.c_int32, C.c_int32, _D, _P, _P, _I64], _I),
 }
 HALO_RECORD_BYTES = 24  # tpm_halo_record
 SFC_KINDS = {"hilbert": 0, "morton": 1}

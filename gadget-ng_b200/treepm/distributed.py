@@ -104,6 +104,14 @@ class _Exchange:
         self.dist.all_gather(out, t, group=self.group)
         return np.stack([o.cpu().numpy() for o in out])
 
+    def allgather_u32(self, local: np.ndarray) -> np.ndarray:
+        """allgather of uint32 words: (size, len) array."""
+        torch = self.torch
+        t = self._home(torch.from_numpy(np.ascontiguousarray(local, dtype=np.uint32).view(np.int32)))
+        out = [torch.empty_like(t) for _ in range(self.size)]
+        self.dist.all_gather(out, t, group=self.group)
+        return np.stack([o.cpu().numpy().view(np.uint32) for o in out])
+
     def alltoall_counts(self, counts: np.ndarray) -> np.ndarray:
         torch = self.torch
         send = self._home(torch.from_numpy(np.ascontiguousarray(counts, dtype=np.int64)))
@@ -139,10 +147,17 @@ class _Exchange:
 class DomainTreePm:
     """One rank of the domain-decomposed TreePM (constructor keys as
     `TreePmSolver`; the periodic walk).  `group` is the torch.distributed
-    process group (default: the world)."""
+    process group (default: the world).  `halo`: "aabb" selects halos by the
+    reference's rule (within r_cut of another rank's particle AABB); "cells"
+    by the cells that rank occupies on a grid at least r_cut wide, which keeps
+    every pair within r_cut and sends far fewer particles once domains are
+    not slabs (the short-range trees then differ from the reference's)."""
 
     def __init__(self, grid_size: int, box_size: float, r_split: float = 0.0, *, r_cut_factor: float = 5.0,
-                 device: int = 0, group=None, overlap: bool = True):
+                 device: int = 0, group=None, overlap: bool = True, halo: str = "aabb"):
+        if halo not in ("aabb", "cells"):
+            raise ValueError("halo is 'aabb' or 'cells'")
+        self.halo = halo
         import torch
         import torch.distributed as dist
         if not dist.is_initialized():
@@ -198,17 +213,31 @@ class DomainTreePm:
         received (now resident in the handle)."""
         torch = self.torch
         ex = self.ex
-        aabbs = ex.allgather_f64(self.owned_aabb())
-        counts = np.zeros(ex.size, dtype=np.int64)
         h = self._h.h
-        check(h, self._L.tpm_halo_select(h, _ptr(np.ascontiguousarray(aabbs.reshape(-1))), ex.size, ex.rank,
-                                         float(self.r_cut), _ptr(counts), None, 0))
+        counts = np.zeros(ex.size, dtype=np.int64)
+        if self.halo == "aabb":
+            table = np.ascontiguousarray(ex.allgather_f64(self.owned_aabb()).reshape(-1))
+
+            def select(send, cap):
+                check(h, self._L.tpm_halo_select(h, _ptr(table), ex.size, ex.rank, float(self.r_cut), _ptr(counts),
+                                                 send, cap))
+        else:
+            grid = C.c_int32()
+            check(h, self._L.tpm_occupancy(h, float(self.r_cut), C.byref(grid), None))
+            words = (grid.value ** 3 + 31) // 32
+            mine = np.zeros(words, dtype=np.uint32)
+            check(h, self._L.tpm_occupancy(h, float(self.r_cut), C.byref(grid), _ptr(mine)))
+            table = np.ascontiguousarray(ex.allgather_u32(mine).reshape(-1))
+
+            def select(send, cap):
+                check(h, self._L.tpm_halo_select_cells(h, _ptr(table), grid.value, ex.size, ex.rank,
+                                                       float(self.r_cut), _ptr(counts), send, cap))
+        select(None, 0)
         total = int(counts.sum())
         rb = _lib.HALO_RECORD_BYTES
         send = torch.empty(max(total * rb, rb), dtype=torch.uint8, device=self.device)
         if total:
-            check(h, self._L.tpm_halo_select(h, _ptr(np.ascontiguousarray(aabbs.reshape(-1))), ex.size, ex.rank,
-                                             float(self.r_cut), _ptr(counts), C.c_void_p(send.data_ptr()), total))
+            select(C.c_void_p(send.data_ptr()), total)
         recv_counts = ex.alltoall_counts(counts)
         recv = ex.alltoallv_bytes(send, counts * rb, recv_counts * rb)
         if ex.on_device:

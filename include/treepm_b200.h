@@ -220,6 +220,19 @@ int tpm_owned_aabb(tpm_handle* h, double aabb6[6]);
  * TPM_ERR_INVALID_ARGUMENT with counts filled and nothing written. */
 int tpm_halo_select(tpm_handle* h, const double* aabbs, int32_t n_ranks, int32_t rank, double width,
                     int64_t* counts, tpm_halo_record* send, int64_t cap);
+/* A tighter halo rule than the AABB (extension; the short-range trees then
+ * differ from the reference's, the interaction sets within r_cut do not): a
+ * periodic grid of *grid = min(64, floor(L / width)) cells per axis (cells at
+ * least `width` wide); tpm_occupancy writes the owned particles' occupancy
+ * (bit c of bits[c / 32], c = (z g + y) g + x, (g^3 + 31) / 32 words; bits may
+ * be NULL to get the grid only).  tpm_halo_select_cells takes every rank's
+ * occupancy (n_ranks x words, host) and selects for rank r != rank the owned
+ * particles within `width` of a cell that r occupies among the 27 around the
+ * particle's own (float64 gaps to the cell faces, width^2 widened by 1e-9
+ * relative); counts and send as tpm_halo_select. */
+int tpm_occupancy(tpm_handle* h, double width, int32_t* grid, uint32_t* bits);
+int tpm_halo_select_cells(tpm_handle* h, const uint32_t* bits, int32_t grid, int32_t n_ranks, int32_t rank,
+                          double width, int64_t* counts, tpm_halo_record* send, int64_t cap);
 /* Replace the halo copies by n records (device memory, e.g. the halo
  * alltoallv's receive buffer); owned particles are kept. */
 int tpm_set_halos(tpm_handle* h, const tpm_halo_record* recv, int64_t n);

@@ -92,7 +92,63 @@ def exchange_halos(parts, width, box):
     return [[(q, sends[q][r]) for q in range(len(parts)) if r in sends[q]] for r in range(len(parts))]
 
 
-def distributed_treepm(pos, mass, owner, eps2, g, nm, box, r_split, r_cut_factor):
+def fixed_point(pos, box):
+    """The 32-bit fixed-point coordinates of positions on the lattice x = q L / 2^32."""
+    u = np.mod(np.asarray(pos, dtype=np.float64) / box, 1.0)
+    return (np.rint(u * 2.0 ** 32).astype(np.uint64) & np.uint64(0xFFFFFFFF)).astype(np.uint64)
+
+
+def occupancy_grid(box, width):
+    g = np.floor(box / width) if width > 0 else 64.0
+    return int(max(1.0, min(64.0, g)))
+
+
+def occupied_cells(q, g):
+    """Boolean g^3 occupancy of particles with fixed-point coordinates q (n, 3)."""
+    c = ((np.asarray(q, dtype=np.uint64).reshape(-1, 3) * np.uint64(g)) >> np.uint64(32)).astype(np.int64)
+    occ = np.zeros(g ** 3, dtype=bool)
+    occ[(c[:, 2] * g + c[:, 1]) * g + c[:, 0]] = True
+    return occ
+
+
+def cells_halo_selection(q_own, occs, rank, width, box):
+    """The cell rule of the library's tpm_halo_select_cells for one rank's
+    particles (fixed point q_own): per destination rank, the indices within
+    `width` (float64 face gaps, width^2 widened by 1e-9) of a cell that rank
+    occupies among the 27 around each particle's cell."""
+    g = occupancy_grid(box, width)
+    q = np.asarray(q_own, dtype=np.uint64).reshape(-1, 3)
+    ci = ((q * np.uint64(g)) >> np.uint64(32)).astype(np.int64)
+    x = q.astype(np.float64) * (box / 2.0 ** 32)
+    cell = box / g
+    w2 = width * width * (1.0 + 1e-9)
+    sel = {r: np.zeros(q.shape[0], dtype=bool) for r in range(len(occs)) if r != rank}
+    for oz in (-1, 0, 1):
+        for oy in (-1, 0, 1):
+            for ox in (-1, 0, 1):
+                gaps = []
+                for k, o in enumerate((ox, oy, oz)):
+                    if o == 0:
+                        gaps.append(np.zeros(q.shape[0]))
+                    elif o > 0:
+                        gaps.append((ci[:, k] + 1).astype(np.float64) * cell - x[:, k])
+                    else:
+                        gaps.append(x[:, k] - ci[:, k].astype(np.float64) * cell)
+                ok = (gaps[0] * gaps[0] + gaps[1] * gaps[1]) + gaps[2] * gaps[2] < w2
+                c = (((ci[:, 2] + oz) % g) * g + (ci[:, 1] + oy) % g) * g + (ci[:, 0] + ox) % g
+                for r in sel:
+                    sel[r] |= ok & occs[r][c]
+    return {r: np.nonzero(m)[0] for r, m in sel.items() if m.any()}
+
+
+def exchange_halos_cells(qparts, width, box):
+    g = occupancy_grid(box, width)
+    occs = [occupied_cells(q, g) for q in qparts]
+    sends = [cells_halo_selection(qparts[r], occs, r, width, box) for r in range(len(qparts))]
+    return [[(q, sends[q][r]) for q in range(len(qparts)) if r in sends[q]] for r in range(len(qparts))]
+
+
+def distributed_treepm(pos, mass, owner, eps2, g, nm, box, r_split, r_cut_factor, halo="aabb"):
     """Accelerations of every particle under the decomposition `owner` (rank
     of each particle): the serial TreePM's long range plus, per rank, the
     periodic short range over its particles and its halos.  Returns
@@ -104,7 +160,11 @@ def distributed_treepm(pos, mass, owner, eps2, g, nm, box, r_split, r_cut_factor
     n_ranks = int(owner.max()) + 1 if owner.size else 1
     members = [np.nonzero(owner == r)[0] for r in range(n_ranks)]
     r_cut = r_cut_factor * r_split
-    halos = exchange_halos([pos[m] for m in members], r_cut, box)
+    if halo == "aabb":
+        halos = exchange_halos([pos[m] for m in members], r_cut, box)
+    else:
+        q = fixed_point(pos, box)
+        halos = exchange_halos_cells([q[m] for m in members], r_cut, box)
     lr = _o.treepm(pos, mass, eps2, g, nm, box, r_split, r_cut_factor, parts=True)["lr"]
     sr = np.zeros_like(pos)
     cnt = np.zeros((pos.shape[0], 2), dtype=np.int64)

@@ -226,3 +226,30 @@ def test_morton_keys_pins():
     # Z order: the top three key bits are the octant (z, y, x)
     k = d.morton_keys([[0.7, 0.2, 0.6]], unit)[0]
     assert int(k) >> 60 == 0b101
+
+
+def test_cells_halo_covers_every_pair_and_is_smaller():
+    """The cell rule (tpm_halo_select_cells) keeps every cross-rank pair within
+    r_cut and, on Morton domains, sends fewer particles than the AABB rule."""
+    from treepm import distributed as D
+    pos, mass = _box(12, 9)
+    keys = dom().morton_keys(pos, dom().compute_aabb_3d(pos))
+    P = 4
+    owner = D.rank_for(keys, D.cutpoints_from_keys(np.sort(keys), P), P)
+    r_cut = 4.5 * 1.25 / 48
+    q = dom().fixed_point(pos, 1.0)
+    assert np.array_equal(q.astype(np.float64) * 2.0 ** -32, pos)
+    cells = dom().exchange_halos_cells([q[owner == r] for r in range(P)], r_cut, 1.0)
+    aabb = dom().exchange_halos([pos[owner == r] for r in range(P)], r_cut, 1.0)
+    members = [np.nonzero(owner == r)[0] for r in range(P)]
+    n_cells = n_aabb = 0
+    for r in range(P):
+        got = np.concatenate([members[s][i] for s, i in cells[r]]) if cells[r] else np.zeros(0, dtype=int)
+        n_cells += got.size
+        n_aabb += sum(i.size for _, i in aabb[r])
+        other = np.nonzero(owner != r)[0]
+        d = dom().minimum_image_scalar(pos[members[r]][:, None, :] - pos[other][None, :, :], 1.0)
+        near = other[np.any(np.sum(d * d, axis=2) < r_cut * r_cut, axis=0)]
+        assert set(near) <= set(got.tolist())
+        assert len(set(got.tolist())) == got.size
+    assert n_cells < n_aabb

@@ -39,7 +39,7 @@ def _rel(a, b):
     return float(np.sqrt(np.mean(r * r)))
 
 
-def _rank_main(rank, world, port, local, phys, q):
+def _rank_main(rank, world, port, local, phys, q, halo="aabb", force_only=False):
     import torch.distributed as dist
     from datetime import timedelta
     sys.path.insert(0, os.path.join(REPO, "gadget-ng_b200"))
@@ -47,7 +47,7 @@ def _rank_main(rank, world, port, local, phys, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
     try:
         from treepm.distributed import DomainTreePm
-        d = DomainTreePm(NM, BOX, phys["r_split"], r_cut_factor=RCF, device=0)
+        d = DomainTreePm(NM, BOX, phys["r_split"], r_cut_factor=RCF, device=0, halo=halo)
         pos, vel, mass, gid = local
         d.set_particles(pos, mass, vel, gid=gid)
         d.compute_forces(phys["eps2"], phys["g"])
@@ -55,6 +55,9 @@ def _rank_main(rank, world, port, local, phys, q):
         counts = d.interaction_counts()
         lr, sr = d.force_parts()
         n_halo = d.last_halo_count
+        if force_only:
+            q.put((rank, dict(acc=acc, counts=counts, sr=sr, n_halo=n_halo)))
+            return
         d.kdk_step(phys["kh"], phys["drift"], phys["kh2"], phys["eps2"], phys["g"])
         _, p1, v1, a1 = d.get_state()
         d.redistribute(sample=64)
@@ -68,12 +71,13 @@ def _rank_main(rank, world, port, local, phys, q):
         dist.destroy_process_group()
 
 
-def _run_ranks(parts, phys):
+def _run_ranks(parts, phys, halo="aabb", force_only=False):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, len(parts), port, parts[r], phys, q)) for r in range(len(parts))]
+    procs = [ctx.Process(target=_rank_main, args=(r, len(parts), port, parts[r], phys, q, halo, force_only))
+             for r in range(len(parts))]
     for p in procs:
         p.start()
     res = {}
@@ -111,7 +115,8 @@ def case():
     gids = [np.nonzero(owner == r)[0] for r in range(2)]
     parts = [(pos[g], vel[g], mass[g], g) for g in gids]
     res = _run_ranks(parts, phys)
-    return dict(pos=pos, vel=vel, mass=mass, owner=owner, gids=gids, phys=phys, res=res)
+    cells = _run_ranks(parts, phys, halo="cells", force_only=True)
+    return dict(pos=pos, vel=vel, mass=mass, owner=owner, gids=gids, phys=phys, res=res, cells=cells)
 
 
 def test_domain_forces_and_interaction_sets_match_oracle(case):
@@ -186,3 +191,17 @@ def test_sfc_keys_bit_exact():
                 np.testing.assert_array_equal(keys, dom().morton_keys(pos, bbox))
             elif bbox[1] == pos[:, 0].max():
                 np.testing.assert_array_equal(keys, oracle().hilbert_keys(pos)[0])
+
+
+def test_cell_halo_rule_matches_oracle(case):
+    """halo="cells": halo counts and interaction sets bit-exact with the
+    restatement of the cell rule, accelerations within 1e-5 rms."""
+    c = case
+    ph = c["phys"]
+    acc, sr, cnt, halos = dom().distributed_treepm(c["pos"], c["mass"], c["owner"], ph["eps2"], ph["g"], NM, BOX,
+                                                   ph["r_split"], RCF, halo="cells")
+    for r in range(2):
+        out, g = c["cells"][r], c["gids"][r]
+        assert out["n_halo"] == halos[r].size
+        np.testing.assert_array_equal(out["counts"], cnt[g])
+        assert _rel(out["acc"], acc[g]) < 1e-5
