@@ -346,3 +346,29 @@ def test_host_kdk_steps_reuse_the_resident_acceleration():
     assert rel_err(vel, v_ref)[0] < 1e-5
     dp = (pos2 - p_ref + 0.5 * b.box_size) % b.box_size - 0.5 * b.box_size
     assert np.max(np.abs(dp)) < 1e-6 * b.box_size
+
+
+def test_host_kdk_step_after_another_call_steps_the_inputs():
+    """A device-resident step between two host-buffer steps changes the
+    resident state: handing back the earlier outputs must then be stepped from
+    those inputs (no speculation on the moved state)."""
+    t = treepm()
+    from treepm import ics
+    b = small_box(16, 100.0, 1.0, 85)
+    nm = 16
+    phys = ics.physics(b, nm, 0.1)
+    d, k1, k2 = t.drift_kick_factors(ics.OMEGA_M, ics.OMEGA_L, 1.0, 0.1, ics.time_between(0.1, 0.102))
+    host = t.TreePmSolver(nm, b.box_size, phys["r_split"], r_cut_factor=4.5)
+    pos = np.ascontiguousarray(b.positions())
+    vel = np.zeros_like(pos)
+    host.kdk_step_host(pos, vel, b.mass, k1, d, k2, phys["eps2"], phys["g"])
+    p1, v1 = pos.copy(), vel.copy()
+    host.kdk_step(k1, d, k2, phys["eps2"], phys["g"])  # the resident state moves on
+    ref = t.TreePmSolver(nm, b.box_size, phys["r_split"], r_cut_factor=4.5)
+    ref.set_particles(p1, b.mass, v1)
+    ref.kdk_step(k1, d, k2, phys["eps2"], phys["g"])
+    p_ref, v_ref, _ = ref.get_state(b.n)
+    host.kdk_step_host(pos, vel, b.mass, k1, d, k2, phys["eps2"], phys["g"])
+    assert rel_err(vel, v_ref)[0] < 1e-5
+    dp = (pos - p_ref + 0.5 * b.box_size) % b.box_size - 0.5 * b.box_size
+    assert np.max(np.abs(dp)) < 1e-6 * b.box_size
