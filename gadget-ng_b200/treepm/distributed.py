@@ -177,6 +177,7 @@ class DomainTreePm:
         self._L = self._h._lib
         self.gid = np.zeros(0, dtype=np.int64)  # global ids of the owned particles, owned order
         self.mass = np.zeros(0)
+        self._forces = None
         self.last_halo_count = 0
         self.last_halo_sent = 0
         self._stream = None
@@ -188,6 +189,7 @@ class DomainTreePm:
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
         self.mass = np.ascontiguousarray(mass, dtype=np.float64).reshape(-1).copy()
         self.solver.set_particles(pos, self.mass, vel)
+        self._forces = None  # (eps2, g) of the accelerations held, if any
         self.gid = (np.arange(pos.shape[0], dtype=np.int64) if gid is None else np.asarray(gid, dtype=np.int64))
 
     @property
@@ -282,6 +284,7 @@ class DomainTreePm:
             self.torch.cuda.synchronize(self.device)
             check(h, L.tpm_force_short_range(h, float(eps2)))
         check(h, L.tpm_force_end(h, float(g), float(kick)))
+        self._forces = (float(eps2), float(g))
 
     # ---- the solver calls ------------------------------------------------------
     def compute_forces(self, eps2: float, g: float) -> None:
@@ -305,8 +308,7 @@ class DomainTreePm:
         """leapfrog_cosmo_kdk_step over the decomposed domain: opening kick +
         drift (owned), halo exchange at the new positions, force evaluation
         with the closing kick fused into the gather."""
-        st = self.solver.stats()
-        if st["force_evaluations"] == 0:
+        if self._forces is None or self._forces[0] != float(eps2):
             self.compute_forces(eps2, g)
         check(self._h.h, self._L.tpm_kick_drift(self._h.h, float(kick_half), float(drift), float(g)))
         self.exchange_halos()
