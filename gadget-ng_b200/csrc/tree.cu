@@ -371,6 +371,9 @@ __global__ void k_depth_scatter(int64_t n_int, const uint8_t* __restrict__ o_dep
 // previous launch): mass and centre of mass summed over the children in
 // octant order, then the quadrupole by the parallel-axis theorem
 // (outer_traceless :197-207), all float64 in the reference's operation order.
+// QUAD: also the quadrupole tensors (the walk reads mass and centre of mass
+// only; the quadrupoles are made when the tree is exported).
+template <bool QUAD>
 __global__ void k_aggregate_level(const uint32_t* __restrict__ nodes, int64_t count, double scale,
                                   const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
                                   const uint32_t* __restrict__ qz, const double* __restrict__ pmass,
@@ -398,6 +401,13 @@ __global__ void k_aggregate_level(const uint32_t* __restrict__ nodes, int64_t co
     comx = ddiv(ax, mt);
     comy = ddiv(ay, mt);
     comz = ddiv(az, mt);
+  }
+  if (!QUAD) {
+    __stcg(&o_mass[P], mt);
+    __stcg(&o_com[3 * (int64_t)P], comx);
+    __stcg(&o_com[3 * (int64_t)P + 1], comy);
+    __stcg(&o_com[3 * (int64_t)P + 2], comz);
+    return;
   }
   // pass 2: the children are read again (cache hits) rather than held in registers
   double qd[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -729,7 +739,8 @@ void launch_octree_links(int64_t n, int64_t n_int, TreeBuffers& t, void* scan_sc
 // Level by level from the deepest internal nodes to the root: each launch
 // finishes one depth, so every node reads finished children without atomics
 // or fences.  One host synchronisation brings the per-depth counts back.
-void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, TreeBuffers& t, cudaStream_t s) {
+void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, TreeBuffers& t, cudaStream_t s,
+                      bool with_quad) {
   (void)n;
   if (n_int <= 0) return;
   uint32_t* hist = t.depth_tab;
@@ -750,9 +761,14 @@ void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, 
   if (offset[DEPTH_BINS] != n_int) throw Error(2, "octree depth buckets do not add up to the node count");
   for (int d = DEPTH_BINS - 1; d >= 0; --d) {
     if (counts[d] == 0) continue;
-    k_aggregate_level<<<grid_for(counts[d], 128, 1ll << 30), 128, 0, s>>>(
-        t.o_cnt + offset[d], counts[d], box / TWO32, p.qx, p.qy, p.qz, p.mass, t.o_slots, t.o_mass, t.o_com,
-        t.o_quad);
+    if (with_quad)
+      k_aggregate_level<true><<<grid_for(counts[d], 128, 1ll << 30), 128, 0, s>>>(
+          t.o_cnt + offset[d], counts[d], box / TWO32, p.qx, p.qy, p.qz, p.mass, t.o_slots, t.o_mass, t.o_com,
+          t.o_quad);
+    else
+      k_aggregate_level<false><<<grid_for(counts[d], 128, 1ll << 30), 128, 0, s>>>(
+          t.o_cnt + offset[d], counts[d], box / TWO32, p.qx, p.qy, p.qz, p.mass, t.o_slots, t.o_mass, t.o_com,
+          t.o_quad);
     TPM_LAUNCH_CHECK();
   }
   k_walk_nodes<<<grid_for(n_int, 256, 1ll << 30), 256, 0, s>>>(n_int, TWO32 / box, t.o_mass, t.o_com, t.o_walk);

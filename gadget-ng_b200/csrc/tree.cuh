@@ -107,7 +107,10 @@ void launch_permute(const Particles& src, const Particles& dst, int64_t n, const
 void launch_karras(int64_t n, TreeBuffers& t, cudaStream_t s);
 void launch_octree_nodes(int64_t n, TreeBuffers& t, cudaStream_t s);
 void launch_octree_links(int64_t n, int64_t n_int, TreeBuffers& t, void* scan_scratch, cudaStream_t s);
-void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, TreeBuffers& t, cudaStream_t s);
+// Level-synchronous moments, deepest level first: mass and centre of mass, and
+// with_quad the quadrupole tensors too.
+void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, TreeBuffers& t, cudaStream_t s,
+                      bool with_quad = false);
 void launch_walk_records(const Particles& p, int64_t n, int64_t n_int, double thr, TreeBuffers& t, cudaStream_t s);
 void launch_groups(int64_t n, int64_t n_int, int group_max, TreeBuffers& t, void* scan_scratch, cudaStream_t s);
 void launch_hilbert_keys(const Particles& p, int64_t n, double box, const TreeParams* prm, uint64_t* keys,

@@ -278,6 +278,7 @@ struct tpm_handle {
   };
   std::vector<Alloc> allocs;
   bool tree_valid = false;
+  bool quad_valid = false;  // the octree's quadrupoles (made for tpm_export_tree only)
   // domain decomposition scratch (sized by the particle capacity)
   uint8_t* owned_mask = nullptr;
   uint64_t* dom_flags = nullptr;
@@ -572,6 +573,7 @@ void fe_tree_walk(tpm_handle* h, double eps2, const uint8_t* only) {
       launch_octree_nodes(n, T, s);
       launch_octree_links(n, h->n_int, T, h->scan_scratch, s);
       launch_aggregate(h->P[h->cur], n, h->n_int, box, T, s);
+      h->quad_valid = false;
       launch_walk_records(h->P[h->cur], n, h->n_int, h->thr, T, s);
       launch_groups(n, h->n_int, walk_targets_per_warp(), T, h->scan_scratch, s);
       TPM_CUDA(cudaMemcpyAsync(sc, T.scalars, sizeof(sc), cudaMemcpyDeviceToHost, s));
@@ -2001,6 +2003,10 @@ int64_t tpm_export_tree(tpm_handle* h, int64_t cap, int32_t* depth, double* mass
     if (!depth || !mass || !com || !quad || !particle || !path_hi || !path_lo)
       throw Error(TPM_ERR_INVALID_ARGUMENT, "null export array");
     cudaStream_t s = h->stream;
+    if (!h->quad_valid && ni > 0) {  // the force evaluation made mass and centre of mass only
+      launch_aggregate(h->P[h->cur], n, ni, h->cfg.box_size, h->T, s, true);
+      h->quad_valid = true;
+    }
     int32_t* dd;
     double *dm, *dc, *dq;
     int64_t* dp;
