@@ -79,22 +79,26 @@ __global__ void k_tree_keys(const uint32_t* __restrict__ qx, const uint32_t* __r
   if (i >= n) return;
   const double x = decode(qx[i], scale), y = decode(qy[i], scale), z = decode(qz[i], scale);
   double cx = prm->center[0], cy = prm->center[1], cz = prm->center[2], h = prm->half;
-  uint64_t hi = 0, lo = 0;
-#pragma unroll 1
-  for (int l = 1; l <= KEY_LEVELS; ++l) {
-    const double q = dmul(h, 0.5);
-    const bool ox = x >= cx, oy = y >= cy, oz = z >= cz;
-    const uint64_t digit = (uint64_t)ox | ((uint64_t)oy << 1) | ((uint64_t)oz << 2);
-    // child_center: centre + off, off = (0.0 +/- q) per axis
-    cx = dadd(cx, ox ? q : -q);
-    cy = dadd(cy, oy ? q : -q);
-    cz = dadd(cz, oz ? q : -q);
-    h = q;
-    if (l <= 21) hi |= digit << (63 - 3 * l);
-    else lo |= digit << (63 - 3 * (l - 21));
+  // levels 1..21 into the high word, 22..42 into the low word; the levels are
+  // unrolled so the digit shifts are constants
+  uint64_t key[2] = {0, 0};
+#pragma unroll
+  for (int w = 0; w < 2; ++w) {
+#pragma unroll
+    for (int l = 1; l <= KEY_LEVELS / 2; ++l) {
+      const double q = dmul(h, 0.5);
+      const bool ox = x >= cx, oy = y >= cy, oz = z >= cz;
+      const uint64_t digit = (uint64_t)ox | ((uint64_t)oy << 1) | ((uint64_t)oz << 2);
+      // child_center: centre + off, off = (0.0 +/- q) per axis
+      cx = dadd(cx, ox ? q : -q);
+      cy = dadd(cy, oy ? q : -q);
+      cz = dadd(cz, oz ? q : -q);
+      h = q;
+      key[w] |= digit << (63 - 3 * l);
+    }
   }
-  key_hi[i] = hi;
-  key_lo[i] = lo;
+  key_hi[i] = key[0];
+  key_lo[i] = key[1];
   perm[i] = (uint32_t)i;
 }
 
