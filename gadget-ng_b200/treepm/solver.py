@@ -118,6 +118,21 @@ class TreePmSolver:
         check(self._h.h, rc)
         return out
 
+    def accelerations_with_costs(self, global_positions, global_masses, eps2: float, g: float, global_indices,
+                                 out=None):
+        """accelerations_with_costs (gravity.rs:36-55): the accelerations and
+        one uint64 work figure per index, the short-range interactions its walk
+        made (leaf pairs + monopoles, the per-target counters of
+        tpm_get_interaction_counts).  Empty costs, as the trait's default, when
+        nothing was walked (no indices, plain PM)."""
+        out = self.accelerations_for_indices(global_positions, global_masses, eps2, g, global_indices, out)
+        idx = np.ascontiguousarray(global_indices, dtype=np.int64).reshape(-1)
+        n = np.asarray(global_positions).reshape(-1, 3).shape[0]
+        if idx.size == 0 or self._h.cfg.flags & _lib.FLAG_PM_ONLY or n < 2:
+            return out, np.zeros(0, dtype=np.uint64)
+        counts = self.interaction_counts(n)
+        return out, counts[idx].sum(axis=1).astype(np.uint64)
+
     # ---- device-resident state (fused integrator path) --------------------
     def set_particles(self, pos, mass, vel=None):
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)

@@ -372,3 +372,25 @@ def test_host_kdk_step_after_another_call_steps_the_inputs():
     assert rel_err(vel, v_ref)[0] < 1e-5
     dp = (pos - p_ref + 0.5 * b.box_size) % b.box_size - 0.5 * b.box_size
     assert np.max(np.abs(dp)) < 1e-6 * b.box_size
+
+
+def test_accelerations_with_costs():
+    """accelerations_with_costs: the accelerations of accelerations_for_indices
+    and, per index, the interactions of its walk (the oracle's counts)."""
+    t = treepm()
+    b = clustered_small(16, 100.0, 57)
+    pos = b.positions()
+    nm = 32
+    eps = b.box_size / 16 / 30
+    rs = 1.25 * b.box_size / nm
+    s = t.TreePmSolver(nm, b.box_size, rs, r_cut_factor=4.5)
+    idx = np.arange(b.n)[::7][::-1].copy()
+    out, costs = s.accelerations_with_costs(pos, b.mass, eps * eps, 1.0, idx)
+    # (two evaluations differ in the last bits: the deposit sums with float32 atomics)
+    np.testing.assert_allclose(out, s.accelerations_for_indices(pos, b.mass, eps * eps, 1.0, idx), rtol=1e-5,
+                               atol=1e-6 * np.abs(out).max())
+    ref = oracle().treepm(pos, b.mass, eps * eps, 1.0, nm, b.box_size, rs, 4.5, counts=True)
+    np.testing.assert_array_equal(costs, ref["counts"][idx].sum(axis=1).astype(np.uint64))
+    assert costs.dtype == np.uint64 and costs.shape == idx.shape
+    _, none = s.accelerations_with_costs(pos, b.mass, eps * eps, 1.0, np.zeros(0, dtype=np.int64))
+    assert none.size == 0
