@@ -205,3 +205,35 @@ def test_cell_halo_rule_matches_oracle(case):
         assert out["n_halo"] == halos[r].size
         np.testing.assert_array_equal(out["counts"], cnt[g])
         assert _rel(out["acc"], acc[g]) < 1e-5
+
+
+def test_domain_entry_points_report_misuse():
+    """The staged force calls out of order return TPM_ERR_NOT_READY; a halo
+    send buffer too small returns TPM_ERR_INVALID_ARGUMENT with the counts
+    filled and nothing written; bad rank arguments are refused."""
+    import ctypes as C
+    import treepm
+    from treepm import ics
+    b = ics.clustered_box(8, BOX, 0.3, 3, min_halo=20, max_halo=60, r_min=0.3, r_max=1.5, seed=41)
+    pos = b.positions()
+    s = treepm.TreePmSolver(NM, BOX, 1.25 * BOX / NM, r_cut_factor=RCF)
+    s.set_particles(pos, b.mass)
+    L, h = s._h._lib, s._h.h
+    assert L.tpm_force_short_range(h, 1e-4) == 7
+    assert L.tpm_force_end(h, 1.0, 0.0) == 7
+    assert L.tpm_force_begin(h) == 0
+    assert L.tpm_force_end(h, 1.0, 0.0) == 7
+    assert L.tpm_force_short_range(h, 1e-4) == 0
+    assert L.tpm_force_end(h, 1.0, 0.0) == 0
+    # rank 1 owns the whole box: every particle within r_cut of it goes there
+    aabbs = np.ascontiguousarray(np.array([[np.inf, -np.inf] * 3, [0.0, BOX] * 3]).reshape(-1))
+    counts = np.zeros(2, dtype=np.int64)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert L.tpm_halo_select(h, p(aabbs), 2, 0, 10.0, p(counts), None, 0) == 0
+    assert counts[0] == 0 and counts[1] == b.n
+    import torch
+    buf = torch.zeros(24 * 4, dtype=torch.uint8, device="cuda")
+    assert L.tpm_halo_select(h, p(aabbs), 2, 0, 10.0, p(counts), C.c_void_p(buf.data_ptr()), 4) == 1
+    assert counts[1] == b.n and int(buf.sum()) == 0
+    assert L.tpm_halo_select(h, p(aabbs), 2, 2, 10.0, p(counts), None, 0) == 1   # rank out of range
+    assert L.tpm_halo_select(h, p(aabbs), 65, 0, 10.0, p(counts), None, 0) == 1  # too many ranks
