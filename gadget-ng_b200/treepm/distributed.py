@@ -36,9 +36,6 @@ from . import _lib
 from ._lib import check
 from .solver import TreePmSolver, _ptr
 
-F64_EPSILON = float(np.finfo(np.float64).eps)
-
-
 class _DeviceArray:
     """A library-owned device buffer seen by torch without a copy
     (__cuda_array_interface__)."""
