@@ -175,7 +175,8 @@ def _exchange_rank(rank, world, port, parts, width, q):
         got = recv[:int(rc.sum()) * 24].view(np.float64).reshape(-1, 3)
         t = torch.full((5,), float(rank + 1))
         ex.allreduce_sum_(t)
-        q.put((rank, got, aabbs, t.numpy()))
+        words = ex.allgather_u32(np.array([0xFFFFFFFF - rank, rank, 1 << 31], dtype=np.uint32))
+        q.put((rank, got, aabbs, t.numpy(), words))
     finally:
         dist.destroy_process_group()
 
@@ -183,7 +184,7 @@ def _exchange_rank(rank, world, port, parts, width, q):
 def test_exchange_layer_two_gloo_ranks():
     """exchange_halos_3d_periodic over the driver's collectives (allgather,
     count all-to-all, alltoallv of records, all-reduce) equals the oracle's
-    all-in-one exchange."""
+    all-in-one exchange; the uint32 allgather of the cell rule keeps every bit."""
     import torch.multiprocessing as mp
     pos, _ = _box(8, 11)
     owner, _, _ = _sfc_owner(pos, 2)
@@ -197,14 +198,15 @@ def test_exchange_layer_two_gloo_ranks():
         p.start()
     res = dict()
     for _ in range(2):
-        r, got, aabbs, t = q.get(timeout=120)
-        res[r] = (got, aabbs, t)
+        r, got, aabbs, t, words = q.get(timeout=120)
+        res[r] = (got, aabbs, t, words)
     for p in procs:
         p.join(60)
         assert p.exitcode == 0
     want = dom().exchange_halos(parts, width, 1.0)
     for r in range(2):
-        got, aabbs, t = res[r]
+        got, aabbs, t, words = res[r]
+        assert words.dtype == np.uint32 and words.tolist() == [[0xFFFFFFFF, 0, 1 << 31], [0xFFFFFFFE, 1, 1 << 31]]
         exp = np.concatenate([parts[s][i] for s, i in want[r]]) if want[r] else np.zeros((0, 3))
         np.testing.assert_array_equal(got, exp)
         np.testing.assert_array_equal(aabbs, np.stack([dom().compute_aabb_3d(p) for p in parts]))
