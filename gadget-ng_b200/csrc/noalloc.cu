@@ -26,9 +26,10 @@ namespace {
 constexpr int64_t NOALLOC_MAX = TPM_NOALLOC_MAX_PARTICLES;
 // bounding box words + TreeParams, then the radix-sort scratch
 constexpr size_t NOALLOC_PARAMS_BYTES = 512;
-constexpr size_t NOALLOC_SORT_BYTES =
-    (size_t)NOALLOC_MAX * (sizeof(uint64_t) + sizeof(uint32_t)) +
-    2 * (size_t)((NOALLOC_MAX + 4095) / 4096) * 256 * sizeof(uint32_t) + 8 * 256 * sizeof(uint32_t) + 2048;
+// the sort's own sizing rule at the largest accepted n, so every n <= NOALLOC_MAX fits
+constexpr size_t NOALLOC_SORT_BYTES = tpm::radix_sort_scratch_bytes(NOALLOC_MAX);
+static_assert(NOALLOC_SORT_BYTES >= tpm::radix_sort_scratch_bytes(NOALLOC_MAX - 1),
+              "scratch sizing must grow with n");
 constexpr size_t NOALLOC_BYTES = NOALLOC_PARAMS_BYTES + NOALLOC_SORT_BYTES;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];

@@ -13,9 +13,6 @@ namespace tpm {
 
 namespace {
 
-constexpr int SORT_BLOCK = 256;
-constexpr int SORT_ITEMS = 8;  // 8 keys per thread: 2048-key tiles (sort 2.84 -> 2.30 ms at 256^3 against 16)
-constexpr int SORT_TILE = SORT_BLOCK * SORT_ITEMS;
 constexpr int SORT_WARPS = SORT_BLOCK / 32;
 
 __global__ void k_hist8(const uint64_t* __restrict__ keys, int64_t n, uint32_t* __restrict__ hist) {
@@ -185,13 +182,6 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_downsweep(const uint64_t* __rest
 }
 
 }  // namespace
-
-size_t radix_sort_scratch_bytes(int64_t n) {
-  int64_t ntiles = (n + SORT_TILE - 1) / SORT_TILE;
-  if (ntiles < 1) ntiles = 1;
-  return (size_t)n * (sizeof(uint64_t) + sizeof(uint32_t)) + 2 * (size_t)ntiles * 256 * sizeof(uint32_t) +
-         8 * 256 * sizeof(uint32_t) + 1024;
-}
 
 void radix_sort_u64(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, void* scratch, size_t scratch_bytes,
                     cudaStream_t s) {

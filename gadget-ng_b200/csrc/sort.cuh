@@ -5,9 +5,17 @@
 #include <stdint.h>
 
 namespace tpm {
+// Keys per tile of one digit pass: 256 threads x 8 keys.
+constexpr int SORT_BLOCK = 256;
+constexpr int SORT_ITEMS = 8;  // 8 keys per thread: 2048-key tiles (sort 2.84 -> 2.30 ms at 256^3 against 16)
+constexpr int SORT_TILE = SORT_BLOCK * SORT_ITEMS;
 // Scratch bytes radix_sort_u64 needs for n pairs (ping-pong copies, per-tile
-// digit counts and offsets, the 8x256 histogram).
-size_t radix_sort_scratch_bytes(int64_t n);
+// digit counts and offsets, the 8x256 histogram, 256-byte alignment of each).
+constexpr size_t radix_sort_scratch_bytes(int64_t n) {
+  return (size_t)n * (sizeof(uint64_t) + sizeof(uint32_t)) +
+         2 * (size_t)(n > SORT_TILE ? (n + SORT_TILE - 1) / SORT_TILE : 1) * 256 * sizeof(uint32_t) +
+         8 * 256 * sizeof(uint32_t) + 1024;
+}
 // Stable ascending sort of keys[0..n) (low key_bits bits) carrying vals.
 // Synchronises the stream once (to skip constant-digit passes).
 void radix_sort_u64(uint64_t* keys, uint32_t* vals, int64_t n, int key_bits, void* scratch, size_t scratch_bytes,

@@ -26,6 +26,12 @@ constexpr double F64_EPSILON = 2.220446049250313e-16;
 // ---------------------------------------------------------------------------
 // bounding box and root cube
 // ---------------------------------------------------------------------------
+// Seeds the min/max words on the stream (no host copy, so nothing pageable is
+// read and the sequence stays stream-ordered).
+__global__ void k_bbox_init(uint32_t* __restrict__ out) {
+  if (threadIdx.x < 6) out[threadIdx.x] = threadIdx.x < 3 ? 0xFFFFFFFFu : 0u;
+}
+
 __global__ void k_bbox(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
                        const uint32_t* __restrict__ qz, int64_t n, uint32_t* __restrict__ out) {
   uint32_t mn[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx[3] = {0u, 0u, 0u};
@@ -681,8 +687,8 @@ __global__ void k_export_paths(int64_t n, int64_t n_int, const uint8_t* __restri
 // launchers
 // ===========================================================================
 void launch_bbox_root(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s) {
-  const uint32_t init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
-  TPM_CUDA(cudaMemcpyAsync(t.bbox, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  k_bbox_init<<<1, 32, 0, s>>>(t.bbox);
+  TPM_LAUNCH_CHECK();
   k_bbox<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(p.qx, p.qy, p.qz, n, t.bbox);
   TPM_LAUNCH_CHECK();
   k_root<<<1, 32, 0, s>>>(t.bbox, box / TWO32, t.params);

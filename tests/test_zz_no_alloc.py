@@ -57,6 +57,21 @@ def test_noalloc_sort_matches_allocating_entry_point_twice():
         assert np.array_equal(order, ref_order)
 
 
+def test_noalloc_sort_at_its_largest_sizes():
+    """n = the fixed maximum and one below it: the scratch holds the sort's
+    per-tile counts at every accepted size, so both sort bit-exactly."""
+    from treepm import _lib, ics
+    full = ics.lattice_box(64, 100.0, 1.0, seed=94)
+    assert full.n == _lib.NOALLOC_MAX_PARTICLES
+    less = ics.Box(full.q[:-1].copy(), full.box_size, full.mass[:-1].copy(), "lattice-1")
+    for box in (full, less, full):
+        rc, keys, order = _noalloc(box.q, box.box_size)
+        assert rc == 0
+        ref_keys, ref_order = _reference(box)
+        assert np.array_equal(keys, ref_keys)
+        assert np.array_equal(order, ref_order)
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     from treepm import _lib, ics
     box = ics.lattice_box(8, 100.0, 1.0, seed=93)
