@@ -5,14 +5,17 @@ of the reference + the periodic wrap): opening half kick, drift, one TreePM
 force evaluation (keys, sort, octree, short-range walk, PM), closing half kick.
 The fused step reuses the previous step's closing acceleration for its opening
 kick; the reference evaluates the force twice per step, and the JSON line also
-reports the per-force-evaluation rate.
+reports the per-force-evaluation rate.  The workload is a trajectory of 10 KDK
+steps with one global dt from a = 0.1 to 0.12; timed steps are steps of that
+trajectory, and an untimed pass over it reports per-step diagnostics and FP64
+Ewald errors.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload clustered256]
   python bench.py --impl reference ...   # the CPU restatement of the reference
 
-Multi-GPU: independent replicas, one per rank (the force path has no
-exchange step on one box), so value = the particle-updates of all ranks / the
-slowest rank's time, and "scaling" is "weak".
+Multi-GPU (N > 1): the domain-decomposed solver (SFC domains, periodic halos,
+density all-reduce) on one box split over the ranks, "scaling": "strong";
+``--replicas`` runs N independent copies instead ("scaling": "weak").
 """
 from __future__ import annotations
 
@@ -44,6 +47,24 @@ WORKLOADS = {
     "treepm128_mesh256": ("treepm_box_128", 256, 0.1, 0.12),
 }
 FLOP_PER_INTERACTION = 37  # FMA = 2, MUFU = 1: the pair-kernel convention of the cost model
+TRAJ_STEPS = 10  # KDK steps from a_start to a_end, one global dt
+
+
+def trajectory(a0, a1, G, steps=TRAJ_STEPS, total=None):
+    """(drift, kick_half, kick_half2, coupling G·a³) of each of `steps` KDK
+    steps with one global dt from a0 to a1 (continued with the same dt to
+    `total` steps when given), and the scale factor after each step
+    (a_of[i] = a after i steps)."""
+    import treepm
+    from treepm import ics
+    dt = ics.time_between(a0, a1) / steps
+    a, factors, a_of = a0, [], [a0]
+    for _ in range(total or steps):
+        d, k1, k2 = treepm.drift_kick_factors(ics.OMEGA_M, ics.OMEGA_L, ics.H0_INTERNAL, a, dt)
+        factors.append((d, k1, k2, G * a ** 3))
+        a = treepm.advance_a(ics.OMEGA_M, ics.OMEGA_L, ics.H0_INTERNAL, a, dt)
+        a_of.append(a)
+    return factors, a_of
 
 
 def env_rank():
@@ -137,9 +158,9 @@ def measured_peaks():
         return {}
 
 
-# DRAM bytes (read + write) of one k_walk launch, from single-pass ncu captures of
-# dram__bytes_read.sum / dram__bytes_write.sum (profiles/k_walk_dram_clustered256.md,
-# profiles/k_walk_treepm128.md).
+# DRAM bytes (read + write) of one k_walk launch on these workloads, from
+# single-pass ncu captures of dram__bytes_read.sum + dram__bytes_write.sum made
+# outside the bench (ncu cannot run inside a timed bench); reported with that label.
 WALK_DRAM_BYTES = {"clustered256_L200": 963312384 + 368289792, "treepm128_L100": 144405760 + 69206272}
 
 
@@ -167,21 +188,51 @@ def stage_rooflines(stage_ms, n, mesh):
     return out
 
 
+def sample_targets(n, n_targets, blocks=64, seed=12345):
+    """Walk targets of the CPU sample: one run of consecutive particle indices
+    at a seeded offset in each of `blocks` equal strata of the index range.
+    The workloads store particles in spatial order (lattice part, then the
+    halos), so the strata cover both in proportion, and a run keeps the cache
+    locality of the full walk (neighbouring targets share tree nodes);
+    scattered single targets walk slower per target than the full evaluation."""
+    n_targets = min(n_targets, n)
+    blocks = max(1, min(blocks, n_targets))
+    blk = n_targets // blocks
+    stratum = n // blocks
+    rng = np.random.default_rng(seed)
+    starts = np.arange(blocks) * stratum + rng.integers(0, stratum - blk + 1, blocks)
+    return (starts[:, None] + np.arange(blk)[None, :]).ravel().astype(np.int64)
+
+
 def cpu_sample(box, mesh, phys, n_targets, threads):
     """The oracle restatement on a bounded sample: full PM + full tree build +
-    the walk of n_targets seeded targets, extrapolated to all particles."""
+    the walk of n_targets seeded targets (runs of consecutive particles),
+    extrapolated to all particles."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
     oracle.build()
     oracle.set_threads(threads)
     pos = box.positions()
-    rng = np.random.default_rng(12345)
-    tg = np.sort(rng.choice(box.n, min(n_targets, box.n), replace=False))
+    tg = sample_targets(box.n, n_targets)
     r = oracle.treepm(pos, box.mass, phys["eps2"], phys["g"], mesh, box.box_size, phys["r_split"],
                       phys["r_cut_factor"], targets=tg)
     t_pm, t_build, t_walk, _ = (float(x) for x in r["times"])
     t_force = t_pm + t_build + t_walk * box.n / len(tg)
     return t_force, dict(pm_s=t_pm, build_s=t_build, walk_s=t_walk, targets=int(len(tg)), threads=threads)
+
+
+def cpu_full(box, mesh, phys, threads):
+    """One complete force evaluation by the oracle restatement: every
+    particle's walk, nothing extrapolated.  Returns seconds and stage times."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    oracle.build()
+    oracle.set_threads(threads)
+    pos = box.positions()
+    r = oracle.treepm(pos, box.mass, phys["eps2"], phys["g"], mesh, box.box_size, phys["r_split"],
+                      phys["r_cut_factor"], targets=np.arange(box.n, dtype=np.int64))
+    t_pm, t_build, t_walk, _ = (float(x) for x in r["times"])
+    return t_pm + t_build + t_walk, dict(pm_s=t_pm, build_s=t_build, walk_s=t_walk)
 
 
 def run_reference(args):
@@ -199,6 +250,12 @@ def run_reference(args):
             times.append(2.0 * t_force)  # the reference evaluates the force twice per KDK step
     step_s = float(np.mean(times))
     value = box.n / step_s
+    full = None
+    if not args.no_cpu_full:
+        t_full, finfo = cpu_full(box, mesh, phys, threads)
+        full = {"seconds": t_full, "extrapolated_seconds": step_s / 2.0, "ratio_full_over_extrapolated":
+                t_full / (step_s / 2.0), **finfo,
+                "note": "one force evaluation with every particle's walk (no extrapolation), after the timed steps"}
     line = {
         "impl": "reference", "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
@@ -208,8 +265,10 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": "particle-updates/s", "cores": threads, "kind": "port",
                          "sample": (f"oracle restatement (C++/OpenMP, FP64) of the reference TreePM: full CIC+FFT PM "
                                     f"and full insertion-octree build over {box.n} particles, periodic walk of "
-                                    f"{info['targets']} seeded targets extrapolated to all; 2 force evaluations "
+                                    f"{info['targets']} seeded targets (one run of consecutive particles in each of 64 strata) extrapolated "
+                                    f"to all; 2 force evaluations "
                                     f"per KDK step as leapfrog.rs:79,86")},
+        "full_force_evaluation": full,
         "e2e": {"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -230,66 +289,85 @@ def fp32_peak_tflops(lib_solver):
 
 def accurate_mode_report(box, mesh, phys, pos, g, targets, ref, device, reps=3):
     """Speed and Ewald error of the extension mode (complete split kernel,
-    opening angle 0.5, CIC deconvolution) on the bench's final state."""
+    CIC deconvolution) on the bench's final state, with the opening angle 0.5
+    and with the relative opening criterion at the reference's default
+    tolerance (err_tol_force_acc = 0.005)."""
     import treepm
     from treepm import accuracy
-    s = treepm.TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"], accurate=True,
-                            theta=0.5, deconvolve_cic=True, device=device)
-    s.set_particles(pos, box.mass)
-    for _ in range(2):
-        s.compute_forces(phys["eps2"], g)
-    ms, inter = [], []
-    for _ in range(reps):
-        s.compute_forces(phys["eps2"], g)
-        st = s.stats()
-        ms.append(st["ms_total"])
-        inter.append(st["leaf_pairs"] + st["monopoles"])
-    _, _, acc = s.get_state(box.n, pos=False, vel=False)
-    rms, p99 = accuracy.relative_errors(acc[targets], ref)
-    s.close()
-    m = float(np.mean(ms))
-    return {"flags": "accurate | deconvolve_cic", "theta": 0.5, "ms_per_force_evaluation": m,
-            "particle_updates_per_s": box.n / (m * 1e-3),
-            "interactions_per_particle": float(np.mean(inter)) / box.n,
-            "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}}
+
+    def one(**crit):
+        s = treepm.TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"],
+                                accurate=True, deconvolve_cic=True, device=device, **crit)
+        s.set_particles(pos, box.mass)
+        for _ in range(2):
+            s.compute_forces(phys["eps2"], g)
+        ms, inter = [], []
+        for _ in range(reps):
+            s.compute_forces(phys["eps2"], g)
+            st = s.stats()
+            ms.append(st["ms_total"])
+            inter.append(st["leaf_pairs"] + st["monopoles"])
+        _, _, acc = s.get_state(box.n, pos=False, vel=False)
+        rms, p99 = accuracy.relative_errors(acc[targets], ref)
+        s.close()
+        m = float(np.mean(ms))
+        return {"ms_per_force_evaluation": m, "particle_updates_per_s": box.n / (m * 1e-3),
+                "interactions_per_particle": float(np.mean(inter)) / box.n,
+                "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}}
+
+    out = {"flags": "accurate | deconvolve_cic", "theta": 0.5}
+    out.update(one(theta=0.5))
+    out["relative_criterion"] = dict(err_tol_force_acc=0.005, **one(opening_criterion=1, err_tol_force_acc=0.005))
+    return out
 
 
-def learned_mode_report(box, mesh, phys, pos, g, targets, ref, device, plain_ms, reps=3):
+def learned_mode_report(box, mesh, phys, pos, g, targets, ref, device, plain_ms, reps=3, path=None, deltas=None):
     """Speed and Ewald error of the learned short range (network outside
-    dense cells, accurate walk inside them) on the bench's final state."""
+    dense cells, accurate walk inside them) on the bench's final state; with
+    `deltas`, once per overdensity threshold of the fallback (cells above it
+    keep the walk)."""
     import treepm
     from treepm import accuracy, learned
-    path = os.path.join(REPO, "gadget-ng_b200", "treepm", "weights", "learned_sr.npz")
+    path = path or os.path.join(REPO, "gadget-ng_b200", "treepm", "weights", "learned_sr.npz")
     if not os.path.exists(path):
         return {"unavailable": "no trained weights file"}
     net = learned.Network.load(path, device)
-    # the network's error dominates this mode, so the fallback walk takes the
-    # widest opening angle the accurate walk allows
-    s = treepm.TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"], accurate=True,
-                            theta=LEARNED_THETA, deconvolve_cic=True, learned=True, device=device)
-    s.set_learned(net)
-    s.set_particles(pos, box.mass)
-    for _ in range(2):
-        s.compute_forces(phys["eps2"], g)
-    sts = []
-    for _ in range(reps):
-        s.compute_forces(phys["eps2"], g)
-        sts.append(s.stats())
-    _, _, acc = s.get_state(box.n, pos=False, vel=False)
-    rms, p99 = accuracy.relative_errors(acc[targets], ref)
-    s.close()
+    sh, sc, o, d0 = net.scales()
+    runs = []
+    for dmax in (deltas or [d0]):
+        net.set_scales(sh, sc, o, dmax)
+        # the network's error dominates this mode, so the fallback walk takes
+        # the widest opening angle the accurate walk allows
+        s = treepm.TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"],
+                                accurate=True, theta=LEARNED_THETA, deconvolve_cic=True, learned=True, device=device)
+        s.set_learned(net)
+        s.set_particles(pos, box.mass)
+        for _ in range(2):
+            s.compute_forces(phys["eps2"], g)
+        sts = []
+        for _ in range(reps):
+            s.compute_forces(phys["eps2"], g)
+            sts.append(s.stats())
+        _, _, acc = s.get_state(box.n, pos=False, vel=False)
+        rms, p99 = accuracy.relative_errors(acc[targets], ref)
+        s.close()
+        m = float(np.mean([st["ms_total"] for st in sts]))
+        st = sts[-1]
+        runs.append({"delta_max": float(dmax), "ms_per_force_evaluation": m,
+                     "particle_updates_per_s": box.n / (m * 1e-3), "speedup_vs_plain_step": plain_ms / m,
+                     "network_fraction": st["learned_particles"] / box.n, "walk_groups": st["walk_groups"],
+                     "groups": st["n_groups"],
+                     "stage_ms": {k: float(np.mean([x[k] for x in sts])) for k in
+                                  ("ms_bbox_keys", "ms_sort", "ms_build", "ms_pm", "ms_learned", "ms_walk",
+                                   "ms_gather_kick")},
+                     "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}})
     net.close()
-    m = float(np.mean([st["ms_total"] for st in sts]))
-    st = sts[-1]
-    return {"flags": "accurate | deconvolve_cic | learned", "theta": LEARNED_THETA,
-            "weights": os.path.relpath(path, REPO),
-            "ms_per_force_evaluation": m, "particle_updates_per_s": box.n / (m * 1e-3),
-            "speedup_vs_plain_step": plain_ms / m,
-            "network_fraction": st["learned_particles"] / box.n, "walk_groups": st["walk_groups"],
-            "groups": st["n_groups"],
-            "stage_ms": {k: float(np.mean([x[k] for x in sts])) for k in
-                         ("ms_bbox_keys", "ms_sort", "ms_build", "ms_pm", "ms_learned", "ms_walk", "ms_gather_kick")},
-            "force_error_vs_ewald": {"rms": rms, "p99": p99, "targets": int(len(targets))}}
+    out = {"flags": "accurate | deconvolve_cic | learned", "theta": LEARNED_THETA,
+           "weights": os.path.relpath(os.path.abspath(path), REPO)}
+    out.update(runs[0])
+    if len(runs) > 1:
+        out["delta_max_sweep"] = runs
+    return out
 
 
 IC_CFG = dict(transfer="eisenstein_hu", sigma8=0.8, omega_m=0.315, omega_lambda=0.685, omega_b=0.049, h=0.674,
@@ -423,56 +501,103 @@ def run_b200(args):
     solver = treepm.TreePmSolver(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"],
                                  device=local)
     stream = torch.cuda.ExternalStream(solver.stream, device=torch.device("cuda", local))
-    # 10 steps from a0 to a1; the factors are float64 host integrals
-    dt = ics.time_between(a0, a1) / 10.0
-    a = a0
-    factors = []
-    for _ in range(args.warmup + args.steps + 1):
-        d, k1, k2 = treepm.drift_kick_factors(ics.OMEGA_M, ics.OMEGA_L, ics.H0_INTERNAL, a, dt)
-        factors.append((d, k1, k2, phys["G"] * a ** 3))
-        a = treepm.advance_a(ics.OMEGA_M, ics.OMEGA_L, ics.H0_INTERNAL, a, dt)
+    # the workload's trajectory: TRAJ_STEPS KDK steps with one global dt from
+    # a0 to a1; the factors are float64 host integrals
+    factors, a_of = trajectory(a0, a1, phys["G"])
 
-    # ---- device-resident loop (value) -----------------------------------
-    solver.set_particles_fixed(box.q, box.mass)
-    for i in range(args.warmup):
-        d, k1, k2, g = factors[i]
-        solver.kdk_step(k1, d, k2, phys["eps2"], g)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    walk_ms, stats = [], []
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        ev0.record(stream)
-        for i in range(args.steps):
-            d, k1, k2, g = factors[args.warmup + i]
-            solver.kdk_step(k1, d, k2, phys["eps2"], g)
-            st = solver.stats()
-            stats.append(st)
-            walk_ms.append(st["ms_walk"])
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    dev_ms = max_over_ranks(ev0.elapsed_time(ev1), "cuda")
-    ms_per_step = dev_ms / args.steps
-    value = whole_job_rate(n, args.steps, dev_ms * 1e-3, world)
+    def restart():
+        """Back to the initial state (zero momenta) with its forces evaluated,
+        so every timed step is one steady-state KDK step."""
+        solver.set_particles_fixed(box.q, box.mass)
+        solver.compute_forces(phys["eps2"], factors[0][3])
 
-    # ---- force error of the last evaluation against FP64 Ewald ------------
+    # ---- the trajectory once, untimed: per-step diagnostics (kinetic energy,
+    # momentum and angular momentum drift) and per-step FP64 Ewald errors
+    from treepm import accuracy, diagnostics
+    traj_rep = None
+    tg = accuracy.seeded_targets(n, args.ewald_targets)
     ewald = accurate = learned_rep = None
+    p_now = ref = None
     if rank == 0 and not args.no_ewald:
-        from treepm import accuracy
-        p_now, _, a_now = solver.get_state(n, pos=True, vel=False, acc=True)
-        tg = accuracy.seeded_targets(n, args.ewald_targets)
-        g_last = factors[args.warmup + args.steps - 1][3]
-        t_e = time.perf_counter()
-        ref = accuracy.ewald_accelerations(p_now, box.mass, box.box_size, g_last, phys["eps2"],
-                                           phys["r_cut_factor"] * phys["r_split"], tg, device=local)
-        rms, p99 = accuracy.relative_errors(a_now[tg], ref)
-        ewald = {"rms": rms, "p99": p99, "targets": int(len(tg)), "seconds": time.perf_counter() - t_e,
+        restart()
+        rows = []
+        p0, v0, a_first = solver.get_state(n)
+        rows.append(dict(diagnostics.record(p0, v0, box.mass, a0), step=0,
+                         force_momentum_residual=diagnostics.force_momentum_residual(a_first, box.mass)))
+        t_e = 0.0
+        for i, (d, k1, k2, g) in enumerate(factors):
+            solver.kdk_step(k1, d, k2, phys["eps2"], g)
+            p_now, v_now, a_now = solver.get_state(n)
+            row = dict(diagnostics.record(p_now, v_now, box.mass, a_of[i + 1]), step=i + 1,
+                       force_momentum_residual=diagnostics.force_momentum_residual(a_now, box.mass))
+            c0 = time.perf_counter()
+            ref = accuracy.ewald_accelerations(p_now, box.mass, box.box_size, g, phys["eps2"],
+                                               phys["r_cut_factor"] * phys["r_split"], tg, device=local)
+            t_e += time.perf_counter() - c0
+            row["ewald_rms"], row["ewald_p99"] = accuracy.relative_errors(a_now[tg], ref)
+            rows.append(row)
+        p_scale = max(math.sqrt(2.0 * r["kinetic_energy"] * r["mass_total"]) for r in rows)
+        traj_rep = {
+            "steps": len(factors), "a": [a0, a1],
+            "rows": rows,
+            "max_momentum_drift_over_rms_momentum": max(
+                float(np.linalg.norm(np.subtract(r["momentum"], rows[0]["momentum"]))) for r in rows) / p_scale,
+            "max_force_momentum_residual": max(r["force_momentum_residual"] for r in rows),
+            "momentum_note": "the reference's periodic walk takes a node below 0.1 r_cut as a monopole even when it "
+                             "holds the target (short_range.rs:316-323), so momentum is not conserved on clustered "
+                             "boxes; the device's residual |sum m a| / max m|a| equals the oracle's on the same state",
+            "ewald_seconds": t_e,
+            "note": "kinetic energy, momentum, angular momentum and com as diagnostics.rs:55-90 on the canonical "
+                    "momenta; Ewald error of each step's closing force on 4096 seeded targets",
+        }
+        last = rows[-1]
+        ewald = {"rms": last["ewald_rms"], "p99": last["ewald_p99"], "targets": int(len(tg)), "seconds": t_e,
+                 "state": f"after the {len(factors)} steps a = {a0} -> {a1}",
                  "reference": "FP64 Ewald, Plummer-softened nearest images within r_cut"}
+        g_last = factors[-1][3]
         if not args.no_accurate:
             accurate = accurate_mode_report(box, mesh, phys, p_now, g_last, tg, ref, local)
-            learned_rep = learned_mode_report(box, mesh, phys, p_now, g_last, tg, ref, local, ms_per_step)
+
+    # ---- device-resident loop (value): K steady-state steps of the trajectory,
+    # timed in segments of at most TRAJ_STEPS steps; each segment starts from
+    # the initial state (restart outside the timed brackets)
+    for i in range(args.warmup):
+        if i % len(factors) == 0:
+            restart()
+        d, k1, k2, g = factors[i % len(factors)]
+        solver.kdk_step(k1, d, k2, phys["eps2"], g)
+    torch.cuda.synchronize()
+    walk_ms, stats = [], []
+    dev_ms_rank = 0.0
+    with ClockSampler(local) as clocks:
+        done = 0
+        while done < args.steps:
+            seg = min(len(factors), args.steps - done)
+            restart()
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            for i in range(seg):
+                d, k1, k2, g = factors[i]
+                solver.kdk_step(k1, d, k2, phys["eps2"], g)
+                st = solver.stats()
+                stats.append(st)
+                walk_ms.append(st["ms_walk"])
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            dev_ms_rank += ev0.elapsed_time(ev1)
+            done += seg
+    dev_ms = max_over_ranks(dev_ms_rank, "cuda")
+    ms_per_step = dev_ms / args.steps
+    value = whole_job_rate(n, args.steps, dev_ms * 1e-3, world)
+    if rank == 0 and p_now is not None and not args.no_accurate:
+        learned_rep = learned_mode_report(box, mesh, phys, p_now, factors[-1][3], tg, ref, local, ms_per_step,
+                                          path=args.learned_weights,
+                                          deltas=[float(x) for x in args.learned_deltas.split(",")] if
+                                          args.learned_deltas else None)
 
     # ---- in-situ P(k) of the final state (analysis, not part of the step) --
     pk_rep = None
@@ -491,30 +616,37 @@ def run_b200(args):
     if rank == 0 and not args.no_ics:
         ic_rep = zeldovich_report(local)
 
-    # ---- end to end through the host-buffer API (e2e) -------------------
-    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
+    # ---- end to end through the host-buffer API (e2e): the whole trajectory
+    # from the initial state, float64 host arrays in and out every step; the
+    # first step meets a new state (upload, encode, two force evaluations)
+    e2e_steps = 0 if args.no_e2e else max(1, min(len(factors), args.e2e_steps))
     pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     vel = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     mass = torch.empty((n,), dtype=torch.float64, pin_memory=True).numpy()
-    pos[:] = box.positions()
-    vel[:] = 0.0
+    p_ic = box.positions()
     mass[:] = box.mass
-    d, k1, k2, g = factors[0]
+
+    def host_ic():
+        pos[:] = p_ic
+        vel[:] = 0.0
+
     if e2e_steps:
-        solver.kdk_step_host(pos, vel, mass, k1, d, k2, phys["eps2"], g)  # warm
+        host_ic()
+        for i in range(2):  # warm: the first two steps of the trajectory
+            d, k1, k2, g = factors[i]
+            solver.kdk_step_host(pos, vel, mass, k1, d, k2, phys["eps2"], g)
+        host_ic()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
     for i in range(e2e_steps):
-        d, k1, k2, g = factors[1 + i]
+        d, k1, k2, g = factors[i]
         solver.kdk_step_host(pos, vel, mass, k1, d, k2, phys["eps2"], g)
-    e1.record(stream)
     torch.cuda.synchronize()
     e2e_wall = max_over_ranks(time.perf_counter() - t0, "cuda")
     e2e_value = whole_job_rate(n, e2e_steps, e2e_wall, world) if e2e_steps else None
+    del p_ic
     h2d = n * (24 + 24 + 8)
     d2h = n * (24 + 24)
 
@@ -534,7 +666,11 @@ def run_b200(args):
         "data": "synthetic",
         "config": {"workload": box.name, "particles": n, "mesh": mesh, "box_mpc_h": box.box_size,
                    "r_s_cells": 1.25, "r_cut_over_r_s": 4.5, "softening": "mean spacing / 30",
-                   "a": [a0, a1], "parallelism": f"{world} independent replica(s)",
+                   "a": [a0, a1], "trajectory_steps": len(factors),
+                   "timing": "K steady-state steps of the a0 -> a1 trajectory, timed in segments of at most "
+                             f"{len(factors)} steps, each from the initial state with its forces evaluated "
+                             "(outside the timed brackets)",
+                   "parallelism": f"{world} independent replica(s)",
                    "l2": "inputs larger than L2 (>= 0.8 GB touched per step)"},
         "per_force_evaluation": {"value": value, "note": "one force evaluation per fused step; the reference "
                                                          "evaluates twice per step"},
@@ -545,17 +681,22 @@ def run_b200(args):
                  "tree_nodes": st["n_tree_nodes"], "groups": st["n_groups"], "max_depth": st["max_tree_depth"]},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": (achieved / peak) if peak else None, "traffic": profile_traffic(box.name),
+                     "traffic_source": "ncu single-pass capture of this workload's walk, not of this run",
                      "kernel": "k_walk (short-range erfc walk)",
                      "note": f"{FLOP_PER_INTERACTION} FLOP per reference interaction (leaf pair or monopole); "
                              "peak = FFMA throughput measured live on this GPU"},
         "e2e": {"value": e2e_value, "unit": "particle-updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
-                "path": "tpm_kdk_step_host: float64 positions, velocities and masses from pinned host memory, "
-                        "state back to host each step; the inputs are the state the previous call returned, so the "
-                        "step runs on the resident state (one force evaluation) while a copy stream uploads and checks "
-                        "the inputs and returns the drifted positions; the momenta are copied after the closing kick"},
+                "steps": e2e_steps,
+                "path": "tpm_kdk_step_host over the whole trajectory from the initial state (wall clock): float64 "
+                        "positions, velocities and masses from pinned host memory, state back to host each step; the "
+                        "first step meets a new state (upload, encode, two force evaluations); later steps get the "
+                        "state the previous call returned, so they run on the resident state (one force evaluation) "
+                        "while a copy stream uploads and checks the inputs and returns the drifted positions; the "
+                        "momenta are copied after the closing kick"},
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "force_error_vs_ewald": ewald,
+        "trajectory_diagnostics": traj_rep,
         "accurate_mode": accurate,
         "learned_mode": learned_rep,
         "power_spectrum": pk_rep,
@@ -567,7 +708,8 @@ def run_b200(args):
         cv = n / (2.0 * t_force)
         line["cpu_baseline"] = {"value": cv, "unit": "particle-updates/s", "cores": info["threads"], "kind": "port",
                                 "sample": (f"oracle restatement (C++/OpenMP, FP64): full PM + full octree build, "
-                                           f"walk of {info['targets']} targets extrapolated; 2 force evaluations "
+                                           f"walk of {info['targets']} targets (one run of consecutive particles in each of 64 strata) "
+                                           f"extrapolated; 2 force evaluations "
                                            f"per step; stages s: pm {info['pm_s']:.2f}, build {info['build_s']:.2f}, "
                                            f"walk-sample {info['walk_s']:.2f}")}
     if rank == 0:
@@ -606,12 +748,7 @@ def run_domain(args):
     box, mesh, a0, a1 = make_box(args.workload)
     phys = ics.physics(box, mesh, a0)
     n = box.n
-    dt = ics.time_between(a0, a1) / 10.0
-    a, factors = a0, []
-    for _ in range(args.warmup + args.steps + 1):
-        d, k1, k2 = treepm.drift_kick_factors(ics.OMEGA_M, ics.OMEGA_L, ics.H0_INTERNAL, a, dt)
-        factors.append((d, k1, k2, phys["G"] * a ** 3))
-        a = treepm.advance_a(ics.OMEGA_M, ics.OMEGA_L, ics.H0_INTERNAL, a, dt)
+    factors, _ = trajectory(a0, a1, phys["G"], total=args.warmup + args.steps + 1)
     dom = DomainTreePm(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"], device=local)
     lo, hi = rank * n // world, (rank + 1) * n // world
     pos = box.positions()[lo:hi]
@@ -674,9 +811,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="clustered256", choices=sorted(WORKLOADS))
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-targets", type=int, default=65536)
+    ap.add_argument("--e2e-steps", type=int, default=TRAJ_STEPS)
+    ap.add_argument("--cpu-targets", type=int, default=262144)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-full", action="store_true",
+                    help="reference arm: skip the one complete (non-extrapolated) CPU force evaluation")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--no-ics", action="store_true", help="skip the Zel'dovich IC timing")
     ap.add_argument("--ics-only", action="store_true", help="time only the Zel'dovich IC generator")
@@ -687,8 +826,13 @@ def main():
     ap.add_argument("--no-ewald", action="store_true", help="skip the FP64 Ewald error report")
     ap.add_argument("--no-accurate", action="store_true", help="skip the accurate-mode report")
     ap.add_argument("--ewald-targets", type=int, default=4096)
+    ap.add_argument("--learned-weights", default=None, help="weights file of the learned mode (default: committed)")
+    ap.add_argument("--learned-deltas", default=None,
+                    help="comma-separated fallback overdensity thresholds to sweep in the learned mode")
     ap.add_argument("--domain", action="store_true",
-                    help="domain-decomposed steps over the ranks (SFC domains, halos, density all-reduce)")
+                    help="domain-decomposed steps over the ranks (SFC domains, halos, density all-reduce); "
+                         "the default when --gpus > 1")
+    ap.add_argument("--replicas", action="store_true", help="with --gpus > 1: independent copies, one per rank")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -698,7 +842,7 @@ def main():
         return run_ics_only(args)
     if args.snapshot_only:
         return run_snapshot_only(args)
-    if args.domain:
+    if args.domain or (args.gpus > 1 and not args.replicas):
         return run_domain(args)
     return run_b200(args)
 

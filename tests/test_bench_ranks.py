@@ -1,8 +1,9 @@
 """The benchmark's multi-rank bookkeeping on CPU (gloo, two ranks).
 
-`bench.py --gpus N` runs N independent replicas; the only cross-rank steps
-are a barrier and the maximum of the per-rank times, and the reference arm
-runs on rank 0 alone.  Both run here without a GPU.
+The timed region of every mode ends in a barrier and the maximum of the
+per-rank times (with --replicas the rate is the units of all copies over the
+slowest rank's time), and the reference arm runs on rank 0 alone.  Both run
+here without a GPU.
 """
 import os
 import socket
