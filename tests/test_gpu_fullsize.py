@@ -63,3 +63,20 @@ def test_pm_box_64_parity():
     ref = oracle().pm(pos, b.mass, g, 64, b.box_size)
     rel = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
     assert float(np.sqrt(np.mean(rel ** 2))) < 1e-5
+
+
+def test_hilbert_keys_and_order_bit_exact_at_256():
+    """Every particle's Hilbert key and the (key, index) sort order of the
+    256³ clustered workload, bit for bit against the oracle (sfc.rs:95-204,
+    :371-372)."""
+    import treepm
+    from treepm import ics
+    box = ics.clustered_box_256()
+    pos = box.positions()
+    s = treepm.TreePmSolver(64, box.box_size, 0.0)
+    s.set_particles(pos, box.mass)
+    keys, order = s.hilbert_keys(box.n)
+    s.close()
+    rk, ro = oracle().hilbert_keys(pos)
+    assert np.array_equal(keys, rk)
+    assert np.array_equal(order, ro)
