@@ -467,6 +467,42 @@ __global__ void k_walk_nodes(int64_t n_int, double inv_scale, const double* __re
   walk[id] = make_uint4(q[0], q[1], q[2], __float_as_uint((float)o_mass[id]));
 }
 
+// Cell centre and |Q|_F of each internal node (relative opening criterion).
+// The node's octant path is the first `depth` digits of any of its particles'
+// keys (sorted order: o_first); the centre follows child_center level by
+// level in float64 as k_tree_keys does.
+__global__ void k_cell_q(int64_t n_int, double inv_scale, const TreeParams* __restrict__ prm,
+                         const uint8_t* __restrict__ o_depth, const uint32_t* __restrict__ o_first,
+                         const uint64_t* __restrict__ key_hi, const uint64_t* __restrict__ key_lo,
+                         const double* __restrict__ o_quad, uint4* __restrict__ out) {
+  int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (id >= n_int) return;
+  const int dep = o_depth[id];
+  const uint32_t p = o_first[id];
+  double c[3] = {prm->center[0], prm->center[1], prm->center[2]};
+  double h = prm->half;
+  for (int l = 1; l <= dep && l <= KEY_LEVELS; ++l) {
+    const uint64_t w = l <= KEY_LEVELS / 2 ? key_hi[p] : key_lo[p];
+    const int ll = l <= KEY_LEVELS / 2 ? l : l - KEY_LEVELS / 2;
+    const uint32_t digit = (uint32_t)(w >> (63 - 3 * ll)) & 7u;
+    const double q = dmul(h, 0.5);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c[d] = dadd(c[d], ((digit >> d) & 1u) ? q : -q);
+    h = q;
+  }
+  uint32_t cq[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double u = c[d] * inv_scale;  // fixed point, wrapped like positions
+    cq[d] = (uint32_t)((unsigned long long)llrint(u) & 0xFFFFFFFFull);
+  }
+  const double* Q = o_quad + 6 * id;
+  double f2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) f2 = fma(Q[k], Q[k], f2);
+  out[id] = make_uint4(cq[0], cq[1], cq[2], __float_as_uint((float)sqrt(f2)));
+}
+
 // ---------------------------------------------------------------------------
 // walk records: children of each internal node contiguous
 // ---------------------------------------------------------------------------
@@ -782,6 +818,13 @@ void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, 
     TPM_LAUNCH_CHECK();
   }
   k_walk_nodes<<<grid_for(n_int, 256, 1ll << 30), 256, 0, s>>>(n_int, TWO32 / box, t.o_mass, t.o_com, t.o_walk);
+  TPM_LAUNCH_CHECK();
+}
+
+void launch_cell_q(int64_t n_int, double box, TreeBuffers& t, cudaStream_t s) {
+  if (n_int <= 0) return;
+  k_cell_q<<<grid_for(n_int, 256, 1ll << 30), 256, 0, s>>>(n_int, TWO32 / box, t.params, t.o_depth, t.o_first,
+                                                           t.key_hi, t.key_lo, t.o_quad, t.o_cell);
   TPM_LAUNCH_CHECK();
 }
 

@@ -80,6 +80,7 @@ struct TreeBuffers {
   double* o_com;   // 3 per node
   double* o_quad;  // 6 per node
   uint4* o_walk;   // fixed-point COM (x, y, z) and float mass bits
+  uint4* o_cell;   // relative opening criterion: fixed-point cell centre (x, y, z), |Q|_F float bits
   WalkNode* recs;  // n_int + n walk records
   // leaves
   int32_t* leaf_oparent;
@@ -112,6 +113,11 @@ void launch_octree_links(int64_t n, int64_t n_int, TreeBuffers& t, void* scan_sc
 void launch_aggregate(const Particles& p, int64_t n, int64_t n_int, double box, TreeBuffers& t, cudaStream_t s,
                       bool with_quad = false);
 void launch_walk_records(const Particles& p, int64_t n, int64_t n_int, double thr, TreeBuffers& t, cudaStream_t s);
+// Per internal node: the centre of its octree cell (child_center replayed
+// along the node's octant path, octree.rs:446-465) in fixed point and the
+// Frobenius norm of its six stored quadrupole components (the relative
+// opening criterion's estimate, octree.rs:769-796).  Needs the quadrupoles.
+void launch_cell_q(int64_t n_int, double box, TreeBuffers& t, cudaStream_t s);
 void launch_groups(int64_t n, int64_t n_int, int group_max, TreeBuffers& t, void* scan_scratch, cudaStream_t s);
 void launch_hilbert_keys(const Particles& p, int64_t n, double box, const TreeParams* prm, uint64_t* keys,
                          uint32_t* vals, cudaStream_t s);

@@ -386,12 +386,39 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       }
       bool open, macmix = false;
       if (ACC && !leaf) {
-        // opening angle s/d < theta, s = 2 * half side (octree.rs:763-809);
-        // a margin on both sides leaves the float-rounding cases to the
-        // per-target test at pop time
-        const float s2 = 4.f * hnode * hnode;
-        const bool accept_all = s2 < a.theta2 * dmin2 * 0.999f;
-        const bool open_all = s2 >= a.theta2 * dmax2 * 1.001f;
+        bool accept_all, open_all;
+        if (a.relative) {
+          // relative criterion (octree.rs:769-796): accept when the target is
+          // outside the node's cell and |Q|_F (d^2 + eps^2) < k M d^5; that
+          // bound falls with d, so the group's nearest and farthest COM
+          // distances decide it for every target, and a group box touching
+          // the cell leaves the node to the per-target test.  Nodes at the
+          // top levels (periodic images) are always opened.
+          const uint4 cc = __ldg(&a.cellq[r1.z]);
+          const float qf = __uint_as_float(cc.w), m = __uint_as_float(r0.w);
+          const uint32_t ccq[3] = {cc.x, cc.y, cc.z};
+          bool touch = true, inside_all = true;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const float c = (float)rel32(ccq[d], oq[d], a.periodic) * a.u_inv;
+            const float lo = c - hnode * 1.0001f, hi = c + hnode * 1.0001f;
+            touch = touch && lo <= bmax[d] && hi >= bmin[d];
+            inside_all = inside_all && lo <= bmin[d] && hi >= bmax[d];
+          }
+          const float dmn = sqrtf(dmin2), dmx = sqrtf(dmax2);
+          accept_all = !touch && dmin2 > 0.f &&
+                       qf * (dmin2 + a.eps2_u) < a.rel_k * m * (dmin2 * dmin2 * dmn) * 0.999f;
+          open_all = (a.periodic && dep < a.img_depth) || inside_all ||
+                     !(qf * (dmax2 + a.eps2_u) < a.rel_k * m * (dmax2 * dmax2 * dmx) * 1.001f);
+          accept_all = accept_all && !open_all;
+        } else {
+          // opening angle s/d < theta, s = 2 * half side (octree.rs:763-809);
+          // a margin on both sides leaves the float-rounding cases to the
+          // per-target test at pop time
+          const float s2 = 4.f * hnode * hnode;
+          accept_all = s2 < a.theta2 * dmin2 * 0.999f;
+          open_all = s2 >= a.theta2 * dmax2 * 1.001f;
+        }
         open = !accept_all;
         macmix = !accept_all && !open_all;
       } else {
@@ -515,8 +542,11 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     const uint32_t take = __ballot_sync(0xffffffffu, lane < avail && incl <= 32u);
     const int k = __popc(take);
     sp -= k;
-    uint4 wrec = make_uint4(0u, 0u, 0u, 0u);
-    if (ACC && lane < k && (e.y & INFO_MAC)) wrec = __ldg(&a.walk[e.w]);
+    uint4 wrec = make_uint4(0u, 0u, 0u, 0u), crec = make_uint4(0u, 0u, 0u, 0u);
+    if (ACC && lane < k && (e.y & INFO_MAC)) {
+      wrec = __ldg(&a.walk[e.w]);
+      if (a.relative) crec = __ldg(&a.cellq[e.w]);
+    }
     // accurate mode: per-target opening angle for nodes undecided for the
     // group; targets that accept take the node as a monopole now, the rest
     // open it
@@ -530,6 +560,10 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const uint4 w = make_uint4(__shfl_sync(0xffffffffu, wrec.x, src), __shfl_sync(0xffffffffu, wrec.y, src),
                                  __shfl_sync(0xffffffffu, wrec.z, src), __shfl_sync(0xffffffffu, wrec.w, src));
       const float hnode = half_side(a.h0_u, dep);
+      uint4 cw = make_uint4(0u, 0u, 0u, 0u);
+      if (a.relative)
+        cw = make_uint4(__shfl_sync(0xffffffffu, crec.x, src), __shfl_sync(0xffffffffu, crec.y, src),
+                        __shfl_sync(0xffffffffu, crec.z, src), __shfl_sync(0xffffffffu, crec.w, src));
       bool accept = false;
       if (has && lane < TPW && ((me >> tgt) & 1u)) {
         float d2 = 0.f;
@@ -539,7 +573,19 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
           const float dd = (float)rel32(wq[d], tq[d], a.periodic) * a.u_inv;
           d2 = fmaf(dd, dd, d2);
         }
-        accept = 4.f * hnode * hnode < a.theta2 * d2;
+        if (a.relative) {
+          // point_in_node_cell with a margin (a target on the cell's face
+          // opens the node), then the truncation estimate
+          const uint32_t cq3[3] = {cw.x, cw.y, cw.z};
+          bool inside = true;
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            inside = inside && fabsf((float)rel32(cq3[d], tq[d], a.periodic) * a.u_inv) <= hnode * 1.0001f;
+          const float qf = __uint_as_float(cw.w), m = __uint_as_float(w.w);
+          accept = !inside && d2 > 0.f && qf * (d2 + a.eps2_u) < a.rel_k * m * (d2 * d2 * sqrtf(d2));
+        } else {
+          accept = 4.f * hnode * hnode < a.theta2 * d2;
+        }
       }
       const uint32_t am = __ballot_sync(0xffffffffu, accept);
       if (am) {  // one monopole entry for the accepting targets (same slot on every lane)

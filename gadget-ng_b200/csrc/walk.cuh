@@ -46,6 +46,9 @@ struct WalkArgs {
   int accurate;      // extension mode: complete split kernel + opening angle
   float theta2;      // opening angle squared (accurate mode)
   float gkc;         // (2/sqrt(pi)) * u/(sqrt(2) r_s): the Gaussian term of the split
+  int relative;      // accurate mode: relative opening criterion instead of the opening angle
+  float rel_k;       // err_tol * u^3 (relative criterion, walk units)
+  const uint4* cellq;  // per internal node: fixed-point cell centre, |Q|_F float bits
   // outputs (physical, per unit G), sorted order
   float* ax;
   float* ay;

@@ -87,8 +87,9 @@ typedef struct tpm_config {
   double r_split;             /* [gravity] r_split; <= 0 selects 2.5 cells (solver.rs:56-62) */
   double r_cut_factor;        /* extension key gravity.r_cut_factor; <= 0 selects 5.0 (solver.rs:80) */
   double theta;               /* [gravity] theta: unused by the parity walk; the opening angle of TPM_FLAG_ACCURATE (0 = 0.5) */
-  int32_t opening_criterion;  /* [gravity] opening_criterion: 0 geometric, 1 relative (unused by TreePM) */
-  double err_tol_force_acc;   /* [gravity] err_tol_force_acc (unused by TreePM) */
+  int32_t opening_criterion;  /* [gravity] opening_criterion: 0 geometric, 1 relative (octree.rs:769-796);
+                                 read by the TPM_FLAG_ACCURATE walk, not by the parity walk */
+  double err_tol_force_acc;   /* [gravity] err_tol_force_acc: the relative criterion's tolerance */
   uint32_t flags;             /* TPM_FLAG_* */
   int32_t device;             /* CUDA device ordinal */
   int64_t memory_cap_bytes;   /* 0 = no cap; otherwise refuse allocations beyond it */

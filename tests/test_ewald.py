@@ -142,3 +142,29 @@ def test_accurate_mode_rejects_wide_opening_angle():
     with pytest.raises(treepm.TreePmError) as e:
         treepm.TreePmSolver(32, 50.0, 0.0, accurate=True, theta=0.6)
     assert e.value.code == 1  # TPM_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.gpu
+def test_accurate_mode_relative_criterion_against_ewald():
+    """The relative opening criterion (octree.rs:769-796: open a node while the
+    quadrupole estimate g |Q|_F / d^5 is at least err_tol times the monopole
+    g M / (d^2 + eps^2), or while the target lies in its cell) on the
+    clustered 32^3 box: a tight tolerance reaches the mesh floor of the
+    opening-angle mode, a loose one is less accurate."""
+    from treepm import ics
+    b = ics.clustered_box(32, 50.0, 0.3, 20, min_halo=50, max_halo=2000, seed=9)
+    tight, p99 = _accurate_error(b, 32, 512, accurate=True, opening_criterion=1, err_tol_force_acc=1e-4,
+                                 deconvolve_cic=True)
+    loose, _ = _accurate_error(b, 32, 512, accurate=True, opening_criterion=1, err_tol_force_acc=0.5,
+                               deconvolve_cic=True)
+    geo, _ = _accurate_error(b, 32, 512, accurate=True, theta=0.5, deconvolve_cic=True)
+    assert tight < 3e-2 and p99 < 1e-1, (tight, p99)
+    assert tight <= 1.05 * geo, (tight, geo)
+    assert loose > tight, (loose, tight)
+
+
+def test_relative_criterion_needs_a_positive_tolerance():
+    import treepm
+    with pytest.raises(treepm.TreePmError) as e:
+        treepm.TreePmSolver(32, 50.0, 0.0, accurate=True, opening_criterion=1, err_tol_force_acc=0.0)
+    assert e.value.code == 1  # TPM_ERR_INVALID_ARGUMENT
