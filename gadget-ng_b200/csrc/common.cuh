@@ -43,6 +43,7 @@ enum : uint32_t {
   DEV_ERR_TIE_RUN = 1u << 4,
   DEV_ERR_NONFINITE = 1u << 5,
   DEV_ERR_MMA_TIMEOUT = 1u << 6,  // a tensor-core wait ran past its time limit
+  DEV_ERR_TMA_TIMEOUT = 1u << 7,  // a TMA (bulk tensor copy) wait ran past its time limit
 };
 
 // ---- fixed point --------------------------------------------------------------

@@ -141,12 +141,13 @@ __global__ void k_ic_sigma_table(IcSpectrum sp, const double* __restrict__ amp_d
 // delta(k) of every half-spectrum mode from the mode seeds, written as the
 // three Psi1 components i n_a / |n|^2 delta (ic_zeldovich.rs:541-585) and,
 // when `delta_out` is given, as delta itself for the second-order fields.
-__global__ void k_ic_modes(int n, int nh, uint64_t seed, const double* __restrict__ sigma_of_n2,
+__global__ void k_ic_modes(int n, int nh, int nhp, uint64_t seed, const double* __restrict__ sigma_of_n2,
                            float2* __restrict__ spec3, int64_t comp_stride, float2* __restrict__ delta_out) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t total = (int64_t)n * n * nh;
+  const int64_t total = (int64_t)n * n * nhp;  // rows of nhp: kx >= nh is padding
   if (i >= total) return;
-  const int kx = (int)(i % nh), y = (int)((i / nh) % n), z = (int)(i / ((int64_t)n * nh));
+  const int kx = (int)(i % nhp), y = (int)((i / nhp) % n), z = (int)(i / ((int64_t)n * nhp));
+  if (kx >= nh) return;
   const int nx = kx, ny = mode_int(y, n), nz = mode_int(z, n), half = n / 2;
   const double n2 = (double)nx * nx + (double)ny * ny + (double)nz * nz;
   float2 out[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
@@ -182,12 +183,13 @@ __global__ void k_ic_modes(int n, int nh, uint64_t seed, const double* __restric
 // Second derivatives of phi from the stored delta (ic_2lpt.rs:86-140):
 // -n_a^2 / |n|^2 delta for a = x, y, z (off_diagonal 0) or -n_a n_b / |n|^2
 // delta for ab = xy, xz, yz (off_diagonal 1).
-__global__ void k_ic_phi_ab(const float2* __restrict__ delta, int n, int nh, float2* __restrict__ spec3,
+__global__ void k_ic_phi_ab(const float2* __restrict__ delta, int n, int nh, int nhp, float2* __restrict__ spec3,
                             int64_t comp_stride, int off_diagonal) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t total = (int64_t)n * n * nh;
+  const int64_t total = (int64_t)n * n * nhp;
   if (i >= total) return;
-  const int kx = (int)(i % nh), y = (int)((i / nh) % n), z = (int)(i / ((int64_t)n * nh));
+  const int kx = (int)(i % nhp), y = (int)((i / nhp) % n), z = (int)(i / ((int64_t)n * nhp));
+  if (kx >= nh) return;
   const float na[3] = {(float)kx, (float)mode_int(y, n), (float)mode_int(z, n)};
   const float n2 = na[0] * na[0] + na[1] * na[1] + na[2] * na[2];
   const float2 dk = delta[i];
@@ -215,12 +217,13 @@ __global__ void k_ic_source(const float* __restrict__ f, float* __restrict__ rho
 
 // Psi2_a(k) = -i n_a / |n|^2 S(k), zero at DC and on the Nyquist planes
 // (ic_2lpt.rs:181-240).
-__global__ void k_ic_psi2_modes(const float2* __restrict__ src, int n, int nh, float2* __restrict__ spec3,
+__global__ void k_ic_psi2_modes(const float2* __restrict__ src, int n, int nh, int nhp, float2* __restrict__ spec3,
                                 int64_t comp_stride) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t total = (int64_t)n * n * nh;
+  const int64_t total = (int64_t)n * n * nhp;
   if (i >= total) return;
-  const int kx = (int)(i % nh), y = (int)((i / nh) % n), z = (int)(i / ((int64_t)n * nh));
+  const int kx = (int)(i % nhp), y = (int)((i / nhp) % n), z = (int)(i / ((int64_t)n * nhp));
+  if (kx >= nh) return;
   const int nx = kx, ny = mode_int(y, n), nz = mode_int(z, n), half = n / 2;
   const float n2 = (float)(nx * nx + ny * ny + nz * nz);
   float2 out[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
@@ -387,7 +390,7 @@ void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cu
       TPM_CUDA(cudaGetDevice(&dev));
       pm_plan_init(temp, n, box, 0.0, 0u, dev);
     }
-    const int64_t nh = n / 2 + 1, plane = (int64_t)n * n * nh, n3 = (int64_t)n * n * n;
+    const int64_t nh = n / 2 + 1, plane = (int64_t)n * n * plan.nhp, n3 = (int64_t)n * n * n;
     const unsigned gm = grid_for(plane, 256, 1ll << 30), gp = grid_for(n3, 256, 1ll << 30);
     const double cell_over_n3 = (box / n) / (double)n3;  // rustfft's inverse is unnormalised
     // sigma(|n|) tabulated by |n|^2 in the density buffer (6 n^2 + 16 bytes of
@@ -403,7 +406,7 @@ void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cu
     k_ic_sigma_table<<<grid_for(n2_max + 1, 256, 1ll << 30), 256, 0, s>>>(sp, amp_dev, n2_max, table);
     TPM_LAUNCH_CHECK();
     // first order; delta kept in the spectrum work array for the second
-    k_ic_modes<<<gm, 256, 0, s>>>(n, (int)nh, c->seed, table, plan.spec3, plane, c->use_2lpt ? plan.spec : nullptr);
+    k_ic_modes<<<gm, 256, 0, s>>>(n, (int)nh, plan.nhp, c->seed, table, plan.spec3, plane, c->use_2lpt ? plan.spec : nullptr);
     TPM_LAUNCH_CHECK();
     pm_inverse_components(plan, 3, s);
     k_ic_particles<<<gp, 256, 0, s>>>(n, box, cell_over_n3 * fa.scale, fa.vel1, plan.force, n3, out);
@@ -411,14 +414,14 @@ void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cu
     if (c->use_2lpt) {
       const float inv_n3 = (float)(1.0 / (double)n3);
       for (int off = 0; off < 2; ++off) {
-        k_ic_phi_ab<<<gm, 256, 0, s>>>(plan.spec, n, (int)nh, plan.spec3, plane, off);
+        k_ic_phi_ab<<<gm, 256, 0, s>>>(plan.spec, n, (int)nh, plan.nhp, plan.spec3, plane, off);
         TPM_LAUNCH_CHECK();
         pm_inverse_components(plan, 3, s);
         k_ic_source<<<gp, 256, 0, s>>>(plan.force, plan.rho, n3, inv_n3, off);
         TPM_LAUNCH_CHECK();
       }
       pm_forward_real(plan, s);  // S(k) replaces delta in the work array
-      k_ic_psi2_modes<<<gm, 256, 0, s>>>(plan.spec, n, (int)nh, plan.spec3, plane);
+      k_ic_psi2_modes<<<gm, 256, 0, s>>>(plan.spec, n, (int)nh, plan.nhp, plan.spec3, plane);
       TPM_LAUNCH_CHECK();
       pm_inverse_components(plan, 3, s);
       k_ic_add_psi2<<<gp, 256, 0, s>>>(n, box, cell_over_n3 * fa.scale * fa.scale, fa.d21, fa.vel2, plan.force, n3,
@@ -426,6 +429,7 @@ void zeldovich_fill(const tpm_zeldovich* c, double box, const Particles& out, cu
       TPM_LAUNCH_CHECK();
     }
     TPM_CUDA(cudaStreamSynchronize(s));
+    pm_check(plan, s);
   } catch (...) {
     if (!reuse) pm_plan_free(temp);
     throw;

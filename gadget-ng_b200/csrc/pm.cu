@@ -15,12 +15,22 @@
 // three real force meshes.  Taking the real part in the reference zeroes the
 // derivative's Nyquist plane (F_x at kx = N/2 and so on); the derivative table
 // is zero there, so the half spectrum is exactly Hermitian.  Every 1D
-// transform is a radix-2 Stockham autosort FFT in shared memory.  Linear in G:
-// the meshes hold forces per unit G, the gather multiplies by g.
+// transform is a two-stage register transform (fft_reg.cuh) with one
+// shared-memory exchange; the y and z passes stage their pencils (CTX
+// adjacent kx columns of a z plane or a y row) with TMA tensor copies, the x
+// passes their contiguous rows with one bulk copy per block.  Half-spectrum
+// rows are padded to an even length (nhp) for the copies' 16-byte rule.
+// Linear in G: the meshes hold forces per unit G, the gather multiplies by g.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
+#include <cstring>
 #include <vector>
 
+#include "../../include/treepm_b200.h"
 #include "common.cuh"
+#include "fft_reg.cuh"
 #include "pm.cuh"
 
 namespace tpm {
@@ -30,15 +40,6 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-
-// Batched Stockham FFT in shared memory.  ROWMAJOR: element (j, c) at
-// a[c * n + j]; otherwise at a[j * cols + c].  Returns the buffer holding the
-// result (a or b).
-template <bool ROWMAJOR>
-__device__ __forceinline__ int fft_addr(int c, int j, int n, int cols) {
-  return ROWMAJOR ? c * n + j : j * cols + c;
-}
 
 // Twiddle exp(-+2 pi i m / n) from the half table tw[m] = exp(-2 pi i m / n), m < n/2.
 __device__ __forceinline__ float2 twiddle(const float2* tw, int m, int n, bool inv) {
@@ -48,85 +49,264 @@ __device__ __forceinline__ float2 twiddle(const float2* tw, int m, int n, bool i
   return w;
 }
 
-// Stockham radix-4 passes (one radix-2 pass last when log2 n is odd): each
-// pass reads a, writes b, then swaps; between passes only shared memory and
-// one barrier.  Pass with Ns outputs done so far: element j of a column,
-// k = j mod Ns, inputs a[j + i n/4] twiddled by w^(i k) with w = exp(-2 pi i /
-// (4 Ns)), a 4-point DFT, outputs b[(j / Ns) 4 Ns + k + i Ns].  cols is a
-// power of two (log2 = lcols).
-template <bool ROWMAJOR>
-__device__ float2* fft_smem(float2* a, float2* b, int n, int logn, int cols, const float2* tw, bool inv) {
-  const int lcols = __ffs(cols) - 1;
-  int Ns = 1, lNs = 0;
-  while (logn - lNs >= 2) {
-    const int q = n >> 2, lq = logn - 2;
-    const int total = q << lcols;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-      int j, c;
-      if (ROWMAJOR) {
-        j = idx & (q - 1);
-        c = idx >> lq;
-      } else {
-        c = idx & (cols - 1);
-        j = idx >> lcols;
-      }
-      const int k = j & (Ns - 1);
-      float2 v0 = a[fft_addr<ROWMAJOR>(c, j, n, cols)];
-      float2 v1 = a[fft_addr<ROWMAJOR>(c, j + q, n, cols)];
-      float2 v2 = a[fft_addr<ROWMAJOR>(c, j + 2 * q, n, cols)];
-      float2 v3 = a[fft_addr<ROWMAJOR>(c, j + 3 * q, n, cols)];
-      if (k) {  // w^(i k) = exp(-2 pi i i k / (4 Ns)) = tw[i k n / (4 Ns)]
-        const int sh = logn - lNs - 2;
-        v1 = cmul(v1, twiddle(tw, k << sh, n, inv));
-        v2 = cmul(v2, twiddle(tw, (2 * k) << sh, n, inv));
-        v3 = cmul(v3, twiddle(tw, (3 * k) << sh, n, inv));
-      }
-      const float2 a0 = cadd(v0, v2), a1 = csub(v0, v2), a2 = cadd(v1, v3), d = csub(v1, v3);
-      // (v1 - v3) * (-i) forward, * (+i) inverse
-      const float2 a3 = inv ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);
-      const int o = ((j - k) << 2) + k;
-      b[fft_addr<ROWMAJOR>(c, o, n, cols)] = cadd(a0, a2);
-      b[fft_addr<ROWMAJOR>(c, o + Ns, n, cols)] = cadd(a1, a3);
-      b[fft_addr<ROWMAJOR>(c, o + 2 * Ns, n, cols)] = csub(a0, a2);
-      b[fft_addr<ROWMAJOR>(c, o + 3 * Ns, n, cols)] = csub(a1, a3);
-    }
-    __syncthreads();
-    float2* t = a;
-    a = b;
-    b = t;
-    Ns <<= 2;
-    lNs += 2;
-  }
-  if (lNs < logn) {  // the last radix-2 pass
-    const int half = n >> 1;
-    const int total = half << lcols;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-      int j, c;
-      if (ROWMAJOR) {
-        j = idx & (half - 1);
-        c = idx >> (logn - 1);
-      } else {
-        c = idx & (cols - 1);
-        j = idx >> lcols;
-      }
-      const int k = j & (Ns - 1);
-      const float2 w = twiddle(tw, k << (logn - 1 - lNs), n, inv);
-      const float2 x0 = a[fft_addr<ROWMAJOR>(c, j, n, cols)];
-      const float2 t = cmul(a[fft_addr<ROWMAJOR>(c, j + half, n, cols)], w);
-      const int o = ((j - k) << 1) + k;
-      b[fft_addr<ROWMAJOR>(c, o, n, cols)] = cadd(x0, t);
-      b[fft_addr<ROWMAJOR>(c, o + Ns, n, cols)] = csub(x0, t);
-    }
-    __syncthreads();
-    float2* t = a;
-    a = b;
-    b = t;
-  }
-  return a;
-}
-
 __device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* tw, int n) {
   for (int i = threadIdx.x; i < (n >> 1); i += blockDim.x) s_tw[i] = tw[i];
+}
+
+// ---- pencil passes (y and z): TMA-staged tiles, register transforms ----------------
+// A block transforms CTX adjacent kx columns of one y row (z pass) or one z
+// plane (y pass) of a half spectrum.  One thread issues the bulk tensor copy
+// of the n x CTX tile into shared memory (8-byte complex elements, rows of CTX
+// values); every thread then runs its share of the two-stage transform of
+// fft_reg.cuh and the valid columns are written back with coalesced stores.
+
+// Columns per tile: 16 (128-byte rows), 8 for the longest transforms.
+template <int LOGN> struct Pencil {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int CTX = N > 512 ? 8 : 16;
+  static constexpr int THREADS = CTX * fftr::Split<LOGN>::N2;
+  static constexpr int ROWS_PER_COPY = N < 256 ? N : 256;  // a tensor-map box spans at most 256 rows
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Stage the tile; false (and DEV_ERR_TMA_TIMEOUT) when the copy does not
+// complete within 2 s.  axis 0: y pencils (rows are y of plane `fixed`), 1: z
+// pencils (rows are z of row `fixed`); zbase = comp * nm.
+template <int LOGN>
+__device__ bool stage_pencil(float2* tile, uint64_t* bar, const CUtensorMap* map, int axis, int kx0, int fixed,
+                             int zbase, uint32_t* err) {
+  using P = Pencil<LOGN>;
+  const uint32_t b = smem_u32(bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b),
+                 "r"((uint32_t)(P::N * P::CTX * sizeof(float2)))
+                 : "memory");
+    for (int r0 = 0; r0 < P::N; r0 += P::ROWS_PER_COPY) {
+      const uint32_t dst = smem_u32(tile + (size_t)r0 * P::CTX);
+      const int y = axis == 0 ? r0 : fixed, z = axis == 0 ? zbase + fixed : zbase + r0;
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+          "[%5];" ::"r"(dst),
+          "l"(map), "r"(kx0), "r"(y), "r"(z), "r"(b)
+          : "memory");
+    }
+  }
+  __syncthreads();  // the barrier is initialised before anyone waits on it
+  bool done = false;
+  const uint64_t t0 = globaltimer_ns();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(b)
+        : "memory");
+    if (ok) {
+      done = true;
+      break;
+    }
+    if (globaltimer_ns() - t0 > 2000000000ull) break;
+  }
+  if (!done && threadIdx.x == 0) atomicOr(err, DEV_ERR_TMA_TIMEOUT);
+  return __syncthreads_and(done) != 0;
+}
+
+// In-place length-N transform of the CTX columns of a [N][CTX] tile (element
+// j of column c at tile[j * CTX + c]); natural order in and out.
+template <int LOGN, bool INV>
+__device__ __forceinline__ void pencil_fft(float2* tile, const float2* s_tw) {
+  using S = fftr::Split<LOGN>;
+  constexpr int N = S::N, N1 = S::N1, N2 = S::N2, R = S::R, CTX = Pencil<LOGN>::CTX;
+  const int c = threadIdx.x % CTX, t = threadIdx.x / CTX;  // t in [0, N2)
+  // stage 1: thread t = j2 holds x[N2 j1 + j2], j1 < N1
+  float2 v[N1];
+#pragma unroll
+  for (int j1 = 0; j1 < N1; ++j1) v[j1] = tile[(N2 * j1 + t) * CTX + c];
+  fftr::dft<N1, INV>(v);
+#pragma unroll
+  for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], twiddle(s_tw, (t * k1) & (N - 1), N, INV));
+  __syncthreads();
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) tile[(k1 * N2 + t) * CTX + c] = v[k1];
+  __syncthreads();
+  // stage 2: N2-point transforms over j2 for k1 = t + N2 r
+  float2 w[R][N2];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int k1 = t + N2 * r;
+#pragma unroll
+    for (int j2 = 0; j2 < N2; ++j2) w[r][j2] = tile[(k1 * N2 + j2) * CTX + c];
+    fftr::dft<N2, INV>(w[r]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int k1 = t + N2 * r;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) tile[(k1 + N1 * k2) * CTX + c] = w[r][k2];
+  }
+  __syncthreads();
+}
+
+// Shared memory of a pencil kernel: `tiles` tiles, the N/2 twiddles, the barrier.
+template <int LOGN> constexpr size_t pencil_smem(int tiles) {
+  return (size_t)tiles * Pencil<LOGN>::N * Pencil<LOGN>::CTX * sizeof(float2) +
+         (size_t)(Pencil<LOGN>::N / 2 > 0 ? Pencil<LOGN>::N / 2 : 1) * sizeof(float2) + 16;
+}
+
+// Store the valid columns (kx < nh) of a tile back to [comp][z][y][kx].
+template <int LOGN>
+__device__ __forceinline__ void store_pencil(const float2* tile, float2* __restrict__ data, int axis, int kx0,
+                                             int fixed, int comp, int nh, int nhp) {
+  using P = Pencil<LOGN>;
+  const int64_t plane = (int64_t)P::N * nhp;
+  float2* base = data + (int64_t)comp * P::N * plane;
+  for (int idx = threadIdx.x; idx < P::N * P::CTX; idx += blockDim.x) {
+    const int r = idx / P::CTX, c = idx % P::CTX, kx = kx0 + c;
+    if (kx >= nh) continue;
+    const int64_t a = axis == 0 ? fixed * plane + (int64_t)r * nhp + kx : r * plane + (int64_t)fixed * nhp + kx;
+    base[a] = tile[idx];
+  }
+}
+
+template <int LOGN>
+__device__ __forceinline__ void pencil_layout(unsigned char* sm, float2*& tile, float2*& tile2, float2*& s_tw,
+                                              uint64_t*& bar, int tiles) {
+  using P = Pencil<LOGN>;
+  tile = reinterpret_cast<float2*>(sm);
+  tile2 = tiles > 1 ? tile + P::N * P::CTX : nullptr;
+  s_tw = tile + (size_t)tiles * P::N * P::CTX;
+  bar = reinterpret_cast<uint64_t*>(s_tw + (P::N / 2 > 0 ? P::N / 2 : 1));
+}
+
+// c2c pass along y (axis 0) or z (axis 1) of ncomp half spectra, in place.
+template <int LOGN, bool INV>
+__global__ void __launch_bounds__(Pencil<LOGN>::THREADS) k_pencil(const __grid_constant__ CUtensorMap map,
+                                                                  float2* __restrict__ data, int axis, int nh,
+                                                                  int nhp, const float2* __restrict__ tw,
+                                                                  uint32_t* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char psm[];
+  float2 *tile, *tile2, *s_tw;
+  uint64_t* bar;
+  pencil_layout<LOGN>(psm, tile, tile2, s_tw, bar, 1);
+  load_twiddles(s_tw, tw, Pencil<LOGN>::N);
+  const int kx0 = blockIdx.x * Pencil<LOGN>::CTX, fixed = blockIdx.y, comp = blockIdx.z;
+  if (!stage_pencil<LOGN>(tile, bar, &map, axis, kx0, fixed, comp * Pencil<LOGN>::N, err)) return;
+  pencil_fft<LOGN, INV>(tile, s_tw);
+  store_pencil<LOGN>(tile, data, axis, kx0, fixed, comp, nh, nhp);
+}
+
+// Forward z pass, Green's function x filter x gradient, and the inverse z
+// passes of the ncomp components (4: the potential itself as well).
+template <int LOGN>
+__global__ void __launch_bounds__(Pencil<LOGN>::THREADS) k_pencil_poisson(
+    const __grid_constant__ CUtensorMap map, float2* __restrict__ spec3, int nh, int nhp,
+    const float2* __restrict__ tw, const float* __restrict__ kval, const float* __restrict__ kfilter,
+    const float* __restrict__ kderiv, float kcoef, int ncomp, uint32_t* __restrict__ err) {
+  using P = Pencil<LOGN>;
+  extern __shared__ __align__(128) unsigned char psm[];
+  float2 *tile, *phi, *s_tw;
+  uint64_t* bar;
+  pencil_layout<LOGN>(psm, tile, phi, s_tw, bar, 2);
+  load_twiddles(s_tw, tw, P::N);
+  const int kx0 = blockIdx.x * P::CTX, y = blockIdx.y;
+  if (!stage_pencil<LOGN>(tile, bar, &map, 1, kx0, y, 0, err)) return;
+  pencil_fft<LOGN, false>(tile, s_tw);
+  // phi(k) = rho(k) kcoef W(k) / k^2
+  for (int idx = threadIdx.x; idx < P::N * P::CTX; idx += blockDim.x) {
+    const int z = idx / P::CTX, kx = kx0 + idx % P::CTX;
+    float2 v = make_float2(0.f, 0.f);
+    if (kx < nh) {
+      const float k2 = kval[kx] * kval[kx] + kval[y] * kval[y] + kval[z] * kval[z];
+      if (k2 > 0.f) {
+        const float sc = kcoef * kfilter[kx] * kfilter[y] * kfilter[z] / k2;
+        v = make_float2(tile[idx].x * sc, tile[idx].y * sc);
+      }
+    }
+    phi[idx] = v;
+  }
+  __syncthreads();
+  for (int comp = 0; comp < ncomp; ++comp) {
+    for (int idx = threadIdx.x; idx < P::N * P::CTX; idx += blockDim.x) {
+      const int z = idx / P::CTX, kx = min(kx0 + idx % P::CTX, nh - 1);
+      const float2 ph = phi[idx];
+      if (comp == 3) {  // the potential itself
+        tile[idx] = ph;
+        continue;
+      }
+      const float d = comp == 0 ? kderiv[kx] : (comp == 1 ? kderiv[y] : kderiv[z]);
+      tile[idx] = make_float2(d * ph.y, -d * ph.x);  // -i D phi
+    }
+    __syncthreads();
+    pencil_fft<LOGN, true>(tile, s_tw);
+    store_pencil<LOGN>(tile, spec3, 1, kx0, y, comp, nh, nhp);
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ double pk_sinc(int k, int nm) {
+  if (k == 0) return 1.0;
+  const double x = (double)k / (double)nm;
+  return sinpi(x) / (M_PI * x);
+}
+
+// Forward z pass of the half spectrum, then every mode into its |k| shell:
+// sum of |rho_k|^2 / W^2 and the mode count, modes with 0 < kx < nm/2 twice
+// (their conjugates are not stored), as power_spectrum.rs:74-110 over the full
+// cube.
+template <int LOGN>
+__global__ void __launch_bounds__(Pencil<LOGN>::THREADS) k_pencil_pk(
+    const __grid_constant__ CUtensorMap map, int nh, const float2* __restrict__ tw, double* __restrict__ pk_sum,
+    unsigned long long* __restrict__ pk_n, uint32_t* __restrict__ err) {
+  using P = Pencil<LOGN>;
+  constexpr int nm = P::N, nb = P::N / 2;
+  extern __shared__ __align__(128) unsigned char psm[];
+  float2 *tile, *unused, *s_tw;
+  uint64_t* bar;
+  pencil_layout<LOGN>(psm, tile, unused, s_tw, bar, 1);
+  double* hs = reinterpret_cast<double*>(psm + pencil_smem<LOGN>(1));
+  unsigned long long* hn = reinterpret_cast<unsigned long long*>(hs + nb);
+  load_twiddles(s_tw, tw, nm);
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    hs[i] = 0.0;
+    hn[i] = 0ull;
+  }
+  const int kx0 = blockIdx.x * P::CTX, y = blockIdx.y;
+  if (!stage_pencil<LOGN>(tile, bar, &map, 1, kx0, y, 0, err)) return;
+  pencil_fft<LOGN, false>(tile, s_tw);
+  const int fy = y <= nb ? y : y - nm;
+  for (int idx = threadIdx.x; idx < nm * P::CTX; idx += blockDim.x) {
+    const int z = idx / P::CTX, kx = kx0 + idx % P::CTX;
+    if (kx >= nh) continue;
+    const int fz = z <= nb ? z : z - nm;
+    const double k2 = (double)kx * kx + (double)fy * fy + (double)fz * fz;
+    if (k2 == 0.0) continue;
+    const double bf = sqrt(k2) - 0.5;
+    if (bf < 0.0 || bf >= (double)nb) continue;
+    const int bin = (int)bf;
+    const double w = pk_sinc(kx, nm) * pk_sinc(fy, nm) * pk_sinc(fz, nm);
+    const double re = tile[idx].x, im = tile[idx].y;
+    const int mult = (kx == 0 || kx == nb) ? 1 : 2;
+    atomicAdd(&hs[bin], mult * (re * re + im * im) / (w * w));
+    atomicAdd(&hn[bin], (unsigned long long)mult);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    if (hn[i]) {
+      atomicAdd(&pk_sum[i], hs[i]);
+      atomicAdd(&pk_n[i], hn[i]);
+    }
 }
 
 // ---- CIC deposit (cic.rs:37-93) ------------------------------------------------
@@ -242,184 +422,178 @@ __global__ void k_cells(const uint32_t* __restrict__ qx, const uint32_t* __restr
 // Inverse: Z[k] = X[k] (1 + i W_k) + conj(X[h-k]) (1 - i W_k), W_k =
 // e^{2 pi i k/nm}, k < h; the unnormalised inverse of Z gives x[2j] and
 // x[2j+1] as its real and imaginary parts (the row spectrum is Hermitian, so
-// X[0] and X[h] are real up to rounding).  Shared memory: the nm/2 twiddles of
-// length nm, the h/2 of length h, two work rows of h per row.
-__device__ __forceinline__ void load_x_twiddles(float2* s_tw, float2* s_th, const float2* tw, int nm) {
-  const int h = nm >> 1;
-  for (int i = threadIdx.x; i < h; i += blockDim.x) s_tw[i] = tw[i];
-  for (int i = threadIdx.x; i < (h >> 1); i += blockDim.x) s_th[i] = tw[2 * i];
-}
+// X[0] and X[h] are real up to rounding).
+//
+// RX rows per block, N2 threads per row (Split<log2 h>).  The block's input
+// rows are one contiguous range of global memory: one bulk copy (no tensor
+// map) stages them in shared memory.  Stage 1 reads a row's elements from
+// there; the exchange between the stages goes through a padded buffer (row of
+// N2 x (N1 + 1)), so neither stage's shared-memory accesses collide in a bank.
 
-__global__ void k_fft_x_r2c(const float* __restrict__ rho, float2* __restrict__ spec, int nm, int logn, int nh,
-                            int rows, int64_t nrows, const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  const int h = nm >> 1;
-  float2* s_tw = sm;
-  float2* s_th = sm + h;
-  float2* a = s_th + (h >> 1 > 0 ? h >> 1 : 1);
-  float2* b = a + rows * h;
-  load_x_twiddles(s_tw, s_th, tw, nm);
-  const int64_t row0 = (int64_t)blockIdx.x * rows;
-  const float2* src = reinterpret_cast<const float2*>(rho);
-  for (int idx = threadIdx.x; idx < rows * h; idx += blockDim.x) {
-    const int r = idx / h, j = idx % h;
-    a[idx] = row0 + r < nrows ? src[(row0 + r) * h + j] : make_float2(0.f, 0.f);
+template <int LOGH> struct RowPass {
+  using S = fftr::Split<LOGH>;
+  static constexpr int H = 1 << LOGH;
+  static constexpr int RX = 256 / S::N2 > 0 ? 256 / S::N2 : 1;  // rows per block: 256 threads
+  static constexpr int THREADS = RX * S::N2;
+  static constexpr int YP = S::N2 * (S::N1 + 1);  // padded exchange row
+};
+
+// One bulk copy of `bytes` contiguous bytes into shared memory; false (and
+// DEV_ERR_TMA_TIMEOUT) when it does not complete within 2 s.
+__device__ bool stage_bulk(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint32_t* err) {
+  const uint32_t b = smem_u32(bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(b)
+                 : "memory");
   }
   __syncthreads();
-  const float2* res = fft_smem<true>(a, b, h, logn - 1, rows, s_th, false);
-  for (int idx = threadIdx.x; idx < rows * nh; idx += blockDim.x) {
-    const int r = idx / nh, k = idx % nh;
-    if (row0 + r >= nrows) continue;
-    const float2 zk = res[r * h + (k == h ? 0 : k)];
-    const float2 zm = res[r * h + (k == 0 || k == h ? 0 : h - k)];
+  bool done = false;
+  const uint64_t t0 = globaltimer_ns();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(b)
+        : "memory");
+    if (ok) {
+      done = true;
+      break;
+    }
+    if (globaltimer_ns() - t0 > 2000000000ull) break;
+  }
+  if (!done && threadIdx.x == 0) atomicOr(err, DEV_ERR_TMA_TIMEOUT);
+  return __syncthreads_and(done) != 0;
+}
+
+// Real rows of nm samples -> half spectra (pitch nhp): the half-length
+// transform of the packed row, then the even / odd split above.
+template <int LOGH>
+__global__ void __launch_bounds__(RowPass<LOGH>::THREADS) k_row_r2c(const float* __restrict__ rho,
+                                                                   float2* __restrict__ spec, int nhp,
+                                                                   int64_t nrows, const float2* __restrict__ tw,
+                                                                   uint32_t* __restrict__ err) {
+  using RP = RowPass<LOGH>;
+  using S = typename RP::S;
+  constexpr int H = RP::H, N1 = S::N1, N2 = S::N2, R = S::R, RX = RP::RX, NM = 2 * H;
+  extern __shared__ __align__(128) unsigned char rsm[];
+  float2* rows = reinterpret_cast<float2*>(rsm);             // RX x H (input, then the transform)
+  float2* ybuf = rows + RX * H;                              // RX x YP
+  float2* s_tw = ybuf + RX * RP::YP;                         // NM / 2 twiddles of length NM
+  uint64_t* bar = reinterpret_cast<uint64_t*>(s_tw + NM / 2);
+  for (int i = threadIdx.x; i < NM / 2; i += blockDim.x) s_tw[i] = tw[i];
+  const int64_t row0 = (int64_t)blockIdx.x * RX;
+  const int nr = (int)min((int64_t)RX, nrows - row0);
+  if (!stage_bulk(rows, rho + row0 * NM, (uint32_t)(nr * NM * sizeof(float)), bar, err)) return;
+  const int rr = threadIdx.x / N2, t = threadIdx.x % N2;
+  float2 out[R][N2];
+  const float2* row = rows + rr * H;
+  {
+    float2 v[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; ++j1) v[j1] = row[N2 * j1 + t];
+    fftr::dft<N1, false>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], twiddle(s_tw, 2 * ((t * k1) & (H - 1)), NM, false));
+    float2* yb = ybuf + rr * RP::YP;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) yb[k1 + t * (N1 + 1)] = v[k1];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int k1 = t + N2 * r;
+#pragma unroll
+      for (int j2 = 0; j2 < N2; ++j2) out[r][j2] = yb[k1 + j2 * (N1 + 1)];
+      fftr::dft<N2, false>(out[r]);
+    }
+  }
+  __syncthreads();
+  // Z[k] in natural order into the row buffer
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) rows[rr * H + (t + N2 * r) + N1 * k2] = out[r][k2];
+  __syncthreads();
+  // split: X[k] = E + w_NM^k O, k = 0..H
+  for (int idx = threadIdx.x; idx < nr * (H + 1); idx += blockDim.x) {
+    const int r = idx / (H + 1), k = idx % (H + 1);
+    const float2 zk = rows[r * H + (k == H ? 0 : k)];
+    const float2 zm = rows[r * H + (k == 0 || k == H ? 0 : H - k)];
     const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-    const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));  // (Zk - conj Zm) / 2i
-    spec[(row0 + r) * nh + k] = cadd(e, cmul(twiddle(s_tw, k, nm, false), o));
+    const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    spec[(row0 + r) * nhp + k] = cadd(e, cmul(twiddle(s_tw, k, NM, false), o));
   }
 }
 
-__global__ void k_fft_x_c2r(const float2* __restrict__ spec3, float* __restrict__ force, int nm, int logn, int nh,
-                            int rows, int64_t nrows, const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  const int h = nm >> 1;
-  float2* s_tw = sm;
-  float2* s_th = sm + h;
-  float2* a = s_th + (h >> 1 > 0 ? h >> 1 : 1);
-  float2* b = a + rows * h;
-  load_x_twiddles(s_tw, s_th, tw, nm);
-  __syncthreads();  // the unpacking below reads s_tw
+// Half spectra (pitch nhp) of ncomp components -> real rows: the merge
+// above, the inverse half-length transform, real / imaginary parts as the
+// even / odd samples.
+template <int LOGH>
+__global__ void __launch_bounds__(RowPass<LOGH>::THREADS) k_row_c2r(const float2* __restrict__ spec3,
+                                                                   float* __restrict__ force, int nhp,
+                                                                   int64_t nrows, const float2* __restrict__ tw,
+                                                                   uint32_t* __restrict__ err) {
+  using RP = RowPass<LOGH>;
+  using S = typename RP::S;
+  constexpr int H = RP::H, N1 = S::N1, N2 = S::N2, R = S::R, RX = RP::RX, NM = 2 * H;
+  extern __shared__ __align__(128) unsigned char rsm[];
+  float2* rows = reinterpret_cast<float2*>(rsm);  // RX x nhp (input spectra)
+  float2* ybuf = rows + (size_t)RX * nhp;         // RX x YP
+  float2* s_tw = ybuf + RX * RP::YP;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(s_tw + NM / 2);
+  for (int i = threadIdx.x; i < NM / 2; i += blockDim.x) s_tw[i] = tw[i];
   const int comp = blockIdx.y;
-  const float2* in = spec3 + comp * nrows * nh;
-  float2* out = reinterpret_cast<float2*>(force + comp * nrows * nm);
-  const int64_t row0 = (int64_t)blockIdx.x * rows;
-  for (int idx = threadIdx.x; idx < rows * h; idx += blockDim.x) {
-    const int r = idx / h, k = idx % h;
-    float2 z = make_float2(0.f, 0.f);
-    if (row0 + r < nrows) {
-      float2 xk = in[(row0 + r) * nh + k];
-      float2 xm = in[(row0 + r) * nh + (h - k)];
-      if (k == 0) xk.y = xm.y = 0.f;  // the real part of the full inverse: Im X[0], Im X[h] drop out
-      const float2 w = twiddle(s_tw, k, nm, true);  // e^{+2 pi i k / nm}
-      // X[k] (1 + i W) + conj(X[h - k]) (1 - i W)
-      const float2 p = make_float2(1.f - w.y, w.x), q = make_float2(1.f + w.y, -w.x);
-      z = cadd(cmul(xk, p), cmul(make_float2(xm.x, -xm.y), q));
-    }
-    a[idx] = z;
-  }
+  const float2* in = spec3 + (int64_t)comp * nrows * nhp;
+  float2* out_rows = reinterpret_cast<float2*>(force + (int64_t)comp * nrows * NM);
+  const int64_t row0 = (int64_t)blockIdx.x * RX;
+  const int nr = (int)min((int64_t)RX, nrows - row0);
+  if (!stage_bulk(rows, in + row0 * nhp, (uint32_t)(nr * nhp * sizeof(float2)), bar, err)) return;
+  const int rr = threadIdx.x / N2, t = threadIdx.x % N2;
+  const float2* X = rows + (size_t)rr * nhp;
+  // Z[k] = X[k] (1 + i W) + conj(X[h - k]) (1 - i W), W = w_NM^-k; Im X[0], Im X[h] drop out
+  auto zin = [&](int k) {
+    float2 xk = X[k], xm = X[H - k];
+    if (k == 0) xk.y = xm.y = 0.f;
+    const float2 w = twiddle(s_tw, k, NM, true);
+    const float2 p = make_float2(1.f - w.y, w.x), q = make_float2(1.f + w.y, -w.x);
+    return cadd(cmul(xk, p), cmul(make_float2(xm.x, -xm.y), q));
+  };
+  float2 v[N1];
+#pragma unroll
+  for (int j1 = 0; j1 < N1; ++j1) v[j1] = rr < nr ? zin(N2 * j1 + t) : make_float2(0.f, 0.f);
+  fftr::dft<N1, true>(v);
+#pragma unroll
+  for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], twiddle(s_tw, 2 * ((t * k1) & (H - 1)), NM, true));
+  float2* yb = ybuf + rr * RP::YP;
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) yb[k1 + t * (N1 + 1)] = v[k1];
   __syncthreads();
-  const float2* res = fft_smem<true>(a, b, h, logn - 1, rows, s_th, true);
-  for (int idx = threadIdx.x; idx < rows * h; idx += blockDim.x) {
-    const int r = idx / h, j = idx % h;
-    if (row0 + r < nrows) out[(row0 + r) * h + j] = res[idx];
+  float2 o[R][N2];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int k1 = t + N2 * r;
+#pragma unroll
+    for (int j2 = 0; j2 < N2; ++j2) o[r][j2] = yb[k1 + j2 * (N1 + 1)];
+    fftr::dft<N2, true>(o[r]);
+  }
+  if (rr < nr) {
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) out_rows[(row0 + rr) * H + (t + N2 * r) + N1 * k2] = o[r][k2];
   }
 }
 
-// ---- y pass (c2c) on [z][y][kx] half spectra, one component per blockIdx.z --------
-__global__ void k_fft_y(float2* __restrict__ spec, int64_t comp_stride, int nm, int logn, int nh, int tx,
-                        const float2* __restrict__ tw, int inv) {
-  extern __shared__ float2 sm[];
-  float2* s_tw = sm;
-  float2* a = sm + (nm >> 1);
-  float2* b = a + nm * tx;
-  load_twiddles(s_tw, tw, nm);
-  const int kx0 = blockIdx.x * tx, z = blockIdx.y;
-  float2* base = spec + blockIdx.z * comp_stride + (int64_t)z * nm * nh;
-  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-    const int y = idx / tx, c = idx % tx;
-    a[idx] = (kx0 + c < nh) ? base[(int64_t)y * nh + kx0 + c] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  const float2* res = fft_smem<false>(a, b, nm, logn, tx, s_tw, inv != 0);
-  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-    const int y = idx / tx, c = idx % tx;
-    if (kx0 + c < nh) base[(int64_t)y * nh + kx0 + c] = res[idx];
-  }
-}
-
-// ---- z pass (c2c) on [z][y][kx] half spectra, one component per blockIdx.z --------
-__global__ void k_fft_z_c2c(float2* __restrict__ spec, int64_t comp_stride, int nm, int logn, int nh, int tx,
-                            const float2* __restrict__ tw, int inv) {
-  extern __shared__ float2 sm[];
-  float2* s_tw = sm;
-  float2* a = sm + (nm >> 1);
-  float2* b = a + nm * tx;
-  load_twiddles(s_tw, tw, nm);
-  const int kx0 = blockIdx.x * tx, y = blockIdx.y;
-  const int64_t plane = (int64_t)nm * nh;
-  float2* base = spec + blockIdx.z * comp_stride + (int64_t)y * nh;
-  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-    const int z = idx / tx, c = idx % tx;
-    a[idx] = (kx0 + c < nh) ? base[z * plane + kx0 + c] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  const float2* res = fft_smem<false>(a, b, nm, logn, tx, s_tw, inv != 0);
-  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-    const int z = idx / tx, c = idx % tx;
-    if (kx0 + c < nh) base[z * plane + kx0 + c] = res[idx];
-  }
-}
-
-// ---- z pass + Green's function x filter x gradient + inverse z pass ---------------
-__global__ void k_fft_z_poisson(const float2* __restrict__ spec, float2* __restrict__ spec3, int nm, int logn,
-                                int nh, int tx, const float2* __restrict__ tw, const float* __restrict__ kval,
-                                const float* __restrict__ kfilter, const float* __restrict__ kderiv, float kcoef,
-                                int ncomp) {
-  extern __shared__ float2 sm[];
-  float2* s_tw = sm;
-  float2* a = sm + (nm >> 1);
-  float2* b = a + nm * tx;
-  float2* c3 = b + nm * tx;
-  load_twiddles(s_tw, tw, nm);
-  const int kx0 = blockIdx.x * tx, y = blockIdx.y;
-  const int64_t plane = (int64_t)nm * nh;
-  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-    const int z = idx / tx, c = idx % tx;
-    a[idx] = (kx0 + c < nh) ? spec[z * plane + (int64_t)y * nh + kx0 + c] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  float2* rho_k = fft_smem<false>(a, b, nm, logn, tx, s_tw, false);
-  float2* spare = rho_k == a ? b : a;
-  // phi(k) = rho(k) * kcoef * W(k) / k^2 ; F_a = -i D_a phi
-  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-    const int z = idx / tx, c = idx % tx;
-    const int kx = kx0 + c;
-    float2 v = make_float2(0.f, 0.f);
-    if (kx < nh) {
-      const float k2 = kval[kx] * kval[kx] + kval[y] * kval[y] + kval[z] * kval[z];
-      if (k2 > 0.f) {
-        const float s = kcoef * kfilter[kx] * kfilter[y] * kfilter[z] / k2;
-        v = make_float2(rho_k[idx].x * s, rho_k[idx].y * s);
-      }
-    }
-    rho_k[idx] = v;  // phi
-  }
-  __syncthreads();
-  for (int comp = 0; comp < ncomp; ++comp) {
-    for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-      const int z = idx / tx, c = idx % tx;
-      const int kx = kx0 + c < nh ? kx0 + c : 0;
-      const float2 ph = rho_k[idx];
-      if (comp == 3) {  // the potential itself
-        c3[idx] = ph;
-        continue;
-      }
-      const float d = comp == 0 ? kderiv[kx] : (comp == 1 ? kderiv[y] : kderiv[z]);
-      c3[idx] = make_float2(d * ph.y, -d * ph.x);
-    }
-    __syncthreads();
-    const float2* res = fft_smem<false>(c3, spare, nm, logn, tx, s_tw, true);
-    float2* out = spec3 + comp * (int64_t)nm * plane;
-    for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-      const int z = idx / tx, c = idx % tx;
-      if (kx0 + c < nh) out[z * plane + (int64_t)y * nh + kx0 + c] = res[idx];
-    }
-    __syncthreads();
-    if (res == spare) {  // keep c3 as the scratch input of the next component
-      float2* t = spare;
-      spare = c3;
-      c3 = t;
-    }
-  }
+template <int LOGH> constexpr size_t row_smem(int cols) {
+  return ((size_t)RowPass<LOGH>::RX * cols + (size_t)RowPass<LOGH>::RX * RowPass<LOGH>::YP + RowPass<LOGH>::H) *
+             sizeof(float2) + 16;
 }
 
 // ---- gather (cic.rs:100-170) fused with the sum LR + SR and the kick -------------
@@ -559,94 +733,128 @@ __global__ void k_pk_deposit_q(const uint32_t* __restrict__ qx, const uint32_t* 
   pk_add_aggregated(live, idx, w, rho);
 }
 
-__device__ __forceinline__ double pk_sinc(int k, int nm) {
-  if (k == 0) return 1.0;
-  const double x = (double)k / (double)nm;
-  return sinpi(x) / (M_PI * x);
-}
+// ---- pencil launches, one instantiation per transform length (4 .. 1024) ------------
+enum PencilOp { PEN_Y_FWD, PEN_Y_INV, PEN_Z_FWD, PEN_Z_INV, PEN_POISSON, PEN_PK };
 
-// Forward z pass of the half spectrum, then every mode into its |k| shell:
-// sum of |rho_k|^2 / W^2 and the mode count, modes with 0 < kx < nm/2 twice
-// (their conjugates are not stored), as power_spectrum.rs:74-110 over the full
-// cube.
-__global__ void k_fft_z_pk(const float2* __restrict__ spec, int nm, int logn, int nh, int tx,
-                           const float2* __restrict__ tw, double* __restrict__ pk_sum,
-                           unsigned long long* __restrict__ pk_n) {
-  extern __shared__ float2 sm[];
-  float2* s_tw = sm;
-  float2* a = sm + (nm >> 1);
-  float2* b = a + nm * tx;
-  double* hs = reinterpret_cast<double*>(b + nm * tx);
-  unsigned long long* hn = reinterpret_cast<unsigned long long*>(hs + (nm >> 1));
-  load_twiddles(s_tw, tw, nm);
-  for (int i = threadIdx.x; i < (nm >> 1); i += blockDim.x) {
-    hs[i] = 0.0;
-    hn[i] = 0ull;
-  }
-  const int kx0 = blockIdx.x * tx, y = blockIdx.y;
-  const int64_t plane = (int64_t)nm * nh;
-  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-    const int z = idx / tx, c = idx % tx;
-    a[idx] = (kx0 + c < nh) ? spec[z * plane + (int64_t)y * nh + kx0 + c] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  const float2* res = fft_smem<false>(a, b, nm, logn, tx, s_tw, false);
-  const int nb = nm >> 1;
-  const int fy = y <= nb ? y : y - nm;
-  for (int idx = threadIdx.x; idx < nm * tx; idx += blockDim.x) {
-    const int z = idx / tx, c = idx % tx;
-    const int kx = kx0 + c;
-    if (kx >= nh) continue;
-    const int fz = z <= nb ? z : z - nm;
-    const double k2 = (double)kx * kx + (double)fy * fy + (double)fz * fz;
-    if (k2 == 0.0) continue;
-    const double bf = sqrt(k2) - 0.5;
-    if (bf < 0.0 || bf >= (double)nb) continue;
-    const int bin = (int)bf;
-    const double w = pk_sinc(kx, nm) * pk_sinc(fy, nm) * pk_sinc(fz, nm);
-    const double re = res[idx].x, im = res[idx].y;
-    const int mult = (kx == 0 || kx == nb) ? 1 : 2;
-    atomicAdd(&hs[bin], mult * (re * re + im * im) / (w * w));
-    atomicAdd(&hn[bin], (unsigned long long)mult);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nb; i += blockDim.x)
-    if (hn[i]) {
-      atomicAdd(&pk_sum[i], hs[i]);
-      atomicAdd(&pk_n[i], hn[i]);
+template <int LOGN>
+void pencil_launch_t(const PmPlan& p, PencilOp op, int ncomp, double* pk_sum, unsigned long long* pk_n,
+                     cudaStream_t s) {
+  using P = Pencil<LOGN>;
+  const int nm = p.nm, ntx = (p.nh + P::CTX - 1) / P::CTX;
+  const CUtensorMap* spec_y = reinterpret_cast<const CUtensorMap*>(p.tmap[0]);
+  const CUtensorMap* spec_z = reinterpret_cast<const CUtensorMap*>(p.tmap[1]);
+  const CUtensorMap* spec3_y = reinterpret_cast<const CUtensorMap*>(p.tmap[2]);
+  const CUtensorMap* spec3_z = reinterpret_cast<const CUtensorMap*>(p.tmap[3]);
+  const size_t sm1 = pencil_smem<LOGN>(1), sm2 = pencil_smem<LOGN>(2);
+  switch (op) {
+    case PEN_Y_FWD:
+    case PEN_Z_FWD: {
+      auto k = k_pencil<LOGN, false>;
+      TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+      k<<<dim3(ntx, nm, 1), P::THREADS, sm1, s>>>(op == PEN_Y_FWD ? *spec_y : *spec_z, p.spec,
+                                                  op == PEN_Y_FWD ? 0 : 1, p.nh, p.nhp, p.twiddle, p.err);
+      break;
     }
+    case PEN_Y_INV:
+    case PEN_Z_INV: {
+      auto k = k_pencil<LOGN, true>;
+      TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+      k<<<dim3(ntx, nm, ncomp), P::THREADS, sm1, s>>>(op == PEN_Y_INV ? *spec3_y : *spec3_z, p.spec3,
+                                                      op == PEN_Y_INV ? 0 : 1, p.nh, p.nhp, p.twiddle, p.err);
+      break;
+    }
+    case PEN_POISSON: {
+      auto k = k_pencil_poisson<LOGN>;
+      TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+      k<<<dim3(ntx, nm), P::THREADS, sm2, s>>>(*spec_z, p.spec3, p.nh, p.nhp, p.twiddle, p.kval, p.kfilter,
+                                               p.kderiv, p.kcoef, p.ncomp, p.err);
+      break;
+    }
+    case PEN_PK: {
+      auto k = k_pencil_pk<LOGN>;
+      const size_t smk = sm1 + (sizeof(double) + sizeof(unsigned long long)) * (size_t)(nm / 2);
+      TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smk));
+      k<<<dim3(ntx, nm), P::THREADS, smk, s>>>(*spec_z, p.nh, p.twiddle, pk_sum, pk_n, p.err);
+      break;
+    }
+  }
+  TPM_LAUNCH_CHECK();
 }
 
-// Threads per block of the FFT passes: the passes loop over their butterflies
-// by blockDim, and 512 threads hide the shared-memory latency of the 2-3
-// resident blocks per SM better than 256 (PM 2.04 -> 1.67 ms at 256^3) or 1024.
-constexpr int FFT_THREADS = 512;
-
-// Full-length rows and columns (y, z passes) per block: 2048 elements per block
-// (8 x 8 at nm = 256: PM 1.67 -> 1.61 ms against 16 x 16; 32-wide tiles are
-// slower), at least 8 columns so a block still reads 64-byte runs.
-inline int rows_for(int nm) {
-  int r = nm >= 2048 ? 1 : 2048 / nm;
-  return r > nm * nm ? nm * nm : r;
+void pencil_launch(const PmPlan& p, PencilOp op, int ncomp = 1, double* pk_sum = nullptr,
+                   unsigned long long* pk_n = nullptr, cudaStream_t s = 0) {
+  switch (p.logn) {
+    case 2: pencil_launch_t<2>(p, op, ncomp, pk_sum, pk_n, s); break;
+    case 3: pencil_launch_t<3>(p, op, ncomp, pk_sum, pk_n, s); break;
+    case 4: pencil_launch_t<4>(p, op, ncomp, pk_sum, pk_n, s); break;
+    case 5: pencil_launch_t<5>(p, op, ncomp, pk_sum, pk_n, s); break;
+    case 6: pencil_launch_t<6>(p, op, ncomp, pk_sum, pk_n, s); break;
+    case 7: pencil_launch_t<7>(p, op, ncomp, pk_sum, pk_n, s); break;
+    case 8: pencil_launch_t<8>(p, op, ncomp, pk_sum, pk_n, s); break;
+    case 9: pencil_launch_t<9>(p, op, ncomp, pk_sum, pk_n, s); break;
+    case 10: pencil_launch_t<10>(p, op, ncomp, pk_sum, pk_n, s); break;
+    default: throw Error(TPM_ERR_INVALID_ARGUMENT, "mesh size outside 4..1024");
+  }
 }
-inline int tx_for(int nm) {
-  int t = 2048 / nm;
-  return t < 8 ? 8 : (t > 16 ? 16 : t);
+
+// ---- x-pass launches (rows of h = nm/2 packed complex values) ---------------------
+template <int LOGH>
+void row_launch_t(const PmPlan& p, bool forward, int ncomp, cudaStream_t s) {
+  using RP = RowPass<LOGH>;
+  const int64_t nrows = (int64_t)p.nm * p.nm;
+  const unsigned blocks = (unsigned)((nrows + RP::RX - 1) / RP::RX);
+  if (forward) {
+    const size_t sm = row_smem<LOGH>(RP::H);
+    TPM_CUDA(cudaFuncSetAttribute(k_row_r2c<LOGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_row_r2c<LOGH><<<blocks, RP::THREADS, sm, s>>>(p.rho, p.spec, p.nhp, nrows, p.twiddle, p.err);
+  } else {
+    const size_t sm = row_smem<LOGH>(p.nhp);
+    TPM_CUDA(cudaFuncSetAttribute(k_row_c2r<LOGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_row_c2r<LOGH><<<dim3(blocks, ncomp), RP::THREADS, sm, s>>>(p.spec3, p.force, p.nhp, nrows, p.twiddle, p.err);
+  }
+  TPM_LAUNCH_CHECK();
 }
 
-// The x passes: rows per block (the half-length rows of 2048 / nm complex
-// elements each make the same 2048-element tile), shared memory, blocks.
-struct XPass {
-  int rows;
-  size_t smem;
-  int blocks;
-};
-inline XPass x_pass(int nm, int64_t nrows) {
-  const int h = nm >> 1;
-  int rows = rows_for(nm) * 2;
-  if ((int64_t)rows > nrows) rows = (int)nrows;
-  const size_t smem = sizeof(float2) * ((size_t)h + (size_t)(h >> 1 > 0 ? h >> 1 : 1) + 2 * (size_t)rows * h);
-  return XPass{rows, smem, (int)((nrows + rows - 1) / rows)};
+void row_launch(const PmPlan& p, bool forward, int ncomp, cudaStream_t s) {
+  switch (p.logn - 1) {
+    case 1: row_launch_t<1>(p, forward, ncomp, s); break;
+    case 2: row_launch_t<2>(p, forward, ncomp, s); break;
+    case 3: row_launch_t<3>(p, forward, ncomp, s); break;
+    case 4: row_launch_t<4>(p, forward, ncomp, s); break;
+    case 5: row_launch_t<5>(p, forward, ncomp, s); break;
+    case 6: row_launch_t<6>(p, forward, ncomp, s); break;
+    case 7: row_launch_t<7>(p, forward, ncomp, s); break;
+    case 8: row_launch_t<8>(p, forward, ncomp, s); break;
+    case 9: row_launch_t<9>(p, forward, ncomp, s); break;
+    default: throw Error(TPM_ERR_INVALID_ARGUMENT, "mesh size outside 4..1024");
+  }
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once (no libcuda link).
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    TPM_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !f) throw Error(TPM_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }
+  return fn;
+}
+
+// Tensor map of `comps` half spectra [comp * nm + z][y][kx] (8-byte complex
+// elements, rows of nhp): box of ctx columns by `rows_y` y rows by `rows_z` z rows.
+void encode_spectrum_map(void* out, float2* base, int nm, int nhp, int comps, int ctx, int rows_y, int rows_z) {
+  CUtensorMap* m = reinterpret_cast<CUtensorMap*>(out);
+  const cuuint64_t dims[3] = {(cuuint64_t)nhp, (cuuint64_t)nm, (cuuint64_t)nm * (cuuint64_t)comps};
+  const cuuint64_t strides[2] = {(cuuint64_t)nhp * sizeof(float2), (cuuint64_t)nhp * sizeof(float2) * (cuuint64_t)nm};
+  const cuuint32_t box[3] = {(cuuint32_t)ctx, (cuuint32_t)rows_y, (cuuint32_t)rows_z};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode_tiled()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(TPM_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
 
 }  // namespace
@@ -656,9 +864,10 @@ void pm_plan_init(PmPlan& p, int nm, double box, double r_split, uint32_t flags,
   p.nm = nm;
   p.logn = ilog2(nm);
   p.nh = nm / 2 + 1;
+  p.nhp = (p.nh + 1) & ~1;  // even: 16-byte rows
   p.box = box;
   const int64_t nm3 = (int64_t)nm * nm * nm;
-  const int64_t nspec = (int64_t)nm * nm * p.nh;
+  const int64_t nspec = (int64_t)nm * nm * p.nhp;
   std::vector<float2> tw(nm / 2);
   for (int m = 0; m < nm / 2; ++m) {
     const double ang = -2.0 * M_PI * (double)m / (double)nm;
@@ -699,12 +908,26 @@ void pm_plan_init(PmPlan& p, int nm, double box, double r_split, uint32_t flags,
   TPM_CUDA(cudaMemcpy(p.kval, kval.data(), sizeof(float) * nm, cudaMemcpyHostToDevice));
   TPM_CUDA(cudaMemcpy(p.kfilter, kfil.data(), sizeof(float) * nm, cudaMemcpyHostToDevice));
   TPM_CUDA(cudaMemcpy(p.kderiv, kder.data(), sizeof(float) * nm, cudaMemcpyHostToDevice));
-  // shared-memory opt-in for the largest variants
-  const int big = 227 * 1024;
-  TPM_CUDA(cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TPM_CUDA(cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TPM_CUDA(cudaFuncSetAttribute(k_fft_z_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  TPM_CUDA(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  // the padding column (kx = nh) is never written: zero it once
+  TPM_CUDA(cudaMemset(p.spec, 0, sizeof(float2) * nspec));
+  TPM_CUDA(cudaMemset(p.spec3, 0, sizeof(float2) * nspec * p.ncomp));
+  TPM_CUDA(cudaMalloc(&p.err, sizeof(uint32_t)));
+  TPM_CUDA(cudaMemset(p.err, 0, sizeof(uint32_t)));
+  // pencil tiles: ctx columns by min(nm, 256) rows along y or z
+  const int ctx = nm > 512 ? 8 : 16, rows = nm < 256 ? nm : 256;
+  encode_spectrum_map(p.tmap[0], p.spec, nm, p.nhp, 1, ctx, rows, 1);
+  encode_spectrum_map(p.tmap[1], p.spec, nm, p.nhp, 1, ctx, 1, rows);
+  encode_spectrum_map(p.tmap[2], p.spec3, nm, p.nhp, p.ncomp, ctx, rows, 1);
+  encode_spectrum_map(p.tmap[3], p.spec3, nm, p.nhp, p.ncomp, ctx, 1, rows);
+}
+
+void pm_check(const PmPlan& p, cudaStream_t s) {
+  uint32_t e = 0;
+  TPM_CUDA(cudaMemcpyAsync(&e, p.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  TPM_CUDA(cudaStreamSynchronize(s));
+  if (!e) return;
+  TPM_CUDA(cudaMemsetAsync(p.err, 0, sizeof(uint32_t), s));
+  throw Error(TPM_ERR_CUDA, "a transform pass's bulk tensor copy did not complete within its time limit");
 }
 
 void pm_plan_free(PmPlan& p) {
@@ -716,6 +939,7 @@ void pm_plan_free(PmPlan& p) {
   cudaFree(p.spec);
   cudaFree(p.spec3);
   cudaFree(p.force);
+  cudaFree(p.err);
   p = PmPlan();
 }
 
@@ -730,25 +954,11 @@ void pm_deposit(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const u
 }
 
 void pm_solve(const PmPlan& p, cudaStream_t s) {
-  const int nm = p.nm, nh = p.nh, logn = p.logn;
-  const int tx = tx_for(nm);
-  const int64_t nrows = (int64_t)nm * nm;
-  const XPass xp = x_pass(nm, nrows);
-  const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
-  const size_t sm_z = sizeof(float2) * ((size_t)(nm / 2) + 3 * (size_t)nm * tx);
-  const int ntx = (nh + tx - 1) / tx;
-  k_fft_x_r2c<<<xp.blocks, FFT_THREADS, xp.smem, s>>>(p.rho, p.spec, nm, logn, nh, xp.rows, nrows, p.twiddle);
-  TPM_LAUNCH_CHECK();
-  k_fft_y<<<dim3(ntx, nm, 1), FFT_THREADS, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
-  TPM_LAUNCH_CHECK();
-  k_fft_z_poisson<<<dim3(ntx, nm), FFT_THREADS, sm_z, s>>>(p.spec, p.spec3, nm, logn, nh, tx, p.twiddle, p.kval, p.kfilter,
-                                                   p.kderiv, p.kcoef, p.ncomp);
-  TPM_LAUNCH_CHECK();
-  k_fft_y<<<dim3(ntx, nm, p.ncomp), FFT_THREADS, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
-  TPM_LAUNCH_CHECK();
-  k_fft_x_c2r<<<dim3(xp.blocks, p.ncomp), FFT_THREADS, xp.smem, s>>>(p.spec3, p.force, nm, logn, nh, xp.rows, nrows,
-                                                                      p.twiddle);
-  TPM_LAUNCH_CHECK();
+  row_launch(p, true, 1, s);
+  pencil_launch(p, PEN_Y_FWD, 1, nullptr, nullptr, s);
+  pencil_launch(p, PEN_POISSON, p.ncomp, nullptr, nullptr, s);
+  pencil_launch(p, PEN_Y_INV, p.ncomp, nullptr, nullptr, s);
+  row_launch(p, false, p.ncomp, s);
 }
 
 void pm_gather_kick(const PmPlan& p, const GatherArgs& a, cudaStream_t s) {
@@ -768,43 +978,22 @@ void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uin
 }
 
 void pm_forward_real(const PmPlan& p, cudaStream_t s) {
-  const int nm = p.nm, nh = p.nh, logn = p.logn;
-  const int tx = tx_for(nm);
-  const int64_t nrows = (int64_t)nm * nm;
-  const XPass xp = x_pass(nm, nrows);
-  const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
-  TPM_CUDA(cudaFuncSetAttribute(k_fft_z_c2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-  const int ntx = (nh + tx - 1) / tx;
-  k_fft_x_r2c<<<xp.blocks, FFT_THREADS, xp.smem, s>>>(p.rho, p.spec, nm, logn, nh, xp.rows, nrows, p.twiddle);
-  TPM_LAUNCH_CHECK();
-  k_fft_y<<<dim3(ntx, nm, 1), FFT_THREADS, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
-  TPM_LAUNCH_CHECK();
-  k_fft_z_c2c<<<dim3(ntx, nm, 1), FFT_THREADS, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
-  TPM_LAUNCH_CHECK();
+  row_launch(p, true, 1, s);
+  pencil_launch(p, PEN_Y_FWD, 1, nullptr, nullptr, s);
+  pencil_launch(p, PEN_Z_FWD, 1, nullptr, nullptr, s);
 }
 
 void pm_inverse_components(const PmPlan& p, int ncomp, cudaStream_t s) {
-  const int nm = p.nm, nh = p.nh, logn = p.logn;
-  const int tx = tx_for(nm);
-  const int64_t nrows = (int64_t)nm * nm;
-  const XPass xp = x_pass(nm, nrows);
-  const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
-  TPM_CUDA(cudaFuncSetAttribute(k_fft_z_c2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-  const int ntx = (nh + tx - 1) / tx;
-  k_fft_z_c2c<<<dim3(ntx, nm, ncomp), FFT_THREADS, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
-  TPM_LAUNCH_CHECK();
-  k_fft_y<<<dim3(ntx, nm, ncomp), FFT_THREADS, sm_y, s>>>(p.spec3, nrows * nh, nm, logn, nh, tx, p.twiddle, 1);
-  TPM_LAUNCH_CHECK();
-  k_fft_x_c2r<<<dim3(xp.blocks, ncomp), FFT_THREADS, xp.smem, s>>>(p.spec3, p.force, nm, logn, nh, xp.rows, nrows,
-                                                                    p.twiddle);
-  TPM_LAUNCH_CHECK();
+  pencil_launch(p, PEN_Z_INV, ncomp, nullptr, nullptr, s);
+  pencil_launch(p, PEN_Y_INV, ncomp, nullptr, nullptr, s);
+  row_launch(p, false, ncomp, s);
 }
 
 void pm_power_spectrum(const PmPlan& p, const double* pos, const uint32_t* qx, const uint32_t* qy,
                        const uint32_t* qz, const double* mass, int64_t n, double total_mass, double* pk_sum,
                        unsigned long long* pk_n, double* k_out, double* pk_out, unsigned long long* n_out,
                        cudaStream_t s) {
-  const int nm = p.nm, nh = p.nh, logn = p.logn, nb = nm / 2;
+  const int nm = p.nm, nb = nm / 2;
   const int64_t nm3 = (int64_t)nm * nm * nm;
   const double cell = p.box / nm;
   TPM_CUDA(cudaMemsetAsync(p.rho, 0, sizeof(float) * nm3, s));
@@ -818,19 +1007,9 @@ void pm_power_spectrum(const PmPlan& p, const double* pos, const uint32_t* qx, c
                                                                  p.rho);
     TPM_LAUNCH_CHECK();
   }
-  const int tx = tx_for(nm);
-  const int64_t nrows = (int64_t)nm * nm;
-  const XPass xp = x_pass(nm, nrows);
-  const size_t sm_y = sizeof(float2) * ((size_t)(nm / 2) + 2 * (size_t)nm * tx);
-  const size_t sm_pk = sm_y + (sizeof(double) + sizeof(unsigned long long)) * (size_t)nb;
-  TPM_CUDA(cudaFuncSetAttribute(k_fft_z_pk, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-  const int ntx = (nh + tx - 1) / tx;
-  k_fft_x_r2c<<<xp.blocks, FFT_THREADS, xp.smem, s>>>(p.rho, p.spec, nm, logn, nh, xp.rows, nrows, p.twiddle);
-  TPM_LAUNCH_CHECK();
-  k_fft_y<<<dim3(ntx, nm, 1), FFT_THREADS, sm_y, s>>>(p.spec, 0, nm, logn, nh, tx, p.twiddle, 0);
-  TPM_LAUNCH_CHECK();
-  k_fft_z_pk<<<dim3(ntx, nm), FFT_THREADS, sm_pk, s>>>(p.spec, nm, logn, nh, tx, p.twiddle, pk_sum, pk_n);
-  TPM_LAUNCH_CHECK();
+  row_launch(p, true, 1, s);
+  pencil_launch(p, PEN_Y_FWD, 1, nullptr, nullptr, s);
+  pencil_launch(p, PEN_PK, 1, pk_sum, pk_n, s);
   std::vector<double> hs((size_t)nb);
   std::vector<unsigned long long> hn((size_t)nb);
   TPM_CUDA(cudaMemcpyAsync(hs.data(), pk_sum, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));

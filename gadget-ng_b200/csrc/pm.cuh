@@ -8,6 +8,7 @@ namespace tpm {
 
 struct PmPlan {
   int nm = 0, logn = 0, nh = 0;
+  int nhp = 0;                // row pitch of the half spectra: nh rounded up to even (16-byte rows, for TMA)
   double box = 0.0;
   float2* twiddle = nullptr;  // e^{-2 pi i m / nm}, m < nm/2
   float* kfilter = nullptr;   // per-axis factor of the filter (and CIC deconvolution)
@@ -19,12 +20,19 @@ struct PmPlan {
   float* force = nullptr;     // ncomp x nm^3 real, per unit G: -dphi/dx, -dphi/dy, -dphi/dz [, phi]
   int ncomp = 3;              // 4 keeps the long-range potential itself (learned short range)
   float kcoef = 0.f;          // -4 pi / V_cell / N^3
+  uint32_t* err = nullptr;    // device status word (DEV_ERR_TMA_TIMEOUT)
+  // TMA tensor maps (CUtensorMap, 128 bytes each) of the half spectra as
+  // [comp * nm + z][y][kx] arrays of 8-byte complex values: spec and spec3,
+  // each with a y-pencil box (CTX x rows x 1) and a z-pencil box (CTX x 1 x rows)
+  alignas(64) unsigned char tmap[4][128];
 };
 
 // Build tables for mesh nm, box L, split r_s (<= 0: no filter), flags
 // (bit 1 CIC deconvolution, bit 2 four-point gradient, bit 6 keep phi).
 void pm_plan_init(PmPlan& p, int nm, double box, double r_split, uint32_t flags, int device);
 void pm_plan_free(PmPlan& p);
+// Throws if a transform pass recorded an error (a TMA wait past its time limit).
+void pm_check(const PmPlan& p, cudaStream_t s);
 
 struct GatherArgs {
   int64_t n;
@@ -59,11 +67,12 @@ void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uin
 struct Particles;
 
 // Unnormalised forward 3D transform of the real field p.rho into the half
-// spectrum p.spec ([z][y][kx], kx <= nm/2).
+// spectrum p.spec ([z][y][kx], kx <= nm/2, row pitch nhp).
 void pm_forward_real(const PmPlan& p, cudaStream_t s);
 
 // Unnormalised inverse 3D transforms of the first ncomp half spectra in
-// spec3 ([z][y][kx] each) into the real grids force[c * nm^3 + (z nm + y) nm + x].
+// spec3 ([z][y][kx] each, row pitch nhp) into the real grids
+// force[c * nm^3 + (z nm + y) nm + x].
 void pm_inverse_components(const PmPlan& p, int ncomp, cudaStream_t s);
 
 // Power spectrum of power_spectrum.rs: CIC assignment (from float64 positions

@@ -342,6 +342,7 @@ int fail(tpm_handle* h, const Error& e) {
 }
 
 void check_dev_err(tpm_handle* h) {
+  if (h->pm.err) pm_check(h->pm, h->stream);
   uint32_t e = 0;
   TPM_CUDA(cudaMemcpyAsync(&e, h->T.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   TPM_CUDA(cudaStreamSynchronize(h->stream));
@@ -425,6 +426,12 @@ void ensure_capacity(tpm_handle* h, int64_t n) {
   h->cap = n;
 }
 
+// The accurate walk with the relative opening criterion ([gravity]
+// opening_criterion = "relative").
+bool relative_mac(const tpm_handle* h) {
+  return (h->cfg.flags & TPM_FLAG_ACCURATE) && h->cfg.opening_criterion == 1;
+}
+
 void ensure_tree_capacity(tpm_handle* h, int64_t n_int) {
   TreeBuffers& T = h->T;
   if (n_int <= T.cap_int) return;
@@ -443,6 +450,7 @@ void ensure_tree_capacity(tpm_handle* h, int64_t n_int) {
   T.o_com = h->alloc<double>(3 * c, 2);
   T.o_quad = h->alloc<double>(6 * c, 2);
   T.o_walk = h->alloc<uint4>(c, 2);
+  T.o_cell = h->alloc<uint4>(c, 2);
   T.recs = h->alloc<WalkNode>(c + h->cap + 8, 2);
   T.grp_count_per_node = h->alloc<uint32_t>(c, 2);
   T.grp_base = h->alloc<uint32_t>(c, 2);
@@ -572,8 +580,12 @@ void fe_tree_walk(tpm_handle* h, double eps2, const uint8_t* only) {
       ensure_tree_capacity(h, h->n_int);
       launch_octree_nodes(n, T, s);
       launch_octree_links(n, h->n_int, T, h->scan_scratch, s);
-      launch_aggregate(h->P[h->cur], n, h->n_int, box, T, s);
-      h->quad_valid = false;
+      // the accurate walk's relative opening criterion reads |Q|_F and the
+      // cell centres: the quadrupole pass runs only for it
+      const bool rel = relative_mac(h);
+      launch_aggregate(h->P[h->cur], n, h->n_int, box, T, s, rel);
+      h->quad_valid = rel;
+      if (rel) launch_cell_q(h->n_int, box, T, s);
       launch_walk_records(h->P[h->cur], n, h->n_int, h->thr, T, s);
       launch_groups(n, h->n_int, walk_targets_per_warp(), T, h->scan_scratch, s);
       TPM_CUDA(cudaMemcpyAsync(sc, T.scalars, sizeof(sc), cudaMemcpyDeviceToHost, s));
@@ -669,6 +681,16 @@ void fe_tree_walk(tpm_handle* h, double eps2, const uint8_t* only) {
         const double th = h->cfg.theta > 0.0 ? h->cfg.theta : 0.5;
         a.theta2 = (float)(th * th);
       }
+      // relative criterion (octree.rs:769-796): accept a node when the
+      // quadrupole estimate g |Q|_F / d^5 is below err_tol times the monopole
+      // g M / (d^2 + eps^2).  The reference leaves g out of the quadrupole
+      // term, which makes its ratio scale with 1/g and with the length unit;
+      // with g on both sides the tolerance is the relative truncation error
+      // the reference documents.  With d and eps in walk units and |Q|_F
+      // physical: |Q|_F (d^2 + eps^2) < err_tol u^3 M d^5
+      a.relative = relative_mac(h) ? 1 : 0;
+      a.cellq = T.o_cell;
+      a.rel_k = (float)(h->cfg.err_tol_force_acc * u * u * u);
       if (a.accurate) {  // no reference decisions to reproduce: no float64 band, no COM-on-target opening
         a.rc2_lo = a.rc2_hi = (float)rc2_u;
         a.prc2_lo = a.prc2_hi = a.rc2_lo;
@@ -929,6 +951,9 @@ int tpm_create(const tpm_config* cfg, tpm_handle** out) {
     // centre of mass inside it, so theta below that never accepts one
     if ((cfg->flags & TPM_FLAG_ACCURATE) && !(cfg->theta == 0.0 || (cfg->theta > 0.0 && cfg->theta < 0.577)))
       throw Error(TPM_ERR_INVALID_ARGUMENT, "accurate mode needs theta in (0, 0.577)");
+    if ((cfg->flags & TPM_FLAG_ACCURATE) && cfg->opening_criterion == 1 &&
+        !(cfg->err_tol_force_acc > 0.0 && std::isfinite(cfg->err_tol_force_acc)))
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "the relative opening criterion needs err_tol_force_acc > 0");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
       cudaGetLastError();
@@ -1686,6 +1711,7 @@ int tpm_power_spectrum(const double* pos, const double* mass, int64_t n, double 
     TPM_CUDA(cudaMemcpy(dmass, mass, sizeof(double) * n, cudaMemcpyHostToDevice));
     std::vector<unsigned long long> hn((size_t)mesh / 2);
     pm_power_spectrum(plan, dpos, nullptr, nullptr, nullptr, dmass, n, mtot, dsum, dn, k, pk, hn.data(), 0);
+    pm_check(plan, 0);
     for (int i = 0; i < mesh / 2; ++i) n_modes[i] = hn[i];
   } catch (const Error& e) {
     rc = e.code ? e.code : TPM_ERR_CUDA;
