@@ -172,6 +172,19 @@ def training_box(seed: int, side: int = 64, box_size: float = 50.0) -> ics.Box:
                              name=f"train{side}_s{seed}")
 
 
+def training_box_mixed(seed: int, side: int = 128) -> ics.Box:
+    """A seeded box at the benchmark's cell size (0.78 Mpc/h, L = side * 100 /
+    128): even seeds from the displaced-lattice generator at 1.0 cell rms, odd
+    seeds from the clustered generator (30 % of the particles in Plummer
+    spheres of 10^3 - 10^5 particles, scale radii 0.05 - 0.5 Mpc/h)."""
+    box_size = side * 100.0 / 128.0
+    if seed % 2 == 0:
+        return ics.lattice_box(side, box_size, 1.0, seed=seed, name=f"train{side}_lattice_s{seed}")
+    n_halos = max(8, int(200 * (side / 256.0) ** 3))
+    return ics.clustered_box(side, box_size, 0.3, n_halos, min_halo=1e3, max_halo=1e5, seed=seed,
+                             name=f"train{side}_clustered_s{seed}")
+
+
 def solver_for(box: ics.Box, mesh: int, device: int = 0, theta: float = 0.5) -> TreePmSolver:
     """The solver configuration the network is trained for and used with
     (training targets with opening angle 0.5; the fallback walk of the
