@@ -749,7 +749,8 @@ def run_domain(args):
     phys = ics.physics(box, mesh, a0)
     n = box.n
     factors, _ = trajectory(a0, a1, phys["G"], total=args.warmup + args.steps + 1)
-    dom = DomainTreePm(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"], device=local)
+    dom = DomainTreePm(mesh, box.box_size, phys["r_split"], r_cut_factor=phys["r_cut_factor"], device=local,
+                       pm="slab" if args.pm_slab else "replicated")
     lo, hi = rank * n // world, (rank + 1) * n // world
     pos = box.positions()[lo:hi]
     dom.set_particles(pos, box.mass[lo:hi], None, gid=np.arange(lo, hi))
@@ -788,7 +789,9 @@ def run_domain(args):
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32 pair arithmetic, int32 fixed-point positions, f64 decisions", "data": "synthetic",
         "config": {"workload": box.name, "particles": n, "mesh": mesh, "box_mpc_h": box.box_size,
-                   "parallelism": f"{world} SFC domain(s), periodic 3D halos of r_cut, density all-reduce",
+                   "parallelism": f"{world} SFC domain(s), periodic 3D halos of r_cut, " +
+                                  ("z-slab PM (two all-to-all transposes)" if args.pm_slab else
+                                   "density all-reduce (replicated PM)"),
                    "l2": "inputs larger than L2 (>= 0.8 GB touched per step)"},
         "domain": {"max_owned": max_owned, "max_halo_particles": max_halo,
                    "halo_fraction": max_halo / max(max_owned, 1), "stage_ms_rank0": stage_ms},
@@ -833,6 +836,7 @@ def main():
                     help="domain-decomposed steps over the ranks (SFC domains, halos, density all-reduce); "
                          "the default when --gpus > 1")
     ap.add_argument("--replicas", action="store_true", help="with --gpus > 1: independent copies, one per rank")
+    ap.add_argument("--pm-slab", action="store_true", help="domain mode: the z-slab PM solve instead of the replicated one")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -165,13 +165,14 @@ template <int LOGN> constexpr size_t pencil_smem(int tiles) {
          (size_t)(Pencil<LOGN>::N / 2 > 0 ? Pencil<LOGN>::N / 2 : 1) * sizeof(float2) + 16;
 }
 
-// Store the valid columns (kx < nh) of a tile back to [comp][z][y][kx].
+// Store the valid columns (kx < nh) of a tile back to [comp][z][y][kx]:
+// prow y rows per z plane, ppc z planes per component.
 template <int LOGN>
 __device__ __forceinline__ void store_pencil(const float2* tile, float2* __restrict__ data, int axis, int kx0,
-                                             int fixed, int comp, int nh, int nhp) {
+                                             int fixed, int comp, int nh, int nhp, int prow, int ppc) {
   using P = Pencil<LOGN>;
-  const int64_t plane = (int64_t)P::N * nhp;
-  float2* base = data + (int64_t)comp * P::N * plane;
+  const int64_t plane = (int64_t)prow * nhp;
+  float2* base = data + (int64_t)comp * ppc * plane;
   for (int idx = threadIdx.x; idx < P::N * P::CTX; idx += blockDim.x) {
     const int r = idx / P::CTX, c = idx % P::CTX, kx = kx0 + c;
     if (kx >= nh) continue;
@@ -190,11 +191,14 @@ __device__ __forceinline__ void pencil_layout(unsigned char* sm, float2*& tile, 
   bar = reinterpret_cast<uint64_t*>(s_tw + (P::N / 2 > 0 ? P::N / 2 : 1));
 }
 
-// c2c pass along y (axis 0) or z (axis 1) of ncomp half spectra, in place.
+// c2c pass along y (axis 0) or z (axis 1) of ncomp half spectra, in place:
+// prow y rows per z plane, ppc z planes per component (the full mesh: nm
+// and nm; a z slab: nm and its planes; a y slab: its rows and nm).
 template <int LOGN, bool INV>
 __global__ void __launch_bounds__(Pencil<LOGN>::THREADS) k_pencil(const __grid_constant__ CUtensorMap map,
                                                                   float2* __restrict__ data, int axis, int nh,
-                                                                  int nhp, const float2* __restrict__ tw,
+                                                                  int nhp, int prow, int ppc,
+                                                                  const float2* __restrict__ tw,
                                                                   uint32_t* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char psm[];
   float2 *tile, *tile2, *s_tw;
@@ -202,16 +206,18 @@ __global__ void __launch_bounds__(Pencil<LOGN>::THREADS) k_pencil(const __grid_c
   pencil_layout<LOGN>(psm, tile, tile2, s_tw, bar, 1);
   load_twiddles(s_tw, tw, Pencil<LOGN>::N);
   const int kx0 = blockIdx.x * Pencil<LOGN>::CTX, fixed = blockIdx.y, comp = blockIdx.z;
-  if (!stage_pencil<LOGN>(tile, bar, &map, axis, kx0, fixed, comp * Pencil<LOGN>::N, err)) return;
+  if (!stage_pencil<LOGN>(tile, bar, &map, axis, kx0, fixed, comp * ppc, err)) return;
   pencil_fft<LOGN, INV>(tile, s_tw);
-  store_pencil<LOGN>(tile, data, axis, kx0, fixed, comp, nh, nhp);
+  store_pencil<LOGN>(tile, data, axis, kx0, fixed, comp, nh, nhp, prow, ppc);
 }
 
 // Forward z pass, Green's function x filter x gradient, and the inverse z
 // passes of the ncomp components (4: the potential itself as well).
+// prow: y rows per z plane of the input and output layouts (nm, or a y
+// slab's rows starting at global row y0).
 template <int LOGN>
 __global__ void __launch_bounds__(Pencil<LOGN>::THREADS) k_pencil_poisson(
-    const __grid_constant__ CUtensorMap map, float2* __restrict__ spec3, int nh, int nhp,
+    const __grid_constant__ CUtensorMap map, float2* __restrict__ spec3, int nh, int nhp, int prow, int y0,
     const float2* __restrict__ tw, const float* __restrict__ kval, const float* __restrict__ kfilter,
     const float* __restrict__ kderiv, float kcoef, int ncomp, uint32_t* __restrict__ err) {
   using P = Pencil<LOGN>;
@@ -220,8 +226,8 @@ __global__ void __launch_bounds__(Pencil<LOGN>::THREADS) k_pencil_poisson(
   uint64_t* bar;
   pencil_layout<LOGN>(psm, tile, phi, s_tw, bar, 2);
   load_twiddles(s_tw, tw, P::N);
-  const int kx0 = blockIdx.x * P::CTX, y = blockIdx.y;
-  if (!stage_pencil<LOGN>(tile, bar, &map, 1, kx0, y, 0, err)) return;
+  const int kx0 = blockIdx.x * P::CTX, yl = blockIdx.y, y = y0 + yl;
+  if (!stage_pencil<LOGN>(tile, bar, &map, 1, kx0, yl, 0, err)) return;
   pencil_fft<LOGN, false>(tile, s_tw);
   // phi(k) = rho(k) kcoef W(k) / k^2
   for (int idx = threadIdx.x; idx < P::N * P::CTX; idx += blockDim.x) {
@@ -250,7 +256,7 @@ __global__ void __launch_bounds__(Pencil<LOGN>::THREADS) k_pencil_poisson(
     }
     __syncthreads();
     pencil_fft<LOGN, true>(tile, s_tw);
-    store_pencil<LOGN>(tile, spec3, 1, kx0, y, comp, nh, nhp);
+    store_pencil<LOGN>(tile, spec3, 1, kx0, yl, comp, nh, nhp, prow, P::N);
     __syncthreads();
   }
 }
@@ -752,7 +758,7 @@ void pencil_launch_t(const PmPlan& p, PencilOp op, int ncomp, double* pk_sum, un
       auto k = k_pencil<LOGN, false>;
       TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
       k<<<dim3(ntx, nm, 1), P::THREADS, sm1, s>>>(op == PEN_Y_FWD ? *spec_y : *spec_z, p.spec,
-                                                  op == PEN_Y_FWD ? 0 : 1, p.nh, p.nhp, p.twiddle, p.err);
+                                                  op == PEN_Y_FWD ? 0 : 1, p.nh, p.nhp, nm, nm, p.twiddle, p.err);
       break;
     }
     case PEN_Y_INV:
@@ -760,14 +766,15 @@ void pencil_launch_t(const PmPlan& p, PencilOp op, int ncomp, double* pk_sum, un
       auto k = k_pencil<LOGN, true>;
       TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
       k<<<dim3(ntx, nm, ncomp), P::THREADS, sm1, s>>>(op == PEN_Y_INV ? *spec3_y : *spec3_z, p.spec3,
-                                                      op == PEN_Y_INV ? 0 : 1, p.nh, p.nhp, p.twiddle, p.err);
+                                                      op == PEN_Y_INV ? 0 : 1, p.nh, p.nhp, nm, nm, p.twiddle,
+                                                      p.err);
       break;
     }
     case PEN_POISSON: {
       auto k = k_pencil_poisson<LOGN>;
       TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-      k<<<dim3(ntx, nm), P::THREADS, sm2, s>>>(*spec_z, p.spec3, p.nh, p.nhp, p.twiddle, p.kval, p.kfilter,
-                                               p.kderiv, p.kcoef, p.ncomp, p.err);
+      k<<<dim3(ntx, nm), P::THREADS, sm2, s>>>(*spec_z, p.spec3, p.nh, p.nhp, nm, 0, p.twiddle, p.kval,
+                                               p.kfilter, p.kderiv, p.kcoef, p.ncomp, p.err);
       break;
     }
     case PEN_PK: {
@@ -797,37 +804,83 @@ void pencil_launch(const PmPlan& p, PencilOp op, int ncomp = 1, double* pk_sum =
   }
 }
 
-// ---- x-pass launches (rows of h = nm/2 packed complex values) ---------------------
-template <int LOGH>
-void row_launch_t(const PmPlan& p, bool forward, int ncomp, cudaStream_t s) {
-  using RP = RowPass<LOGH>;
-  const int64_t nrows = (int64_t)p.nm * p.nm;
-  const unsigned blocks = (unsigned)((nrows + RP::RX - 1) / RP::RX);
-  if (forward) {
-    const size_t sm = row_smem<LOGH>(RP::H);
-    TPM_CUDA(cudaFuncSetAttribute(k_row_r2c<LOGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_row_r2c<LOGH><<<blocks, RP::THREADS, sm, s>>>(p.rho, p.spec, p.nhp, nrows, p.twiddle, p.err);
-  } else {
-    const size_t sm = row_smem<LOGH>(p.nhp);
-    TPM_CUDA(cudaFuncSetAttribute(k_row_c2r<LOGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_row_c2r<LOGH><<<dim3(blocks, ncomp), RP::THREADS, sm, s>>>(p.spec3, p.force, p.nhp, nrows, p.twiddle, p.err);
+// ---- slab pencil launches ------------------------------------------------------------
+template <int LOGN>
+void slab_pencil_t(const PmPlan& p, const PmSlab& sl, int op, cudaStream_t s) {
+  using P = Pencil<LOGN>;
+  const int nm = p.nm, ntx = (p.nh + P::CTX - 1) / P::CTX;
+  const size_t sm1 = pencil_smem<LOGN>(1), sm2 = pencil_smem<LOGN>(2);
+  if (op == 0) {  // forward y on this rank's planes
+    auto k = k_pencil<LOGN, false>;
+    TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    k<<<dim3(ntx, sl.nzl, 1), P::THREADS, sm1, s>>>(*reinterpret_cast<const CUtensorMap*>(sl.tmap[0]), sl.spec, 0,
+                                                    p.nh, p.nhp, nm, sl.nzl, p.twiddle, p.err);
+  } else if (op == 1) {  // z passes + Poisson on the received y rows
+    auto k = k_pencil_poisson<LOGN>;
+    TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    k<<<dim3(ntx, sl.nyl), P::THREADS, sm2, s>>>(*reinterpret_cast<const CUtensorMap*>(sl.tmap[2]), sl.t3, p.nh,
+                                                 p.nhp, sl.nyl, sl.rank * sl.nyl, p.twiddle, p.kval, p.kfilter,
+                                                 p.kderiv, p.kcoef, sl.ncomp, p.err);
+  } else {  // inverse y of the force spectra of this rank's planes
+    auto k = k_pencil<LOGN, true>;
+    TPM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    k<<<dim3(ntx, sl.nzl, sl.ncomp), P::THREADS, sm1, s>>>(*reinterpret_cast<const CUtensorMap*>(sl.tmap[1]),
+                                                           sl.spec3, 0, p.nh, p.nhp, nm, sl.nzl, p.twiddle, p.err);
   }
   TPM_LAUNCH_CHECK();
 }
 
-void row_launch(const PmPlan& p, bool forward, int ncomp, cudaStream_t s) {
-  switch (p.logn - 1) {
-    case 1: row_launch_t<1>(p, forward, ncomp, s); break;
-    case 2: row_launch_t<2>(p, forward, ncomp, s); break;
-    case 3: row_launch_t<3>(p, forward, ncomp, s); break;
-    case 4: row_launch_t<4>(p, forward, ncomp, s); break;
-    case 5: row_launch_t<5>(p, forward, ncomp, s); break;
-    case 6: row_launch_t<6>(p, forward, ncomp, s); break;
-    case 7: row_launch_t<7>(p, forward, ncomp, s); break;
-    case 8: row_launch_t<8>(p, forward, ncomp, s); break;
-    case 9: row_launch_t<9>(p, forward, ncomp, s); break;
+void slab_pencil(const PmPlan& p, const PmSlab& sl, int op, cudaStream_t s) {
+  switch (p.logn) {
+    case 2: slab_pencil_t<2>(p, sl, op, s); break;
+    case 3: slab_pencil_t<3>(p, sl, op, s); break;
+    case 4: slab_pencil_t<4>(p, sl, op, s); break;
+    case 5: slab_pencil_t<5>(p, sl, op, s); break;
+    case 6: slab_pencil_t<6>(p, sl, op, s); break;
+    case 7: slab_pencil_t<7>(p, sl, op, s); break;
+    case 8: slab_pencil_t<8>(p, sl, op, s); break;
+    case 9: slab_pencil_t<9>(p, sl, op, s); break;
+    case 10: slab_pencil_t<10>(p, sl, op, s); break;
     default: throw Error(TPM_ERR_INVALID_ARGUMENT, "mesh size outside 4..1024");
   }
+}
+
+// ---- x-pass launches (rows of h = nm/2 packed complex values) ---------------------
+// nrows rows of the real meshes `real` and spectra `spec` (per component:
+// nrows rows each).
+template <int LOGH>
+void row_launch_t(const PmPlan& p, bool forward, float* real, float2* spec, int64_t nrows, int ncomp,
+                  cudaStream_t s) {
+  using RP = RowPass<LOGH>;
+  const unsigned blocks = (unsigned)((nrows + RP::RX - 1) / RP::RX);
+  if (forward) {
+    const size_t sm = row_smem<LOGH>(RP::H);
+    TPM_CUDA(cudaFuncSetAttribute(k_row_r2c<LOGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_row_r2c<LOGH><<<blocks, RP::THREADS, sm, s>>>(real, spec, p.nhp, nrows, p.twiddle, p.err);
+  } else {
+    const size_t sm = row_smem<LOGH>(p.nhp);
+    TPM_CUDA(cudaFuncSetAttribute(k_row_c2r<LOGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_row_c2r<LOGH><<<dim3(blocks, ncomp), RP::THREADS, sm, s>>>(spec, real, p.nhp, nrows, p.twiddle, p.err);
+  }
+  TPM_LAUNCH_CHECK();
+}
+
+void row_launch(const PmPlan& p, bool forward, float* real, float2* spec, int64_t nrows, int ncomp, cudaStream_t s) {
+  switch (p.logn - 1) {
+    case 1: row_launch_t<1>(p, forward, real, spec, nrows, ncomp, s); break;
+    case 2: row_launch_t<2>(p, forward, real, spec, nrows, ncomp, s); break;
+    case 3: row_launch_t<3>(p, forward, real, spec, nrows, ncomp, s); break;
+    case 4: row_launch_t<4>(p, forward, real, spec, nrows, ncomp, s); break;
+    case 5: row_launch_t<5>(p, forward, real, spec, nrows, ncomp, s); break;
+    case 6: row_launch_t<6>(p, forward, real, spec, nrows, ncomp, s); break;
+    case 7: row_launch_t<7>(p, forward, real, spec, nrows, ncomp, s); break;
+    case 8: row_launch_t<8>(p, forward, real, spec, nrows, ncomp, s); break;
+    case 9: row_launch_t<9>(p, forward, real, spec, nrows, ncomp, s); break;
+    default: throw Error(TPM_ERR_INVALID_ARGUMENT, "mesh size outside 4..1024");
+  }
+}
+void row_launch(const PmPlan& p, bool forward, int ncomp, cudaStream_t s) {
+  row_launch(p, forward, forward ? p.rho : p.force, forward ? p.spec : p.spec3, (int64_t)p.nm * p.nm, ncomp, s);
 }
 
 // cuTensorMapEncodeTiled from the driver, looked up once (no libcuda link).
@@ -843,12 +896,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
   return fn;
 }
 
-// Tensor map of `comps` half spectra [comp * nm + z][y][kx] (8-byte complex
-// elements, rows of nhp): box of ctx columns by `rows_y` y rows by `rows_z` z rows.
-void encode_spectrum_map(void* out, float2* base, int nm, int nhp, int comps, int ctx, int rows_y, int rows_z) {
+// Tensor map of half spectra [plane][y][kx] (8-byte complex elements, rows of
+// nhp, ny rows per plane, `planes` planes over all components): box of ctx
+// columns by `rows_y` y rows by `rows_z` planes.
+void encode_spectrum_map(void* out, float2* base, int ny, int nhp, int64_t planes, int ctx, int rows_y, int rows_z) {
   CUtensorMap* m = reinterpret_cast<CUtensorMap*>(out);
-  const cuuint64_t dims[3] = {(cuuint64_t)nhp, (cuuint64_t)nm, (cuuint64_t)nm * (cuuint64_t)comps};
-  const cuuint64_t strides[2] = {(cuuint64_t)nhp * sizeof(float2), (cuuint64_t)nhp * sizeof(float2) * (cuuint64_t)nm};
+  const cuuint64_t dims[3] = {(cuuint64_t)nhp, (cuuint64_t)ny, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)nhp * sizeof(float2), (cuuint64_t)nhp * sizeof(float2) * (cuuint64_t)ny};
   const cuuint32_t box[3] = {(cuuint32_t)ctx, (cuuint32_t)rows_y, (cuuint32_t)rows_z};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = encode_tiled()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
@@ -915,10 +969,10 @@ void pm_plan_init(PmPlan& p, int nm, double box, double r_split, uint32_t flags,
   TPM_CUDA(cudaMemset(p.err, 0, sizeof(uint32_t)));
   // pencil tiles: ctx columns by min(nm, 256) rows along y or z
   const int ctx = nm > 512 ? 8 : 16, rows = nm < 256 ? nm : 256;
-  encode_spectrum_map(p.tmap[0], p.spec, nm, p.nhp, 1, ctx, rows, 1);
-  encode_spectrum_map(p.tmap[1], p.spec, nm, p.nhp, 1, ctx, 1, rows);
-  encode_spectrum_map(p.tmap[2], p.spec3, nm, p.nhp, p.ncomp, ctx, rows, 1);
-  encode_spectrum_map(p.tmap[3], p.spec3, nm, p.nhp, p.ncomp, ctx, 1, rows);
+  encode_spectrum_map(p.tmap[0], p.spec, nm, p.nhp, nm, ctx, rows, 1);
+  encode_spectrum_map(p.tmap[1], p.spec, nm, p.nhp, nm, ctx, 1, rows);
+  encode_spectrum_map(p.tmap[2], p.spec3, nm, p.nhp, (int64_t)nm * p.ncomp, ctx, rows, 1);
+  encode_spectrum_map(p.tmap[3], p.spec3, nm, p.nhp, (int64_t)nm * p.ncomp, ctx, 1, rows);
 }
 
 void pm_check(const PmPlan& p, cudaStream_t s) {
@@ -1023,6 +1077,88 @@ void pm_power_spectrum(const PmPlan& p, const double* pos, const uint32_t* qx, c
     n_out[i] = hn[i];
     pk_out[i] = hn[i] ? hs[i] * scale * scale * norm / (double)hn[i] : 0.0;
   }
+}
+
+// ---- z-slab decomposition ---------------------------------------------------------
+void pm_slab_init(PmSlab& sl, const PmPlan& p, int rank, int ranks) {
+  const int nm = p.nm;
+  if (ranks < 1 || rank < 0 || rank >= ranks || nm % ranks != 0)
+    throw Error(TPM_ERR_INVALID_ARGUMENT, "pm_grid_size must be a multiple of the rank count");
+  pm_slab_free(sl);
+  sl.rank = rank;
+  sl.ranks = ranks;
+  sl.nzl = nm / ranks;
+  sl.nyl = nm / ranks;
+  sl.ncomp = 3;
+  const int64_t nhp = p.nhp, nm2 = (int64_t)nm * nm;
+  const int64_t slab_spec = (int64_t)sl.nzl * nm * nhp, ycols = (int64_t)nm * sl.nyl * nhp;
+  TPM_CUDA(cudaMalloc(&sl.rho, sizeof(float) * sl.nzl * nm2));
+  TPM_CUDA(cudaMalloc(&sl.spec, sizeof(float2) * slab_spec));
+  TPM_CUDA(cudaMalloc(&sl.send, sizeof(float2) * ycols * sl.ncomp));
+  TPM_CUDA(cudaMalloc(&sl.recv, sizeof(float2) * ycols * sl.ncomp));
+  TPM_CUDA(cudaMalloc(&sl.t3, sizeof(float2) * ycols * sl.ncomp));
+  TPM_CUDA(cudaMalloc(&sl.spec3, sizeof(float2) * slab_spec * sl.ncomp));
+  TPM_CUDA(cudaMalloc(&sl.force, sizeof(float) * sl.nzl * nm2 * sl.ncomp));
+  // padding columns (kx = nh) are never written
+  TPM_CUDA(cudaMemset(sl.spec, 0, sizeof(float2) * slab_spec));
+  TPM_CUDA(cudaMemset(sl.send, 0, sizeof(float2) * ycols * sl.ncomp));
+  TPM_CUDA(cudaMemset(sl.recv, 0, sizeof(float2) * ycols * sl.ncomp));
+  TPM_CUDA(cudaMemset(sl.t3, 0, sizeof(float2) * ycols * sl.ncomp));
+  TPM_CUDA(cudaMemset(sl.spec3, 0, sizeof(float2) * slab_spec * sl.ncomp));
+  sl.send_bytes = sizeof(float2) * (size_t)slab_spec;  // the forward transpose; the return one sends ncomp times as much
+  const int ctx = nm > 512 ? 8 : 16, rows = nm < 256 ? nm : 256;
+  encode_spectrum_map(sl.tmap[0], sl.spec, nm, p.nhp, sl.nzl, ctx, rows, 1);
+  encode_spectrum_map(sl.tmap[1], sl.spec3, nm, p.nhp, (int64_t)sl.nzl * sl.ncomp, ctx, rows, 1);
+  encode_spectrum_map(sl.tmap[2], sl.recv, sl.nyl, p.nhp, nm, ctx, 1, rows);
+}
+
+void pm_slab_free(PmSlab& sl) {
+  cudaFree(sl.rho);
+  cudaFree(sl.spec);
+  cudaFree(sl.send);
+  cudaFree(sl.recv);
+  cudaFree(sl.t3);
+  cudaFree(sl.spec3);
+  cudaFree(sl.force);
+  sl = PmSlab();
+}
+
+void pm_slab_forward(const PmPlan& p, const PmSlab& sl, cudaStream_t s) {
+  const int nm = p.nm;
+  const int64_t nhp = p.nhp;
+  row_launch(p, true, sl.rho, sl.spec, (int64_t)sl.nzl * nm, 1, s);
+  slab_pencil(p, sl, 0, s);
+  // send[dest][zl][yl][kx] = spec[zl][dest nyl + yl][kx]
+  const size_t w = sizeof(float2) * (size_t)sl.nyl * nhp;
+  for (int d = 0; d < sl.ranks; ++d)
+    TPM_CUDA(cudaMemcpy2DAsync(sl.send + (int64_t)d * sl.nzl * sl.nyl * nhp, w, sl.spec + (int64_t)d * sl.nyl * nhp,
+                               sizeof(float2) * (size_t)nm * nhp, w, sl.nzl, cudaMemcpyDeviceToDevice, s));
+}
+
+void pm_slab_poisson(const PmPlan& p, const PmSlab& sl, cudaStream_t s) {
+  // recv is [src][zl][yl][kx] = [z][yl][kx]: every z of this rank's y rows
+  slab_pencil(p, sl, 1, s);
+  // send[dest][comp][zl][yl][kx] = t3[comp][dest nzl + zl][yl][kx]
+  const int64_t blk = (int64_t)sl.nzl * sl.nyl * p.nhp;
+  for (int d = 0; d < sl.ranks; ++d)
+    for (int c = 0; c < sl.ncomp; ++c)
+      TPM_CUDA(cudaMemcpyAsync(sl.send + ((int64_t)d * sl.ncomp + c) * blk,
+                               sl.t3 + (int64_t)c * p.nm * sl.nyl * p.nhp + (int64_t)d * blk, sizeof(float2) * blk,
+                               cudaMemcpyDeviceToDevice, s));
+}
+
+void pm_slab_inverse(const PmPlan& p, const PmSlab& sl, cudaStream_t s) {
+  const int nm = p.nm;
+  const int64_t nhp = p.nhp, blk = (int64_t)sl.nzl * sl.nyl * nhp;
+  // spec3[comp][zl][src nyl + yl][kx] = recv[src][comp][zl][yl][kx]
+  const size_t w = sizeof(float2) * (size_t)sl.nyl * nhp;
+  for (int r = 0; r < sl.ranks; ++r)
+    for (int c = 0; c < sl.ncomp; ++c)
+      TPM_CUDA(cudaMemcpy2DAsync(sl.spec3 + (int64_t)c * sl.nzl * nm * nhp + (int64_t)r * sl.nyl * nhp,
+                                 sizeof(float2) * (size_t)nm * nhp, sl.recv + ((int64_t)r * sl.ncomp + c) * blk, w, w,
+                                 sl.nzl, cudaMemcpyDeviceToDevice, s));
+  slab_pencil(p, sl, 2, s);
+  row_launch(p, false, sl.force, sl.spec3, (int64_t)sl.nzl * nm, sl.ncomp, s);
 }
 
 }  // namespace tpm

@@ -66,6 +66,34 @@ void pm_cells(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const uin
 
 struct Particles;
 
+// z-slab decomposition of the PM solve over `ranks` processes (slab_fft.rs
+// :209-330): rank r owns z planes [r nzl, (r+1) nzl) of the density and the
+// force meshes and, between the two transposes, y rows [r nyl, (r+1) nyl) of
+// the half spectrum with every z.  The caller moves the buffers between the
+// ranks (reduce-scatter of the density into `rho`, two equal-split
+// all-to-alls from `send` into `recv`, all-gather of `force`).
+struct PmSlab {
+  int rank = 0, ranks = 0, nzl = 0, nyl = 0, ncomp = 3;
+  float* rho = nullptr;     // nzl x nm x nm: this rank's planes of the summed density
+  float2* spec = nullptr;   // nzl x nm x nhp: after the x and y passes
+  float2* send = nullptr;   // transpose send buffer (ncomp x nm x nyl x nhp)
+  float2* recv = nullptr;   // transpose receive buffer, same size
+  float2* t3 = nullptr;     // ncomp x nm x nyl x nhp: force spectra, [z][y - y0][kx]
+  float2* spec3 = nullptr;  // ncomp x nzl x nm x nhp: force spectra of this rank's planes
+  float* force = nullptr;   // ncomp x nzl x nm x nm: force slabs, per unit G
+  size_t send_bytes = 0;    // bytes of one transpose (every rank sends and receives as many)
+  alignas(64) unsigned char tmap[3][128];  // spec y pencils, spec3 y pencils, recv z pencils
+};
+void pm_slab_init(PmSlab& sl, const PmPlan& p, int rank, int ranks);
+void pm_slab_free(PmSlab& sl);
+// x and y passes of this rank's density planes, then the forward transpose's send buffer.
+void pm_slab_forward(const PmPlan& p, const PmSlab& sl, cudaStream_t s);
+// After the forward all-to-all: z passes with the Green's function, filter
+// and gradient on the received y rows, then the return transpose's send buffer.
+void pm_slab_poisson(const PmPlan& p, const PmSlab& sl, cudaStream_t s);
+// After the return all-to-all: inverse y and x passes into the force slabs.
+void pm_slab_inverse(const PmPlan& p, const PmSlab& sl, cudaStream_t s);
+
 // Unnormalised forward 3D transform of the real field p.rho into the half
 // spectrum p.spec ([z][y][kx], kx <= nm/2, row pitch nhp).
 void pm_forward_real(const PmPlan& p, cudaStream_t s);

@@ -228,6 +228,7 @@ struct tpm_handle {
   uint32_t* pcounts = nullptr;
   TreeBuffers T{};
   PmPlan pm;
+  PmSlab slab;  // z-slab decomposition of the PM solve (domain-decomposed runs)
   void* sort_scratch = nullptr;
   size_t sort_bytes = 0;
   void* scan_scratch = nullptr;
@@ -745,7 +746,7 @@ void fe_tree_walk(tpm_handle* h, double eps2, const uint8_t* only) {
 
 // fe_long_range: CIC deposit (unless the caller deposited already), FFT
 // Poisson solve, gather fused with the short-range sum and the kick, stats.
-void fe_long_range(tpm_handle* h, double g, double kick, bool deposit) {
+void fe_long_range(tpm_handle* h, double g, double kick, bool deposit, bool solve = true) {
   cudaStream_t s = h->stream;
   const int64_t n = h->n;
   const bool use_net = h->fe.use_net;
@@ -754,7 +755,7 @@ void fe_long_range(tpm_handle* h, double g, double kick, bool deposit) {
   const Particles& P = h->P[h->cur];
   if (!use_net) {
     if (deposit) pm_deposit(h->pm, P.qx, P.qy, P.qz, P.massf, n, s);
-    pm_solve(h->pm, s);
+    if (solve) pm_solve(h->pm, s);
   }
   TPM_CUDA(cudaEventRecord(h->ev[5], s));
   GatherArgs ga{};
@@ -1017,6 +1018,7 @@ void tpm_destroy(tpm_handle* h) {
   cudaSetDevice(h->cfg.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (const auto& a : h->allocs) cudaFree(a.p);
+  pm_slab_free(h->slab);
   pm_plan_free(h->pm);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -1253,13 +1255,13 @@ int tpm_force_short_range(tpm_handle* h, double eps2) {
   return TPM_OK;
 }
 
-int tpm_force_end(tpm_handle* h, double g, double kick) {
+static int force_end(tpm_handle* h, double g, double kick, bool solve) {
   if (!h) return TPM_ERR_INVALID_ARGUMENT;
   try {
     TPM_CUDA(cudaSetDevice(h->cfg.device));
     if (h->fe.phase != 2) throw Error(TPM_ERR_NOT_READY, "tpm_force_short_range first");
     if (h->n > 0) {
-      fe_long_range(h, g, kick, false);
+      fe_long_range(h, g, kick, false, solve);
     } else {
       h->fe.phase = 0;
       h->forces_valid = true;
@@ -1272,6 +1274,52 @@ int tpm_force_end(tpm_handle* h, double g, double kick) {
   }
   return TPM_OK;
 }
+
+int tpm_force_end(tpm_handle* h, double g, double kick) { return force_end(h, g, kick, true); }
+int tpm_force_end_solved(tpm_handle* h, double g, double kick) { return force_end(h, g, kick, false); }
+
+int tpm_pm_slab_setup(tpm_handle* h, int32_t rank, int32_t ranks, tpm_slab_buffers* out) {
+  if (!h || !out) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (h->pm_only || h->learned) throw Error(TPM_ERR_INVALID_ARGUMENT, "the slab PM serves the TreePM solver");
+    if (ranks < 1 || ranks > MAX_RANKS || rank < 0 || rank >= ranks)
+      throw Error(TPM_ERR_INVALID_ARGUMENT, "rank out of range");
+    if (h->slab.ranks != ranks || h->slab.rank != rank) pm_slab_init(h->slab, h->pm, rank, ranks);
+    const PmSlab& sl = h->slab;
+    const int64_t nm = h->pm.nm;
+    out->density_slab = sl.rho;
+    out->send = sl.send;
+    out->recv = sl.recv;
+    out->forward_bytes = (int64_t)sl.send_bytes;
+    out->return_bytes = (int64_t)sl.send_bytes * sl.ncomp;
+    out->force_slab = sl.force;
+    out->force_mesh = h->pm.force;
+    out->planes = sl.nzl;
+    out->slab_cells = (int64_t)sl.nzl * nm * nm;
+    out->mesh_cells = nm * nm * nm;
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+
+static int slab_stage(tpm_handle* h, int stage) {
+  if (!h) return TPM_ERR_INVALID_ARGUMENT;
+  try {
+    TPM_CUDA(cudaSetDevice(h->cfg.device));
+    if (h->slab.ranks < 1) throw Error(TPM_ERR_NOT_READY, "tpm_pm_slab_setup first");
+    if (stage == 0) pm_slab_forward(h->pm, h->slab, h->stream);
+    else if (stage == 1) pm_slab_poisson(h->pm, h->slab, h->stream);
+    else pm_slab_inverse(h->pm, h->slab, h->stream);
+  } catch (const Error& e) {
+    return fail(h, e);
+  }
+  return TPM_OK;
+}
+int tpm_pm_slab_forward(tpm_handle* h) { return slab_stage(h, 0); }
+int tpm_pm_slab_poisson(tpm_handle* h) { return slab_stage(h, 1); }
+int tpm_pm_slab_inverse(tpm_handle* h) { return slab_stage(h, 2); }
 
 int tpm_kick_drift(tpm_handle* h, double kick_half, double drift, double g) {
   if (!h) return TPM_ERR_INVALID_ARGUMENT;

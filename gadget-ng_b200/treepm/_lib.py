@@ -51,6 +51,22 @@ class TpmConfig(C.Structure):
     ]
 
 
+class TpmSlabBuffers(C.Structure):
+    """tpm_slab_buffers: device buffers of the z-slab PM solve."""
+    _fields_ = [
+        ("density_slab", C.c_void_p),
+        ("send", C.c_void_p),
+        ("recv", C.c_void_p),
+        ("forward_bytes", C.c_int64),
+        ("return_bytes", C.c_int64),
+        ("force_slab", C.c_void_p),
+        ("force_mesh", C.c_void_p),
+        ("planes", C.c_int32),
+        ("slab_cells", C.c_int64),
+        ("mesh_cells", C.c_int64),
+    ]
+
+
 class TpmZeldovich(C.Structure):
     """tpm_zeldovich: the reference's Zel'dovich IC configuration
     (crates/gadget-ng-core/src/ic_zeldovich.rs:621-640 arguments)."""
@@ -205,6 +221,11 @@ SIGNATURES = {
     "tpm_mesh_density": ([_P, C.POINTER(_P), C.POINTER(_I64)], _I),
     "tpm_force_short_range": ([_P, _D], _I),
     "tpm_force_end": ([_P, _D, _D], _I),
+    "tpm_force_end_solved": ([_P, _D, _D], _I),
+    "tpm_pm_slab_setup": ([_P, C.c_int32, C.c_int32, _P], _I),
+    "tpm_pm_slab_forward": ([_P], _I),
+    "tpm_pm_slab_poisson": ([_P], _I),
+    "tpm_pm_slab_inverse": ([_P], _I),
     "tpm_kick_drift": ([_P, _D, _D, _D], _I),
     "tpm_particle_counts": ([_P, C.POINTER(_I64), C.POINTER(_I64)], _I),
     "tpm_sfc_keys": ([_P, _P, C.c_int32, _P], _I),

@@ -131,6 +131,36 @@ class _Exchange:
                                     [int(x) for x in send_bytes], group=self.group)
         return recv.to(self.device)
 
+    def reduce_scatter_sum_(self, out, t) -> None:
+        """reduce_scatter of t (equal contiguous chunks, rank order) into out:
+        out = the sum over ranks of this rank's chunk (gloo: all-reduce, then
+        the chunk)."""
+        if self.on_device:
+            self.dist.reduce_scatter_tensor(out, t, group=self.group)
+            return
+        c = t.cpu()
+        self.dist.all_reduce(c, group=self.group)
+        n = out.numel()
+        out.copy_(c[self.rank * n:(self.rank + 1) * n])
+
+    def alltoall_equal_(self, out, t) -> None:
+        """all-to-all of equal contiguous chunks (rank order) from t into out."""
+        if self.on_device:
+            self.dist.all_to_all_single(out, t, group=self.group)
+            return
+        o = self.torch.empty_like(out, device="cpu")
+        self.dist.all_to_all_single(o, t.cpu(), group=self.group)
+        out.copy_(o)
+
+    def allgather_into_(self, out, t) -> None:
+        """all-gather of equal chunks t (rank order) into out."""
+        if self.on_device:
+            self.dist.all_gather_into_tensor(out, t, group=self.group)
+            return
+        parts = [self.torch.empty_like(t, device="cpu") for _ in range(self.size)]
+        self.dist.all_gather(parts, t.cpu(), group=self.group)
+        out.copy_(self.torch.cat(parts))
+
     def allreduce_sum_(self, t) -> None:
         """allreduce_sum_f64_slice (lib.rs:200-210) in place on a device tensor."""
         if self.on_device:
@@ -148,13 +178,21 @@ class DomainTreePm:
     reference's rule (within r_cut of another rank's particle AABB); "cells"
     by the cells that rank occupies on a grid at least r_cut wide, which keeps
     every pair within r_cut and sends far fewer particles once domains are
-    not slabs (the short-range trees then differ from the reference's)."""
+    not slabs (the short-range trees then differ from the reference's).
+    `pm`: "replicated" sums the density mesh on every rank and solves it
+    everywhere (allreduce_sum_f64_slice, lib.rs:200-210); "slab" splits the
+    solve into z slabs with two all-to-all transposes (slab_fft.rs:209-330,
+    the reference's pm_slab path; pm_grid_size a multiple of the rank count)
+    and all-gathers the force meshes for the gather."""
 
     def __init__(self, grid_size: int, box_size: float, r_split: float = 0.0, *, r_cut_factor: float = 5.0,
-                 device: int = 0, group=None, overlap: bool = True, halo: str = "aabb"):
+                 device: int = 0, group=None, overlap: bool = True, halo: str = "aabb", pm: str = "replicated"):
         if halo not in ("aabb", "cells"):
             raise ValueError("halo is 'aabb' or 'cells'")
+        if pm not in ("replicated", "slab"):
+            raise ValueError("pm is 'replicated' or 'slab'")
         self.halo = halo
+        self.pm = pm
         import torch
         import torch.distributed as dist
         if not dist.is_initialized():
@@ -179,6 +217,7 @@ class DomainTreePm:
         self.last_halo_sent = 0
         self._stream = None
         self._side = None
+        self._slab = None
 
     # ---- particles -----------------------------------------------------------
     def set_particles(self, pos, mass, vel=None, gid=None):
@@ -259,13 +298,60 @@ class DomainTreePm:
             self._side = torch.cuda.Stream(device=self.device)
         return self._stream, self._side
 
+    def _slab_buffers(self):
+        if self._slab is None:
+            b = _lib.TpmSlabBuffers()
+            check(self._h.h, self._L.tpm_pm_slab_setup(self._h.h, self.ex.rank, self.ex.size, C.byref(b)))
+            dev = self.device
+            t = lambda ptr, n, ts: self.torch.as_tensor(_DeviceArray(ptr, n, ts), device=dev)
+            self._slab = dict(
+                rho=t(b.density_slab, b.slab_cells, "<f4"),
+                send=t(b.send, b.return_bytes, "|u1"), recv=t(b.recv, b.return_bytes, "|u1"),
+                fwd=int(b.forward_bytes), ret=int(b.return_bytes),
+                force_slab=t(b.force_slab, 3 * b.slab_cells, "<f4"), force=t(b.force_mesh, 3 * b.mesh_cells, "<f4"),
+                slab_cells=int(b.slab_cells), mesh_cells=int(b.mesh_cells))
+        return self._slab
+
+    def _slab_solve(self) -> None:
+        """The z-slab PM solve (tpm_pm_slab_*): reduce-scatter of the density,
+        forward transpose, z passes, return transpose, all-gather of the force
+        slabs into the meshes the gather reads."""
+        h, L, ex = self._h.h, self._L, self.ex
+        sb = self._slab_buffers()
+        ext, _ = self._streams()
+        sync = lambda: (ext.synchronize(), self.torch.cuda.synchronize(self.device))
+        sync()
+        ex.reduce_scatter_sum_(sb["rho"], self._mesh_tensor())
+        sync()
+        check(h, L.tpm_pm_slab_forward(h))
+        sync()
+        ex.alltoall_equal_(sb["recv"][:sb["fwd"]], sb["send"][:sb["fwd"]])
+        sync()
+        check(h, L.tpm_pm_slab_poisson(h))
+        sync()
+        ex.alltoall_equal_(sb["recv"][:sb["ret"]], sb["send"][:sb["ret"]])
+        sync()
+        check(h, L.tpm_pm_slab_inverse(h))
+        sync()
+        n, m = sb["slab_cells"], sb["mesh_cells"]
+        for c in range(3):
+            ex.allgather_into_(sb["force"][c * m:(c + 1) * m], sb["force_slab"][c * n:(c + 1) * n])
+        sync()
+
     def _force(self, eps2: float, g: float, kick: float) -> None:
         """Force evaluation of the owned particles with the current halos:
         deposit -> density all-reduce (overlapped with the walk on NCCL) ->
-        FFT solve -> gather (+ kick)."""
+        FFT solve -> gather (+ kick); with pm="slab" the solve is split over
+        the ranks (_slab_solve) and runs before the walk."""
         h = self._h.h
         L = self._L
         check(h, L.tpm_force_begin(h))
+        if self.pm == "slab":
+            self._slab_solve()
+            check(h, L.tpm_force_short_range(h, float(eps2)))
+            check(h, L.tpm_force_end_solved(h, float(g), float(kick)))
+            self._forces = (float(eps2), float(g))
+            return
         mesh = self._mesh_tensor()
         if self.overlap:
             ext, side = self._streams()

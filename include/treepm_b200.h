@@ -250,6 +250,47 @@ int tpm_force_begin(tpm_handle* h);
 int tpm_mesh_density(tpm_handle* h, float** density, int64_t* cells);
 int tpm_force_short_range(tpm_handle* h, double eps2);
 int tpm_force_end(tpm_handle* h, double g, double kick);
+/* tpm_force_end without the FFT solve: the gather reads the force meshes the
+ * caller assembled (the z-slab path below), per unit G, [c][z][y][x]. */
+int tpm_force_end_solved(tpm_handle* h, double g, double kick);
+
+/* z-slab decomposition of the PM solve (crates/gadget-ng-pm/src/slab_fft.rs
+ * :209-330 and slab_pm.rs:1-30, the reference's `pm_slab` path): instead of
+ * summing the whole density mesh on every rank and solving it everywhere,
+ * rank r owns z planes [r nzl, (r+1) nzl) (nzl = pm_grid_size / ranks; the
+ * mesh size must be a multiple of the rank count).  Between tpm_force_begin
+ * and tpm_force_end_solved, with the caller's collectives on the listed device
+ * buffers, in this order:
+ *   1. reduce-scatter of the tpm_mesh_density mesh over the ranks into
+ *      density_slab (rank r gets planes r nzl ..);
+ *   2. tpm_pm_slab_forward: x and y transforms of those planes, send filled;
+ *   3. all-to-all of forward_bytes (equal splits) from send into recv;
+ *   4. tpm_pm_slab_poisson: z transforms, Green's function x filter x
+ *      gradient and inverse z transforms of the y rows [r nyl, (r+1) nyl),
+ *      send filled again;
+ *   5. all-to-all of return_bytes from send into recv;
+ *   6. tpm_pm_slab_inverse: inverse y and x transforms into force_slab
+ *      (3 x slab_cells floats);
+ *   7. all-gather of each component's slab into force_mesh (3 x mesh_cells).
+ * Each stage runs on the handle's stream; the caller orders its collectives
+ * after it.  tpm_pm_slab_setup allocates the slab buffers once per
+ * (rank, ranks) and returns their addresses. */
+typedef struct tpm_slab_buffers {
+  float* density_slab;    /* slab_cells floats */
+  void* send;             /* transpose send buffer (return_bytes) */
+  void* recv;             /* transpose receive buffer (return_bytes) */
+  int64_t forward_bytes;  /* bytes of the first all-to-all (forward_bytes / ranks per peer) */
+  int64_t return_bytes;   /* bytes of the second all-to-all */
+  float* force_slab;      /* 3 x slab_cells floats, per unit G */
+  float* force_mesh;      /* 3 x mesh_cells floats: the meshes tpm_force_end_solved gathers from */
+  int32_t planes;         /* nzl */
+  int64_t slab_cells;     /* nzl x nm x nm */
+  int64_t mesh_cells;     /* nm^3 */
+} tpm_slab_buffers;
+int tpm_pm_slab_setup(tpm_handle* h, int32_t rank, int32_t ranks, tpm_slab_buffers* out);
+int tpm_pm_slab_forward(tpm_handle* h);
+int tpm_pm_slab_poisson(tpm_handle* h);
+int tpm_pm_slab_inverse(tpm_handle* h);
 /* The opening half of a domain-decomposed KDK step: halo copies dropped,
  * then v += a kick_half (the cached acceleration rescaled by g / g_prev) and
  * the drift with the periodic wrap, for the owned particles. */
