@@ -67,6 +67,11 @@ __device__ __forceinline__ double rem_euclid(double a, double b) {
   return r < 0.0 ? dadd(r, fabs(b)) : r;
 }
 
+// rem_euclid(c, m) for c in [0, 2 m): c, or c - m (exact, Sterbenz) from m
+// on.  A decoded fixed-point coordinate times nm / L lies in [0, nm], so the
+// CIC cell coordinate needs no general remainder.
+__device__ __forceinline__ double rem_once(double c, double m) { return c >= m ? dsub(c, m) : c; }
+
 // minimum_image (crates/gadget-ng-treepm/src/short_range.rs:53-63), exact f64.
 __device__ __forceinline__ double minimum_image(double dx, double box) {
   double half = dmul(box, 0.5);

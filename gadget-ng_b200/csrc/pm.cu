@@ -321,14 +321,25 @@ struct Cic {
   float wx[2], wy[2], wz[2];
 };
 
+// One CIC axis with the integer <-> float64 conversions done by float64
+// adds instead of conversion instructions (the conversion pipe was 93 % busy
+// in the deposit, ahead of every other unit): the exact float64 of q as the
+// bit pattern of 2^52 + q minus 2^52, and floor(c) as the low word of the
+// round-down sum c + 2^52 (c in [0, nm)).  Same values as (double)q, floor and
+// (int) on these ranges; the upper node index wraps without a division.
+constexpr double TWO52 = 4503599627370496.0;
+__device__ __forceinline__ double u32_to_f64(uint32_t q) {
+  return dsub(__hiloint2double(0x43300000, (int)q), TWO52);
+}
+
 __device__ __forceinline__ void cic_axis(uint32_t q, double scale, double inv_cell, double nmf, int nm, int* i,
                                          float* w) {
-  const double c = rem_euclid(dmul(decode(q, scale), inv_cell), nmf);
-  const double f = floor(c);
-  const int i0 = (int)f;
-  const double d = dsub(c, f);
+  const double c = rem_once(dmul(dmul(u32_to_f64(q), scale), inv_cell), nmf);
+  const double t = __dadd_rd(c, TWO52);  // 2^52 + floor(c)
+  const int i0 = __double2loint(t);
+  const double d = dsub(c, dsub(t, TWO52));
   i[0] = i0;
-  i[1] = (i0 + 1) % nm;
+  i[1] = i0 + 1 == nm ? 0 : i0 + 1;
   w[0] = (float)dsub(1.0, d);
   w[1] = (float)d;
 }
@@ -342,19 +353,37 @@ __device__ __forceinline__ Cic cic_of(uint32_t qx, uint32_t qy, uint32_t qz, dou
   return c;
 }
 
-// The particles arrive in octree order, so lanes of a warp often share a
-// CIC cell (in a Plummer core, hundreds of particles share one).  Lanes with
-// the same base cell (hence the same 8 nodes) are grouped with match_any; the
-// group's first lane sums their 8 weighted masses through shuffles and issues
-// the 8 atomics for all of them.  The cell index and the weights are the
-// reference's (float64 position arithmetic, product m wx wy wz).
-__global__ void k_deposit(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+// The particles arrive in octree order, so a warp's 32 particles sit in a
+// compact region and lanes often share a CIC cell.  Lanes with the same base
+// cell are grouped with match_any and the group's first lane sums their 8
+// weighted masses through shuffles.  Those leaders then add their 8 sums into
+// a per-warp 8 x 8 x 8 node window in shared memory placed at the warp's
+// smallest base cell, one corner slot at a time (within a slot every leader
+// writes a different node, so a plain read-modify-write suffices); the
+// window's non-zero nodes then go to the mesh with one atomic each, lanes on
+// consecutive x of a window row so that one atomic instruction covers four
+// mesh rows.  A warp whose base cells do not fit in the window adds its sums
+// to the mesh directly.  At 256^3 (16.7 M particles) the deposit went from
+// 512 to 454 us: neighbouring particles' shared corner nodes take one atomic
+// instead of up to eight.
+constexpr int DEP_THREADS = 256;
+constexpr int DEP_WIN = 8;  // window side (nodes); the flush indexes x, y, z by 3-bit fields
+static_assert(DEP_WIN == 8, "the window flush decodes w as (z << 6) | (y << 3) | x");
+
+// d in (-nm, nm) to the periodic offset in [-nm/2, nm/2)
+__device__ __forceinline__ int wrap_offset(int d, int nm) {
+  return d >= nm / 2 ? d - nm : (d < -nm / 2 ? d + nm : d);
+}
+
+__global__ void __launch_bounds__(DEP_THREADS) k_deposit(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
                           const uint32_t* __restrict__ qz, const float* __restrict__ m, int64_t n, double scale,
                           double inv_cell, int nm, float* __restrict__ rho, const uint32_t* __restrict__ id,
                           uint32_t id_limit) {
+  __shared__ __align__(16) float s_win[DEP_THREADS / 32][DEP_WIN * DEP_WIN * DEP_WIN];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  const bool live = i < n && (!id || id[i] < id_limit);  // halo copies deposit nothing
+  float* win = s_win[threadIdx.x >> 5];
+  const bool live = i < n && (!id || id[i] < id_limit);
   Cic c{};
   float mi = 0.f;
   uint32_t key = 0xFFFFFFFFu;
@@ -365,48 +394,91 @@ __global__ void k_deposit(const uint32_t* __restrict__ qx, const uint32_t* __res
   }
   const uint32_t peers = __match_any_sync(0xffffffffu, key);
   const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
-  const int64_t nm2 = (int64_t)nm * nm;
-  if (rounds == 1) {  // no two lanes share a cell
-    if (!live) return;
+  float sum[8];
+  if (rounds == 1) {
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
       for (int b = 0; b < 2; ++b)
 #pragma unroll
-        for (int d = 0; d < 2; ++d)
-          atomicAdd(&rho[c.iz[a] * nm2 + (int64_t)c.iy[b] * nm + c.ix[d]], mi * c.wx[d] * c.wy[b] * c.wz[a]);
-    return;
-  }
-  float sum[8];
+        for (int d = 0; d < 2; ++d) sum[a * 4 + b * 2 + d] = mi * c.wx[d] * c.wy[b] * c.wz[a];
+  } else {
 #pragma unroll
-  for (int k = 0; k < 8; ++k) sum[k] = 0.f;
-  uint32_t rest = peers;
-  for (int r = 0; r < rounds; ++r) {  // the same count on every lane: full-warp shuffles
-    const int src = rest ? __ffs(rest) - 1 : lane;
-    const bool take = rest != 0u;
-    rest &= rest - 1u;
-    const float sm = __shfl_sync(0xffffffffu, mi, src);
-    const float x0 = __shfl_sync(0xffffffffu, c.wx[0], src), x1 = __shfl_sync(0xffffffffu, c.wx[1], src);
-    const float y0 = __shfl_sync(0xffffffffu, c.wy[0], src), y1 = __shfl_sync(0xffffffffu, c.wy[1], src);
-    const float z0 = __shfl_sync(0xffffffffu, c.wz[0], src), z1 = __shfl_sync(0xffffffffu, c.wz[1], src);
-    if (take) {
-      sum[0] += sm * x0 * y0 * z0;
-      sum[1] += sm * x1 * y0 * z0;
-      sum[2] += sm * x0 * y1 * z0;
-      sum[3] += sm * x1 * y1 * z0;
-      sum[4] += sm * x0 * y0 * z1;
-      sum[5] += sm * x1 * y0 * z1;
-      sum[6] += sm * x0 * y1 * z1;
-      sum[7] += sm * x1 * y1 * z1;
+    for (int k = 0; k < 8; ++k) sum[k] = 0.f;
+    uint32_t rest = peers;
+    for (int r = 0; r < rounds; ++r) {
+      const int src = rest ? __ffs(rest) - 1 : lane;
+      const bool take = rest != 0u;
+      rest &= rest - 1u;
+      const float sm = __shfl_sync(0xffffffffu, mi, src);
+      const float x0 = __shfl_sync(0xffffffffu, c.wx[0], src), x1 = __shfl_sync(0xffffffffu, c.wx[1], src);
+      const float y0 = __shfl_sync(0xffffffffu, c.wy[0], src), y1 = __shfl_sync(0xffffffffu, c.wy[1], src);
+      const float z0 = __shfl_sync(0xffffffffu, c.wz[0], src), z1 = __shfl_sync(0xffffffffu, c.wz[1], src);
+      if (take) {
+        sum[0] += sm * x0 * y0 * z0;
+        sum[1] += sm * x1 * y0 * z0;
+        sum[2] += sm * x0 * y1 * z0;
+        sum[3] += sm * x1 * y1 * z0;
+        sum[4] += sm * x0 * y0 * z1;
+        sum[5] += sm * x1 * y0 * z1;
+        sum[6] += sm * x0 * y1 * z1;
+        sum[7] += sm * x1 * y1 * z1;
+      }
     }
   }
-  if (!live || lane != __ffs(peers) - 1) return;
+  const bool lead = live && lane == __ffs(peers) - 1;
+  const uint32_t leaders = __ballot_sync(0xffffffffu, lead);
+  if (leaders == 0u) return;
+  const int f = __ffs(leaders) - 1;
+  const int o[3] = {__shfl_sync(0xffffffffu, c.ix[0], f), __shfl_sync(0xffffffffu, c.iy[0], f),
+                    __shfl_sync(0xffffffffu, c.iz[0], f)};
+  const int mine[3] = {c.ix[0], c.iy[0], c.iz[0]};
+  int rel[3], lo[3];
+  bool fits = true;
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
+  for (int d = 0; d < 3; ++d) {
+    rel[d] = wrap_offset(mine[d] - o[d], nm);
+    lo[d] = __reduce_min_sync(0xffffffffu, lead ? rel[d] : 0x7FFFFFFF);
+    const int hi = __reduce_max_sync(0xffffffffu, lead ? rel[d] : -0x7FFFFFFF);
+    fits = fits && hi - lo[d] + 2 <= DEP_WIN;
+  }
+  const int64_t nm2 = (int64_t)nm * nm;
+  if (!fits) {
+    if (!lead) return;
 #pragma unroll
-    for (int b = 0; b < 2; ++b)
+    for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int d = 0; d < 2; ++d) atomicAdd(&rho[c.iz[a] * nm2 + (int64_t)c.iy[b] * nm + c.ix[d]], sum[a * 4 + b * 2 + d]);
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int d = 0; d < 2; ++d) atomicAdd(&rho[c.iz[a] * nm2 + (int64_t)c.iy[b] * nm + c.ix[d]], sum[a * 4 + b * 2 + d]);
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < DEP_WIN * DEP_WIN * DEP_WIN / 128; ++k)
+    reinterpret_cast<float4*>(win)[lane + 32 * k] = make_float4(0.f, 0.f, 0.f, 0.f);
+  __syncwarp();
+  const int base = ((rel[2] - lo[2]) * DEP_WIN + (rel[1] - lo[1])) * DEP_WIN + (rel[0] - lo[0]);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (lead) {
+      const int w = base + ((k >> 2) * DEP_WIN + ((k >> 1) & 1)) * DEP_WIN + (k & 1);
+      win[w] += sum[k];
+    }
+    __syncwarp();
+  }
+  // consecutive lanes take consecutive x of a window row, so one atomic
+  // instruction touches four mesh rows
+#pragma unroll 4
+  for (int k = 0; k < DEP_WIN * DEP_WIN * DEP_WIN / 32; ++k) {
+    const int w = lane + 32 * k;
+    const float v = win[w];
+    if (v == 0.f) continue;
+    int gx = o[0] + lo[0] + (w & 7), gy = o[1] + lo[1] + ((w >> 3) & 7), gz = o[2] + lo[2] + (w >> 6);
+    gx = gx < 0 ? gx + nm : (gx >= nm ? gx - nm : gx);
+    gy = gy < 0 ? gy + nm : (gy >= nm ? gy - nm : gy);
+    gz = gz < 0 ? gz + nm : (gz >= nm ? gz - nm : gz);
+    atomicAdd(&rho[gz * nm2 + (int64_t)gy * nm + gx], v);
+  }
 }
 
 __global__ void k_cells(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
@@ -1002,7 +1074,7 @@ void pm_deposit(const PmPlan& p, const uint32_t* qx, const uint32_t* qy, const u
   const int64_t nm3 = (int64_t)p.nm * p.nm * p.nm;
   TPM_CUDA(cudaMemsetAsync(p.rho, 0, sizeof(float) * nm3, s));
   if (n == 0) return;
-  k_deposit<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(qx, qy, qz, massf, n, p.box / TWO32, (double)p.nm / p.box,
+  k_deposit<<<grid_for(n, DEP_THREADS, 1ll << 30), DEP_THREADS, 0, s>>>(qx, qy, qz, massf, n, p.box / TWO32, (double)p.nm / p.box,
                                                         p.nm, p.rho, id, id_limit);
   TPM_LAUNCH_CHECK();
 }
