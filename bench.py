@@ -777,6 +777,8 @@ def run_domain(args):
             stats.append(dom.solver.stats())
         ev1.record(stream)
         torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
     dev_ms = max_over_ranks(ev0.elapsed_time(ev1), "cuda")
     owned = dom.n_owned
     max_owned = int(max_over_ranks(float(owned), "cuda"))

@@ -128,6 +128,42 @@ def test_two_ranks_close_to_serial():
     assert cnt.sum() > 0
 
 
+def test_four_ranks_tail_comes_from_shifted_root_cubes():
+    """Where the decomposed short range departs from the serial one at P = 4.
+    Each rank builds its octree over its own + halo particles
+    (distributed.rs:60-145), whose bounding cube is the root cell.  A rank
+    whose local + halo particles span the serial root cube has the serial
+    cells at every depth and reproduces the serial forces to the r_cut
+    boundary's level (only nodes cut by the halo edge change their COM); a
+    rank whose cube differs has every cell shifted, so its monopoles group
+    other particles, including monopoles that hold the target, and some of
+    its particles feel relative differences of order one.  Morton domains of
+    a perturbed 20^3 lattice: seed 7 has one such rank (rank 0), seeds 8 and
+    9 none."""
+    nm, rs, P = 16, 1.25 / 16, 4
+    for seed, shifted in ((7, {0}), (8, set()), (9, set())):
+        pos, mass = _box(20, seed)
+        keys = dom().morton_keys(pos, np.array([0.0, 0.0, 0.0, 1.0, 1.0, 1.0]))
+        cuts = dom().cutpoints(np.sort(keys), P)
+        owner = np.array([dom().rank_for(k, cuts, P) for k in keys])
+        acc, _, _, halos = dom().distributed_treepm(pos, mass, owner, 1e-6, 1.0, nm, 1.0, rs, 4.5)
+        ref = oracle().treepm(pos, mass, 1e-6, 1.0, nm, 1.0, rs, 4.5)["acc"]
+        rel = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        serial = oracle().octree(pos, mass)
+        found = set()
+        for r in range(P):
+            mine = np.nonzero(owner == r)[0]
+            tree = oracle().octree(pos[np.concatenate([mine, halos[r]])], mass[np.concatenate([mine, halos[r]])])
+            same = np.array_equal(tree["root_center"], serial["root_center"]) and \
+                tree["root_half"] == serial["root_half"]
+            if same:
+                assert rel[mine].max() < 5e-5, (seed, r, rel[mine].max())
+            else:
+                found.add(r)
+                assert rel[mine].max() > 1e-2, (seed, r, rel[mine].max())
+        assert found == shifted, (seed, found)
+
+
 def test_driver_sfc_helpers_match_oracle():
     from treepm import distributed as D
     rng = np.random.default_rng(1)
