@@ -364,11 +364,12 @@ __device__ __forceinline__ Cic cic_of(uint32_t qx, uint32_t qy, uint32_t qz, dou
 // consecutive x of a window row so that one atomic instruction covers four
 // mesh rows.  A warp whose base cells do not fit in the window adds its sums
 // to the mesh directly.  At 256^3 (16.7 M particles) the deposit went from
-// 512 to 454 us: neighbouring particles' shared corner nodes take one atomic
-// instead of up to eight.
+// 512 to 330 us with the window, the used-rows flush and the segmented sums:
+// neighbouring particles' shared corner nodes take one atomic instead of up
+// to eight.
 constexpr int DEP_THREADS = 256;
 constexpr int DEP_WIN = 8;  // window side (nodes); the flush indexes x, y, z by 3-bit fields
-static_assert(DEP_WIN == 8, "the window flush decodes w as (z << 6) | (y << 3) | x");
+static_assert(DEP_WIN == 8, "the flush maps eight lanes to a window row");
 
 // d in (-nm, nm) to the periodic offset in [-nm/2, nm/2)
 __device__ __forceinline__ int wrap_offset(int d, int nm) {
@@ -395,34 +396,48 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(const uint32_t* __restr
   const uint32_t peers = __match_any_sync(0xffffffffu, key);
   const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
   float sum[8];
-  if (rounds == 1) {
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+  for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < 2; ++b)
 #pragma unroll
-        for (int d = 0; d < 2; ++d) sum[a * 4 + b * 2 + d] = mi * c.wx[d] * c.wy[b] * c.wz[a];
-  } else {
+      for (int d = 0; d < 2; ++d) sum[a * 4 + b * 2 + d] = mi * c.wx[d] * c.wy[b] * c.wz[a];
+  if (rounds > 1) {
+    // groups of consecutive lanes (octree order makes them the rule): a
+    // segmented suffix sum, five shuffle steps whatever the group size; the
+    // group's first lane ends with its total
+    const int end = 32 - __clz(peers);
+    if (__all_sync(0xffffffffu, __popc(peers) == end - (__ffs(peers) - 1))) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) sum[k] = 0.f;
-    uint32_t rest = peers;
-    for (int r = 0; r < rounds; ++r) {
-      const int src = rest ? __ffs(rest) - 1 : lane;
-      const bool take = rest != 0u;
-      rest &= rest - 1u;
-      const float sm = __shfl_sync(0xffffffffu, mi, src);
-      const float x0 = __shfl_sync(0xffffffffu, c.wx[0], src), x1 = __shfl_sync(0xffffffffu, c.wx[1], src);
-      const float y0 = __shfl_sync(0xffffffffu, c.wy[0], src), y1 = __shfl_sync(0xffffffffu, c.wy[1], src);
-      const float z0 = __shfl_sync(0xffffffffu, c.wz[0], src), z1 = __shfl_sync(0xffffffffu, c.wz[1], src);
-      if (take) {
-        sum[0] += sm * x0 * y0 * z0;
-        sum[1] += sm * x1 * y0 * z0;
-        sum[2] += sm * x0 * y1 * z0;
-        sum[3] += sm * x1 * y1 * z0;
-        sum[4] += sm * x0 * y0 * z1;
-        sum[5] += sm * x1 * y0 * z1;
-        sum[6] += sm * x0 * y1 * z1;
-        sum[7] += sm * x1 * y1 * z1;
+      for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float y = __shfl_down_sync(0xffffffffu, sum[k], off);
+          if (lane + off < end) sum[k] += y;
+        }
+      }
+    } else {  // scattered groups: the leader gathers its members one at a time
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sum[k] = 0.f;
+      uint32_t rest = peers;
+      for (int r = 0; r < rounds; ++r) {  // the same count on every lane: full-warp shuffles
+        const int src = rest ? __ffs(rest) - 1 : lane;
+        const bool take = rest != 0u;
+        rest &= rest - 1u;
+        const float sm = __shfl_sync(0xffffffffu, mi, src);
+        const float x0 = __shfl_sync(0xffffffffu, c.wx[0], src), x1 = __shfl_sync(0xffffffffu, c.wx[1], src);
+        const float y0 = __shfl_sync(0xffffffffu, c.wy[0], src), y1 = __shfl_sync(0xffffffffu, c.wy[1], src);
+        const float z0 = __shfl_sync(0xffffffffu, c.wz[0], src), z1 = __shfl_sync(0xffffffffu, c.wz[1], src);
+        if (take) {
+          sum[0] += sm * x0 * y0 * z0;
+          sum[1] += sm * x1 * y0 * z0;
+          sum[2] += sm * x0 * y1 * z0;
+          sum[3] += sm * x1 * y1 * z0;
+          sum[4] += sm * x0 * y0 * z1;
+          sum[5] += sm * x1 * y0 * z1;
+          sum[6] += sm * x0 * y1 * z1;
+          sum[7] += sm * x1 * y1 * z1;
+        }
       }
     }
   }
@@ -433,14 +448,15 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(const uint32_t* __restr
   const int o[3] = {__shfl_sync(0xffffffffu, c.ix[0], f), __shfl_sync(0xffffffffu, c.iy[0], f),
                     __shfl_sync(0xffffffffu, c.iz[0], f)};
   const int mine[3] = {c.ix[0], c.iy[0], c.iz[0]};
-  int rel[3], lo[3];
+  int rel[3], lo[3], ext[3];
   bool fits = true;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     rel[d] = wrap_offset(mine[d] - o[d], nm);
     lo[d] = __reduce_min_sync(0xffffffffu, lead ? rel[d] : 0x7FFFFFFF);
     const int hi = __reduce_max_sync(0xffffffffu, lead ? rel[d] : -0x7FFFFFFF);
-    fits = fits && hi - lo[d] + 2 <= DEP_WIN;
+    ext[d] = hi - lo[d] + 2;  // nodes used along this axis
+    fits = fits && ext[d] <= DEP_WIN;
   }
   const int64_t nm2 = (int64_t)nm * nm;
   if (!fits) {
@@ -466,14 +482,20 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(const uint32_t* __restr
     }
     __syncwarp();
   }
-  // consecutive lanes take consecutive x of a window row, so one atomic
-  // instruction touches four mesh rows
-#pragma unroll 4
-  for (int k = 0; k < DEP_WIN * DEP_WIN * DEP_WIN / 32; ++k) {
-    const int w = lane + 32 * k;
-    const float v = win[w];
+  // the used rows of the window to the mesh, four rows per pass with
+  // consecutive lanes on consecutive x, so one atomic instruction touches four
+  // mesh rows; row r is (y, z) = (r mod ext_y, r div ext_y), the division by
+  // a multiply (r < 64, ext_y <= 8)
+  const int rows = ext[1] * ext[2];
+  const uint32_t mdiv = (65536u + (uint32_t)ext[1] - 1u) / (uint32_t)ext[1];
+  const int x = lane & 7;
+  for (int r0 = 0; r0 < rows; r0 += 4) {
+    const int r = r0 + (lane >> 3);
+    if (r >= rows || x >= ext[0]) continue;
+    const int zz = (int)(((uint32_t)r * mdiv) >> 16), yy = r - zz * ext[1];
+    const float v = win[(zz * DEP_WIN + yy) * DEP_WIN + x];
     if (v == 0.f) continue;
-    int gx = o[0] + lo[0] + (w & 7), gy = o[1] + lo[1] + ((w >> 3) & 7), gz = o[2] + lo[2] + (w >> 6);
+    int gx = o[0] + lo[0] + x, gy = o[1] + lo[1] + yy, gz = o[2] + lo[2] + zz;
     gx = gx < 0 ? gx + nm : (gx >= nm ? gx - nm : gx);
     gy = gy < 0 ? gy + nm : (gy >= nm ? gy - nm : gy);
     gz = gz < 0 ? gz + nm : (gz >= nm ? gz - nm : gz);
