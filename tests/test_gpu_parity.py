@@ -331,21 +331,30 @@ def test_host_kdk_steps_reuse_the_resident_acceleration():
     assert rel_err(vel, v_dev)[0] < 1e-5
     dp = (pos - p_dev + 0.5 * b.box_size) % b.box_size - 0.5 * b.box_size
     assert np.max(np.abs(dp)) < 1e-6 * b.box_size
-    # a perturbed state is not the returned one: the speculative step on the
-    # resident state is discarded, the step evaluates twice and still matches a
-    # device step from the same state
-    pos2 = pos.copy()
-    pos2[0, 0] = (pos2[0, 0] + 1e-3) % b.box_size
-    ref = t.TreePmSolver(nm, b.box_size, phys["r_split"], r_cut_factor=4.5)
-    ref.set_particles(pos2, b.mass, vel)
+    # a perturbed state is not the returned one.  Particle 1 is not among the
+    # 256 evenly spaced particles the host compares before it queues any work
+    # (indices k n / 256: 0, 16, 32, ... here), so the step runs speculatively
+    # on the resident state, the device check rejects it, and the step
+    # evaluates twice more; particle 0 is compared on the host, so that state
+    # is stepped from the upload at once (two evaluations, nothing discarded).
+    # Both match a device step from the same state.
     d, k1, k2 = steps[0]
-    ref.kdk_step(k1, d, k2, phys["eps2"], phys["g"])
-    p_ref, v_ref, _ = ref.get_state(b.n)
-    host.kdk_step_host(pos2, vel, b.mass, k1, d, k2, phys["eps2"], phys["g"])
-    assert host.stats()["force_evaluations"] == 7
-    assert rel_err(vel, v_ref)[0] < 1e-5
-    dp = (pos2 - p_ref + 0.5 * b.box_size) % b.box_size - 0.5 * b.box_size
-    assert np.max(np.abs(dp)) < 1e-6 * b.box_size
+    before = host.stats()["force_evaluations"]
+    for idx, extra in ((1, 3), (0, 2)):
+        pos2 = pos.copy()
+        vel2 = vel.copy()
+        pos2[idx, 0] = (pos2[idx, 0] + 1e-3) % b.box_size
+        ref = t.TreePmSolver(nm, b.box_size, phys["r_split"], r_cut_factor=4.5)
+        ref.set_particles(pos2, b.mass, vel2)
+        ref.kdk_step(k1, d, k2, phys["eps2"], phys["g"])
+        p_ref, v_ref, _ = ref.get_state(b.n)
+        host.kdk_step_host(pos2, vel2, b.mass, k1, d, k2, phys["eps2"], phys["g"])
+        assert host.stats()["force_evaluations"] == before + extra, (idx, host.stats()["force_evaluations"])
+        before += extra
+        assert rel_err(vel2, v_ref)[0] < 1e-5
+        dp = (pos2 - p_ref + 0.5 * b.box_size) % b.box_size - 0.5 * b.box_size
+        assert np.max(np.abs(dp)) < 1e-6 * b.box_size
+        pos, vel = pos2, vel2  # the next call hands back what this one returned, then perturbs it
 
 
 def test_host_kdk_step_after_another_call_steps_the_inputs():
