@@ -239,21 +239,26 @@ __global__ void k_oct_nodes(int64_t nb, const int32_t* __restrict__ bpre, const 
                             uint32_t* __restrict__ o_first, uint32_t* __restrict__ o_last,
                             uint32_t* __restrict__ max_depth) {
   int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (b >= nb) return;
-  const uint32_t c = cnt[b];
-  if (c == 0) return;
-  const int32_t par = bparent[b];
-  const int start = (par < 0 ? -1 : bpre[par] / 3) + 1;
-  const int32_t p0 = par < 0 ? -1 : owner_deepest(par, bparent, cnt, base);
-  const uint32_t id0 = base[b];
-  for (uint32_t k = 0; k < c; ++k) {
-    const uint32_t id = id0 + k;
-    o_parent[id] = k == 0 ? p0 : (int32_t)(id - 1);
-    o_depth[id] = (uint8_t)(start + k);
-    o_first[id] = bfirst[b];
-    o_last[id] = blast[b];
+  uint32_t deep = 0;
+  const uint32_t c = b < nb ? cnt[b] : 0u;
+  if (c != 0) {
+    const int32_t par = bparent[b];
+    const int start = (par < 0 ? -1 : bpre[par] / 3) + 1;
+    const int32_t p0 = par < 0 ? -1 : owner_deepest(par, bparent, cnt, base);
+    const uint32_t id0 = base[b];
+    for (uint32_t k = 0; k < c; ++k) {
+      const uint32_t id = id0 + k;
+      o_parent[id] = k == 0 ? p0 : (int32_t)(id - 1);
+      o_depth[id] = (uint8_t)(start + k);
+      o_first[id] = bfirst[b];
+      o_last[id] = blast[b];
+    }
+    deep = (uint32_t)(start + c);
   }
-  atomicMax(max_depth, (uint32_t)(start + c));  // deepest leaf bound
+  // deepest leaf bound: one atomic per warp (one per thread on a single
+  // address serialised the kernel)
+  deep = __reduce_max_sync(0xffffffffu, deep);
+  if ((threadIdx.x & 31) == 0 && deep) atomicMax(max_depth, deep);
 }
 
 __global__ void k_leaf_parents(int64_t n, const int32_t* __restrict__ leaf_bparent,
