@@ -77,35 +77,58 @@ __global__ void k_root(const uint32_t* __restrict__ bb, double scale, TreeParams
 // ---------------------------------------------------------------------------
 // octant-path keys
 // ---------------------------------------------------------------------------
+// 21 octant levels of the reference's insertion octree from the cell state
+// (centre, half side) onward: the digit is the octant of the particle against
+// the centre, then child_center moves the centre by +/- half/2 per axis, all
+// in float64 as the reference does.  The levels are unrolled so the digit
+// shifts are constants.
+__device__ __forceinline__ uint64_t octant_word(double x, double y, double z, double& cx, double& cy, double& cz,
+                                               double& h) {
+  uint64_t key = 0;
+#pragma unroll
+  for (int l = 1; l <= KEY_LEVELS / 2; ++l) {
+    const double q = dmul(h, 0.5);
+    const bool ox = x >= cx, oy = y >= cy, oz = z >= cz;
+    const uint64_t digit = (uint64_t)ox | ((uint64_t)oy << 1) | ((uint64_t)oz << 2);
+    cx = dadd(cx, ox ? q : -q);
+    cy = dadd(cy, oy ? q : -q);
+    cz = dadd(cz, oz ? q : -q);
+    h = q;
+    key |= digit << (63 - 3 * l);
+  }
+  return key;
+}
+
+// Levels 1..21 of every particle (the sort key).  Levels 22..42 only
+// separate particles that share the first 21 (tie runs), so k_tie_low makes
+// them for those alone.
 __global__ void k_tree_keys(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
                             const uint32_t* __restrict__ qz, int64_t n, double scale,
                             const TreeParams* __restrict__ prm, uint64_t* __restrict__ key_hi,
-                            uint64_t* __restrict__ key_lo, uint32_t* __restrict__ perm) {
+                            uint32_t* __restrict__ perm) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double x = decode(qx[i], scale), y = decode(qy[i], scale), z = decode(qz[i], scale);
   double cx = prm->center[0], cy = prm->center[1], cz = prm->center[2], h = prm->half;
-  // levels 1..21 into the high word, 22..42 into the low word; the levels are
-  // unrolled so the digit shifts are constants
-  uint64_t key[2] = {0, 0};
-#pragma unroll
-  for (int w = 0; w < 2; ++w) {
-#pragma unroll
-    for (int l = 1; l <= KEY_LEVELS / 2; ++l) {
-      const double q = dmul(h, 0.5);
-      const bool ox = x >= cx, oy = y >= cy, oz = z >= cz;
-      const uint64_t digit = (uint64_t)ox | ((uint64_t)oy << 1) | ((uint64_t)oz << 2);
-      // child_center: centre + off, off = (0.0 +/- q) per axis
-      cx = dadd(cx, ox ? q : -q);
-      cy = dadd(cy, oy ? q : -q);
-      cz = dadd(cz, oz ? q : -q);
-      h = q;
-      key[w] |= digit << (63 - 3 * l);
-    }
-  }
-  key_hi[i] = key[0];
-  key_lo[i] = key[1];
+  key_hi[i] = octant_word(x, y, z, cx, cy, cz, h);
   perm[i] = (uint32_t)i;
+}
+
+// After the sort: the low word (levels 22..42) of every particle in a run of
+// equal high keys, stored by original index for k_fix_ties.
+__global__ void k_tie_low(const uint32_t* __restrict__ qx, const uint32_t* __restrict__ qy,
+                          const uint32_t* __restrict__ qz, int64_t n, double scale,
+                          const TreeParams* __restrict__ prm, const uint64_t* __restrict__ hi,
+                          const uint32_t* __restrict__ perm, uint64_t* __restrict__ lo_by_index) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t k = hi[i];
+  if (!((i > 0 && hi[i - 1] == k) || (i + 1 < n && hi[i + 1] == k))) return;
+  const uint32_t j = perm[i];
+  const double x = decode(qx[j], scale), y = decode(qy[j], scale), z = decode(qz[j], scale);
+  double cx = prm->center[0], cy = prm->center[1], cz = prm->center[2], h = prm->half;
+  (void)octant_word(x, y, z, cx, cy, cz, h);
+  lo_by_index[j] = octant_word(x, y, z, cx, cy, cz, h);
 }
 
 // Runs of equal high keys (particles sharing the first 21 octant levels) are
@@ -121,7 +144,7 @@ __global__ void k_fix_ties(int64_t n, const uint64_t* __restrict__ hi, uint32_t*
   const bool starts = (i == 0 || hi[i - 1] != k) && (i + 1 < n && hi[i + 1] == k);
   const bool inside = (i > 0 && hi[i - 1] == k);
   if (!starts) {
-    if (!inside) lo_sorted[i] = lo_by_index[perm[i]];
+    if (!inside) lo_sorted[i] = 0;  // a particle alone in its level-21 cell: its low word is never read
     return;
   }
   int64_t e = i + 1;
@@ -738,11 +761,14 @@ void launch_bbox_root(const Particles& p, int64_t n, double box, TreeBuffers& t,
 
 void launch_tree_keys(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s) {
   k_tree_keys<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(p.qx, p.qy, p.qz, n, box / TWO32, t.params, t.key_hi,
-                                                          t.key_lo_tmp, t.perm);
+                                                          t.perm);
   TPM_LAUNCH_CHECK();
 }
 
-void launch_fix_ties(int64_t n, TreeBuffers& t, cudaStream_t s) {
+void launch_fix_ties(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s) {
+  k_tie_low<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(p.qx, p.qy, p.qz, n, box / TWO32, t.params, t.key_hi,
+                                                        t.perm, t.key_lo_tmp);
+  TPM_LAUNCH_CHECK();
   k_fix_ties<<<grid_for(n, 256, 1ll << 30), 256, 0, s>>>(n, t.key_hi, t.perm, t.key_lo_tmp, t.key_lo, t.err);
   TPM_LAUNCH_CHECK();
 }

@@ -103,7 +103,7 @@ constexpr int DEPTH_BINS = 64;  // octree depths are at most KEY_LEVELS
 
 void launch_bbox_root(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s);
 void launch_tree_keys(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s);
-void launch_fix_ties(int64_t n, TreeBuffers& t, cudaStream_t s);
+void launch_fix_ties(const Particles& p, int64_t n, double box, TreeBuffers& t, cudaStream_t s);
 void launch_permute(const Particles& src, const Particles& dst, int64_t n, const uint32_t* perm, cudaStream_t s);
 void launch_karras(int64_t n, TreeBuffers& t, cudaStream_t s);
 void launch_octree_nodes(int64_t n, TreeBuffers& t, cudaStream_t s);

@@ -547,7 +547,7 @@ void fe_sort(tpm_handle* h) {
     launch_tree_keys(h->P[h->cur], n, box, T, s);
     TPM_CUDA(cudaEventRecord(h->ev[1], s));
     radix_sort_u64(T.key_hi, T.perm, n, 63, h->sort_scratch, h->sort_bytes, s);
-    launch_fix_ties(n, T, s);
+    launch_fix_ties(h->P[h->cur], n, box, T, s);
     launch_permute(h->P[h->cur], h->P[1 - h->cur], n, T.perm, s);
     h->cur = 1 - h->cur;
     TPM_CUDA(cudaEventRecord(h->ev[2], s));
