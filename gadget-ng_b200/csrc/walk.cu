@@ -210,11 +210,18 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
       s = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
     }
     const bool in = (mask >> t) & 1u;
-    const bool ok = in && s <= a.prc2_lo;
+    bool ok = in && s <= a.prc2_lo;
     if (!ACC) {  // accurate mode reproduces no float64 decisions
       // s in (prc2_lo, prc2_hi]: positive floats order like their bit patterns
       bool amb = in && (__float_as_uint(s) - a.prc2_lo_bits - 1u) < a.pband_bits;
-      if (MONO) amb = amb || (in && r2b < a.tiny_u);
+      if (MONO) {
+        // a centre of mass within a few quanta of the target: resolve_list
+        // alone decides it (take it, or open it when it is the target's own
+        // position), so it must not enter the sum here as well
+        const bool near = in && r2b < a.tiny_u;
+        amb = amb || near;
+        ok = ok && !near;
+      }
       amb_any = amb_any || amb;
     }
     float f = pair_factor<ACC>(a, r2b, A.w);

@@ -132,6 +132,32 @@ def test_short_range_parity_and_interaction_set(kind):
     assert rms < 1e-4, (rms, p99)
 
 
+def test_monopole_with_centre_next_to_its_target_counts_once():
+    """A terminal cell holding the target and one neighbour two fixed-point
+    quanta away is a monopole whose centre of mass lies one quantum from the
+    target (the reference takes it, short_range.rs:316-323).  Its float
+    distance falls below the walk's coincidence threshold, so the float64
+    test decides it, and it must enter the sum and the count exactly once."""
+    import types
+    t = treepm()
+    L, ns, nm = 100.0, 16, 16
+    g = (np.arange(ns) + 0.5) * (L / ns)
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    q = np.round(np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1) / L * 2.0 ** 32)
+    k = 5 * ns * ns + 7 * ns + 9
+    q = np.vstack([q, q[k] + np.array([2.0, 0.0, 0.0])])  # the neighbour: two quanta along x
+    pos = q * (L / 2.0 ** 32)
+    b = types.SimpleNamespace(positions=lambda: pos, mass=np.full(pos.shape[0], 1.0 / pos.shape[0]), n=pos.shape[0],
+                              box_size=L)
+    s, sr, ref, cnt, st = _sr_parity(b, nm)
+    per = s.interaction_counts(b.n)
+    for i in (k, b.n - 1):
+        assert cnt[i, 1] >= 1, cnt[i]
+        assert np.array_equal(per[i], cnt[i]), (i, per[i], cnt[i])
+    assert np.array_equal(per, cnt)
+    assert global_rel(sr, ref) < RMS_TOL
+
+
 def test_short_range_aperiodic_parity():
     b = small_box(16, 100.0, 1.0, 21)
     s, sr, ref, cnt, st = _sr_parity(b, 32, periodic=False)
