@@ -188,13 +188,14 @@ __global__ void k_permute(Particles src, Particles dst, int64_t n, const uint32_
 // ---------------------------------------------------------------------------
 // binary radix tree (Karras 2012, section 4)
 // ---------------------------------------------------------------------------
-// Common prefix, in bits of the 126-bit digit string, of sorted keys i and j.
-__device__ __forceinline__ int delta(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, int64_t n,
-                                     int64_t i, int64_t j) {
-  if (j < 0 || j >= n) return -1;
-  uint64_t a = hi[i] ^ hi[j];
+// Common prefix, in bits of the 126-bit digit string, of sorted keys i
+// (preloaded) and j; j out of [0, n) on either side gives -1.
+__device__ __forceinline__ int delta_i(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, int64_t n,
+                                       uint64_t hi_i, uint64_t lo_i, int64_t i, int64_t j) {
+  if ((uint64_t)j >= (uint64_t)n) return -1;
+  const uint64_t a = hi_i ^ __ldg(&hi[j]);
   if (a) return __clzll((long long)a) - 1;
-  uint64_t b = lo[i] ^ lo[j];
+  const uint64_t b = lo_i ^ __ldg(&lo[j]);
   if (b) return 63 + __clzll((long long)b) - 1;
   return 126 + __clzll((long long)(i ^ j));
 }
@@ -205,21 +206,24 @@ __global__ void k_karras(int64_t n, const uint64_t* __restrict__ hi, const uint6
                          int32_t* __restrict__ leaf_bparent) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
-  const int d = (delta(hi, lo, n, i, i + 1) - delta(hi, lo, n, i, i - 1)) >= 0 ? 1 : -1;
-  const int dmin = delta(hi, lo, n, i, i - d);
+  const uint64_t hi_i = hi[i], lo_i = lo[i];
+  // the direction d and the steps along it (i + k d as a sign choice, not a product)
+  const bool up = delta_i(hi, lo, n, hi_i, lo_i, i, i + 1) - delta_i(hi, lo, n, hi_i, lo_i, i, i - 1) >= 0;
+  auto at = [&](int64_t k) { return up ? i + k : i - k; };
+  const int dmin = delta_i(hi, lo, n, hi_i, lo_i, i, at(-1));
   int64_t lmax = 2;
-  while (delta(hi, lo, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  while (delta_i(hi, lo, n, hi_i, lo_i, i, at(lmax)) > dmin) lmax <<= 1;
   int64_t l = 0;
   for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
-    if (delta(hi, lo, n, i, i + (l + t) * d) > dmin) l += t;
-  const int64_t j = i + l * d;
-  const int dnode = delta(hi, lo, n, i, j);
+    if (delta_i(hi, lo, n, hi_i, lo_i, i, at(l + t)) > dmin) l += t;
+  const int64_t j = at(l);
+  const int dnode = delta_i(hi, lo, n, hi_i, lo_i, i, j);
   int64_t s = 0, t = l;
   do {
     t = (t + 1) >> 1;
-    if (delta(hi, lo, n, i, i + (s + t) * d) > dnode) s += t;
+    if (delta_i(hi, lo, n, hi_i, lo_i, i, at(s + t)) > dnode) s += t;
   } while (t > 1);
-  const int64_t gamma = i + s * d + (d < 0 ? -1 : 0);
+  const int64_t gamma = at(s) + (up ? 0 : -1);
   const int64_t first = i < j ? i : j, last = i < j ? j : i;
   const bool left_leaf = first == gamma, right_leaf = last == gamma + 1;
   bl[i] = (uint32_t)gamma | (left_leaf ? LEAF_BIT : 0u);
