@@ -84,7 +84,7 @@ __device__ __forceinline__ double aabb_axis(double dc, double h) {
 }
 
 // min_dist2_to_aabb_periodic (short_range.rs:72-84) or its aperiodic twin (:173-181).
-__device__ double d2_aabb(const double xi[3], const double com[3], double h, double box, int periodic) {
+__device__ __forceinline__ double d2_aabb(const double xi[3], const double com[3], double h, double box, int periodic) {
   double e[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -115,7 +115,7 @@ __device__ __forceinline__ void node_com(const WalkArgs& a, uint32_t node, doubl
 }
 
 // Does target p keep open internal node `node` (cull test only)?
-__device__ bool exact_open_pass(const WalkArgs& a, uint32_t p, uint32_t node) {
+__device__ __forceinline__ bool exact_open_pass(const WalkArgs& a, uint32_t p, uint32_t node) {
   double xi[3], c[3];
   target_pos(a, p, xi);
   node_com(a, node, c);
@@ -125,7 +125,7 @@ __device__ bool exact_open_pass(const WalkArgs& a, uint32_t p, uint32_t node) {
 
 // Terminal node decision: 0 = skip, 1 = interact, 2 = open for this target
 // (monopole whose centre of mass coincides with the target).
-__device__ int exact_terminal(const WalkArgs& a, uint32_t p, uint32_t node) {
+__device__ __forceinline__ int exact_terminal(const WalkArgs& a, uint32_t p, uint32_t node) {
   double xi[3], c[3];
   target_pos(a, p, xi);
   node_com(a, node, c);
@@ -235,7 +235,7 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
 
 // Float64 decisions for this lane's borderline pairs of one list (rare).
 template <bool MONO, int TPW>
-__device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float tx,
+__device__ __forceinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float tx,
                                           float ty, float tz, float* f3, uint32_t* nok, uint32_t* nexact) {
   constexpr int STRIDE = 32 / TPW;
   const int t = lane & (TPW - 1);
