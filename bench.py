@@ -785,6 +785,10 @@ def run_domain(args):
     max_halo = int(max_over_ranks(float(max(halos) if halos else 0), "cuda"))
     stage_ms = {k: float(np.mean([s[k] for s in stats])) for k in
                 ("ms_bbox_keys", "ms_sort", "ms_build", "ms_walk", "ms_pm", "ms_gather_kick", "ms_total")}
+    # the dominant kernel on rank 0's GPU: its walk over its own particles and halos
+    inter0 = float(np.mean([s["leaf_pairs"] + s["monopoles"] for s in stats]))
+    achieved0 = inter0 * FLOP_PER_INTERACTION / (stage_ms["ms_walk"] * 1e-3) / 1e12
+    peak0 = None if args.no_peak else fp32_peak_tflops(dom.solver)
     line = {
         "metric": "particle-updates/s", "value": n * args.steps / (dev_ms * 1e-3), "unit": "particle-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
@@ -797,7 +801,13 @@ def run_domain(args):
                    "l2": "inputs larger than L2 (>= 0.8 GB touched per step)"},
         "domain": {"max_owned": max_owned, "max_halo_particles": max_halo,
                    "halo_fraction": max_halo / max(max_owned, 1), "stage_ms_rank0": stage_ms},
+        "roofline": {"bound": "fp32", "achieved": achieved0, "peak": peak0, "unit": "TFLOP/s",
+                     "frac": (achieved0 / peak0) if peak0 else None, "traffic": None,
+                     "kernel": "k_walk (short-range erfc walk) on rank 0",
+                     "note": f"{FLOP_PER_INTERACTION} FLOP per reference interaction of rank 0's walk / its "
+                             "CUDA-event walk time; peak = FFMA throughput measured live on rank 0's GPU"},
         "e2e": None,
+        "e2e_note": "the domain-decomposed path keeps its particles resident and has no host-buffer step",
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "clocks": clocks.summary(),
     }

@@ -206,6 +206,34 @@ def test_pm_mesh_matches_oracle_mesh():
         assert np.sqrt(np.mean((got - want) ** 2)) < 2e-6 * np.sqrt(np.mean(want ** 2))
 
 
+@pytest.mark.parametrize("layout", ["corner_clump", "sparse", "one_cell"])
+def test_deposit_windows_match_oracle(layout):
+    """The deposit sums neighbouring particles' corner nodes in a per-warp
+    node window before the mesh atomics: a dense clump straddling the corner
+    of the periodic box (windows that wrap on every axis), particles spread
+    too far for one window (the direct path), and hundreds of particles in one
+    cell (whole warps sharing a base cell).  The density equals the
+    restatement's CIC (cic.rs:37-93) to float32 rounding."""
+    t = treepm()
+    rng = np.random.default_rng({"corner_clump": 3, "sparse": 4, "one_cell": 5}[layout])
+    L, nm = 32.0, 32
+    if layout == "corner_clump":
+        pos = np.mod(rng.normal(0.0, 1.5, (6000, 3)), L)
+    elif layout == "sparse":
+        pos = rng.uniform(0.0, L, (3000, 3))
+    else:
+        pos = np.mod(np.array([7.3, 19.6, 30.9]) + rng.uniform(0.0, 0.9, (900, 3)), L)
+    q = np.floor(pos / L * 2.0 ** 32) % 2.0 ** 32
+    pos = q * (L / 2.0 ** 32)
+    mass = rng.uniform(0.5, 1.5, pos.shape[0])
+    s = t.PmSolver(nm, L)
+    s.accelerations_for_indices(pos, mass, 0.0, 1.0, [0])
+    rho = s.mesh()[0]
+    ref = oracle().cic_assign(pos, mass, L, nm)
+    assert np.max(np.abs(rho - ref)) < 2e-6 * np.max(ref), np.max(np.abs(rho - ref)) / np.max(ref)
+    assert abs(float(np.sum(rho, dtype=np.float64)) - float(np.sum(ref))) < 1e-5 * float(np.sum(ref))
+
+
 @pytest.mark.parametrize("kind", ["lattice", "clustered"])
 def test_treepm_parity(kind):
     t = treepm()
