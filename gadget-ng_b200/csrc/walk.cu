@@ -700,12 +700,10 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
       wide = wide || ((int64_t)mx - (int64_t)mn > WIDE_GROUP);
     }
     wide = wide || a.single_target;
-    if (!wide) {
-      walk_targets<TPW, ACC>(a, first, count, list_l, list_m, owner, stk, rpos, rmask);
-    } else {
-      for (uint32_t t = 0; t < count; ++t)
-        walk_targets<TPW, ACC>(a, first + t, 1u, list_l, list_m, owner, stk, rpos, rmask);
-    }
+    // one call site: the group at once, or its targets one at a time
+    const uint32_t walks = wide ? count : 1u;
+    for (uint32_t t = 0; t < walks; ++t)
+      walk_targets<TPW, ACC>(a, wide ? first + t : first, wide ? 1u : count, list_l, list_m, owner, stk, rpos, rmask);
   }
 }
 
