@@ -530,13 +530,17 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     __syncwarp();
     // before the next check the pop adds up to 32 monopole entries (accurate
     // mode) and the next classification up to 32 to either list
-    if (nll > CHUNK_L - 32 || nlm > chunk_m<ACC>() - (ACC ? 64 : 32)) {
-      flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, tf[0], tf[1], tf[2], acc, nleaf, nmono, nexact, neval);
+    // (one call site of the list evaluation, the last flush included: the
+    // kernel's code stays small enough for the instruction cache)
+    const bool done = sp == 0;
+    if (done || nll > CHUNK_L - 32 || nlm > chunk_m<ACC>() - (ACC ? 64 : 32)) {
+      if (nll + nlm > 0)
+        flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, tf[0], tf[1], tf[2], acc, nleaf, nmono, nexact, neval);
       __syncwarp();
       nll = 0;
       nlm = 0;
     }
-    if (sp == 0) break;
+    if (done) break;
     // ---- pop a batch whose children fill at most one warp
     const int avail = sp < 32 ? sp : 32;
     uint4 e = make_uint4(0u, 0u, 0u, 0u);
@@ -624,9 +628,6 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       item = ofirst + ((uint32_t)lane - oexcl);
       imask = omask;
     }
-  }
-  if (nll + nlm > 0) {
-    flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, tf[0], tf[1], tf[2], acc, nleaf, nmono, nexact, neval);
   }
   __syncwarp();
   if (TPW < 32) {  // fold the two lanes of each target
