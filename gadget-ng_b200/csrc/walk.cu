@@ -235,7 +235,7 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
 
 // Float64 decisions for this lane's borderline pairs of one list (rare).
 template <bool MONO, int TPW>
-__device__ __forceinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float tx,
+__device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float tx,
                                           float ty, float tz, float* f3, uint32_t* nok, uint32_t* nexact) {
   constexpr int STRIDE = 32 / TPW;
   const int t = lane & (TPW - 1);
