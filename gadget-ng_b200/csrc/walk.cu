@@ -36,7 +36,7 @@ namespace {
 
 constexpr int WALK_WARPS = 4;
 constexpr int WALK_THREADS = WALK_WARPS * 32;
-constexpr int CHUNK_L = 48;  // leaf-list capacity (small lists leave the L1 to the tree records)
+constexpr int CHUNK_L = 64;  // leaf-list capacity (walk 72.9 -> 72.5 ms at 256^3 against 48; 32 is slower)
 // monopole-list capacity: the accurate mode also emits monopoles at pop time
 template <bool ACC> constexpr int chunk_m() { return ACC ? 96 : 64; }
 constexpr int32_t WIDE_GROUP = 1 << 28;  // quanta: 1/16 of the box
