@@ -184,19 +184,29 @@ struct Acc {
   }
 };
 
-// Evaluate one interaction list against this lane's target.  MONO selects the
-// monopole list (AABB-gap test) or the leaf list (bare-distance test; the
-// aperiodic walk's leaves carry their half side and take the AABB test too).
-// Borderline pairs are left out here and flagged; resolve_list settles them.
-template <bool MONO, int TPW, bool ACC>
-__device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, int nl, int lane, float tx, float ty,
-                                           float tz, float& fx, float& fy, float& fz, uint32_t& nok, bool& amb_any) {
-  // TPW targets per warp; with 16, lanes t and t + 16 share target t and
-  // take alternate entries
-  constexpr int STRIDE = 32 / TPW;
-  const int t = lane & (TPW - 1);
+// Lanes of the pair phase.  A group of c targets leaves 32 - c lanes without
+// a target of their own, so R = 32 / c lanes share each target: lane l
+// evaluates target l % c against entries l / c, l / c + R, ... of each list
+// (lanes from R c on evaluate nothing), and the R partial sums of a target
+// are folded when its walk ends.  Packed in one register: target | first
+// entry << 8 | R << 16.
+__device__ __forceinline__ uint32_t pair_lanes(int lane, uint32_t c) {
+  const uint32_t r = 32u / c, t = (uint32_t)lane % c, off = (uint32_t)lane / c;
+  return t | ((off < r ? off : 255u) << 8) | (r << 16);
+}
+
+// Evaluate one interaction list against this lane's pair-phase target.  MONO
+// selects the monopole list (AABB-gap test) or the leaf list (bare-distance
+// test; the aperiodic walk's leaves carry their half side and take the AABB
+// test too).  Borderline pairs are left out here and flagged; resolve_list
+// settles them.
+template <bool MONO, bool ACC>
+__device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, int nl, uint32_t lanes, float tx,
+                                           float ty, float tz, float& fx, float& fy, float& fz, uint32_t& nok,
+                                           bool& amb_any) {
+  const int t = lanes & 0xffu, stride = lanes >> 16;
 #pragma unroll 1
-  for (int e = lane / TPW; e < nl; e += STRIDE) {
+  for (int e = (lanes >> 8) & 0xffu; e < nl; e += stride) {
     const float4 A = *reinterpret_cast<const float4*>(&L[e].x);
     const uint4 B = *reinterpret_cast<const uint4*>(&L[e].h);
     const float h = __uint_as_float(B.x);
@@ -234,12 +244,11 @@ __device__ __forceinline__ void flush_list(const WalkArgs& a, const Entry* L, in
 }
 
 // Float64 decisions for this lane's borderline pairs of one list (rare).
-template <bool MONO, int TPW>
-__device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, int lane, uint32_t p, float tx,
-                                          float ty, float tz, float* f3, uint32_t* nok, uint32_t* nexact) {
-  constexpr int STRIDE = 32 / TPW;
-  const int t = lane & (TPW - 1);
-  for (int e = lane / TPW; e < nl; e += STRIDE) {
+template <bool MONO>
+__device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int nl, uint32_t lanes, uint32_t p,
+                                          float tx, float ty, float tz, float* f3, uint32_t* nok, uint32_t* nexact) {
+  const int t = lanes & 0xffu, stride = lanes >> 16;
+  for (int e = (lanes >> 8) & 0xffu; e < nl; e += stride) {
     const float4 A = *reinterpret_cast<const float4*>(&L[e].x);
     const uint4 B = *reinterpret_cast<const uint4*>(&L[e].h);
     const float h = __uint_as_float(B.x);
@@ -268,19 +277,27 @@ __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int
   }
 }
 
-// Evaluate both interaction lists against this lane's target.
-template <int TPW, bool ACC>
+// Evaluate both interaction lists against this lane's pair-phase target
+// (pair_lanes; its position is read from the lane that holds it, its
+// particle is first + target).
+template <bool ACC>
 __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nll, const Entry* Lm, int nlm, int lane,
-                                      uint32_t p, float tx, float ty, float tz, Acc& acc, uint32_t& nleaf, uint32_t& nmono, uint32_t& nexact, uint32_t& neval) {
+                                      uint32_t count, uint32_t first, const float* tf, Acc& acc, uint32_t& nleaf,
+                                      uint32_t& nmono, uint32_t& nexact, uint32_t& neval) {
+  const uint32_t lanes = pair_lanes(lane, count);  // recomputed here: one register less across the traversal
   float fx = 0.f, fy = 0.f, fz = 0.f;
   bool amb_any = false;
   neval += (uint32_t)(nll + nlm);
-  flush_list<false, TPW, ACC>(a, Ll, nll, lane, tx, ty, tz, fx, fy, fz, nleaf, amb_any);
-  flush_list<true, TPW, ACC>(a, Lm, nlm, lane, tx, ty, tz, fx, fy, fz, nmono, amb_any);
+  const int t = lanes & 0xffu;
+  const float tx = __shfl_sync(0xffffffffu, tf[0], t), ty = __shfl_sync(0xffffffffu, tf[1], t);
+  const float tz = __shfl_sync(0xffffffffu, tf[2], t);
+  flush_list<false, ACC>(a, Ll, nll, lanes, tx, ty, tz, fx, fy, fz, nleaf, amb_any);
+  flush_list<true, ACC>(a, Lm, nlm, lanes, tx, ty, tz, fx, fy, fz, nmono, amb_any);
   if (!ACC && amb_any) {
     float f3[3] = {fx, fy, fz};
-    resolve_list<false, TPW>(a, Ll, nll, lane, p, tx, ty, tz, f3, &nleaf, &nexact);
-    resolve_list<true, TPW>(a, Lm, nlm, lane, p, tx, ty, tz, f3, &nmono, &nexact);
+    const uint32_t p = first + (uint32_t)t;
+    resolve_list<false>(a, Ll, nll, lanes, p, tx, ty, tz, f3, &nleaf, &nexact);
+    resolve_list<true>(a, Lm, nlm, lanes, p, tx, ty, tz, f3, &nmono, &nexact);
     fx = f3[0];
     fy = f3[1];
     fz = f3[2];
@@ -535,7 +552,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     const bool done = sp == 0;
     if (done || nll > CHUNK_L - 32 || nlm > chunk_m<ACC>() - (ACC ? 64 : 32)) {
       if (nll + nlm > 0)
-        flush<TPW, ACC>(a, Ll, nll, Lm, nlm, lane, p, tf[0], tf[1], tf[2], acc, nleaf, nmono, nexact, neval);
+        flush<ACC>(a, Ll, nll, Lm, nlm, lane, count, first, tf, acc, nleaf, nmono, nexact, neval);
       __syncwarp();
       nll = 0;
       nlm = 0;
@@ -630,14 +647,20 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     }
   }
   __syncwarp();
-  if (TPW < 32) {  // fold the two lanes of each target
-    float ox = __shfl_xor_sync(0xffffffffu, acc.sx, 16), oy = __shfl_xor_sync(0xffffffffu, acc.sy, 16);
-    float oz = __shfl_xor_sync(0xffffffffu, acc.sz, 16);
-    float cx = __shfl_xor_sync(0xffffffffu, acc.cx, 16), cy = __shfl_xor_sync(0xffffffffu, acc.cy, 16);
-    float cz = __shfl_xor_sync(0xffffffffu, acc.cz, 16);
-    acc.add(ox - cx, oy - cy, oz - cz);
-    nleaf += __shfl_xor_sync(0xffffffffu, nleaf, 16);
-    nmono += __shfl_xor_sync(0xffffffffu, nmono, 16);
+  // fold the R pair-phase lanes of each target (lanes t + j count) into lane t
+  const uint32_t nrep = 32u / count;
+  for (uint32_t j = 1; j < nrep; ++j) {
+    const int src = lane + (int)(j * count);  // in range for the lanes t < count that keep the result
+    const float ox = __shfl_sync(0xffffffffu, acc.sx, src), oy = __shfl_sync(0xffffffffu, acc.sy, src);
+    const float oz = __shfl_sync(0xffffffffu, acc.sz, src);
+    const float cx = __shfl_sync(0xffffffffu, acc.cx, src), cy = __shfl_sync(0xffffffffu, acc.cy, src);
+    const float cz = __shfl_sync(0xffffffffu, acc.cz, src);
+    const uint32_t ol = __shfl_sync(0xffffffffu, nleaf, src), om = __shfl_sync(0xffffffffu, nmono, src);
+    if ((uint32_t)lane < count) {
+      acc.add(ox - cx, oy - cy, oz - cz);
+      nleaf += ol;
+      nmono += om;
+    }
   }
   if (has && lane < TPW) {
     a.ax[p] = (acc.sx - acc.cx) * a.out_scale;
@@ -646,7 +669,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     a.pcounts[2 * (int64_t)p] = nleaf;
     a.pcounts[2 * (int64_t)p + 1] = nmono;
   }
-  if (lane >= TPW) nleaf = nmono = 0;  // counted once per target
+  if ((uint32_t)lane >= count || lane >= TPW) nleaf = nmono = 0;  // counted once per target
   // statistics
   unsigned long long l = nleaf, m = nmono, x = nexact;
   for (int off = 16; off > 0; off >>= 1) {
@@ -657,7 +680,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
   if (lane == 0) {
     atomicAdd(&a.stats[0], l);
     atomicAdd(&a.stats[1], m);
-    atomicAdd(&a.stats[2], (unsigned long long)neval * (unsigned long long)TPW);
+    atomicAdd(&a.stats[2], (unsigned long long)neval * 32ull / nrep);  // lane evaluations
     atomicAdd(&a.stats[3], x);
   }
 }
