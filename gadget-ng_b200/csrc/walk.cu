@@ -18,8 +18,11 @@
 // internal nodes get a per-target test when they are popped, which refines the
 // mask, so the hierarchical culls of the reference are reproduced exactly.
 // Terminal nodes (leaves and monopole-depth cells) go to an interaction list
-// in shared memory; every lane evaluates the whole list against its own
-// target with its own final test fused into the pair kernel.  Any decision
+// in shared memory; the lanes evaluate the list against the group's targets
+// with each target's own final test fused into the pair kernel (a group of c
+// targets gives every target 32 / c lanes, each on a share of the entries).
+// The running per-target sums stay in shared memory between list flushes, so
+// the traversal keeps its registers (and more resident warps).  Any decision
 // that falls inside a narrow band around r_cut is re-evaluated in float64
 // with the reference's exact expression, so the interaction set equals the
 // reference's.  Pair arithmetic is FP32: exact fixed-point differences split
@@ -280,11 +283,15 @@ __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int
 // Evaluate both interaction lists against this lane's pair-phase target
 // (pair_lanes; its position is read from the lane that holds it, its
 // particle is first + target).
+// The lane's running sums live in shared memory between flushes (s0 = sx, sy,
+// sz, cx; s1 = cy, cz, leaf count, monopole count bits), so they hold no
+// registers across the traversal.
 template <bool ACC>
 __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nll, const Entry* Lm, int nlm, int lane,
-                                      uint32_t count, uint32_t first, const float* tf, Acc& acc, uint32_t& nleaf,
-                                      uint32_t& nmono, uint32_t& nexact, uint32_t& neval) {
+                                      uint32_t count, uint32_t first, const float* tf, float4* s0, float4* s1,
+                                      uint32_t& nexact, uint32_t& neval) {
   const uint32_t lanes = pair_lanes(lane, count);  // recomputed here: one register less across the traversal
+  uint32_t nleaf = 0, nmono = 0;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   bool amb_any = false;
   neval += (uint32_t)(nll + nlm);
@@ -303,7 +310,12 @@ __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nl
     fz = f3[2];
   }
   __syncwarp();
+  const float4 A = s0[lane], B = s1[lane];
+  Acc acc = {A.x, A.y, A.z, A.w, B.x, B.y};
   acc.add(fx, fy, fz);
+  s0[lane] = make_float4(acc.sx, acc.sy, acc.sz, acc.cx);
+  s1[lane] = make_float4(acc.cy, acc.cz, __uint_as_float(__float_as_uint(B.z) + nleaf),
+                         __uint_as_float(__float_as_uint(B.w) + nmono));
 }
 
 // Stack entry of an open node: its children's record range, mask of the
@@ -320,7 +332,7 @@ constexpr uint32_t INFO_MAC = 0x40000000u;  // opening angle undecided for the g
 // Walk the tree for targets [first, first + count) (count <= TPW) with one warp.
 template <int TPW, bool ACC>
 __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, Entry* Ll, Entry* Lm, uint8_t* owner,
-                             StackEntry* stk, float4* rpos, uint4* rmask) {
+                             StackEntry* stk, float4* rpos, uint4* rmask, float4* s0, float4* s1) {
   const int lane = threadIdx.x & 31;
   const int tgt = lane & (TPW - 1);  // this lane's target within the group
   const uint32_t p = first + ((uint32_t)tgt < count ? (uint32_t)tgt : 0u);
@@ -343,8 +355,9 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     bmax[d] = (float)mx * a.u_inv;
   }
   const uint32_t mask0 = __ballot_sync(0xffffffffu, has && lane < TPW);  // bit t: target t
-  Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  uint32_t nleaf = 0, nmono = 0, nexact = 0, neval = 0;
+  s0[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+  s1[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+  uint32_t nexact = 0, neval = 0;
   int nll = 0, nlm = 0, sp = 0;
 
   // the first item is the root record
@@ -354,11 +367,10 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
   // each iteration pops at least one node, so a walk over a well-formed tree
   // ends within (internal nodes + 1) iterations; the cap turns a malformed
   // tree into an error flag instead of an endless loop
-  const int64_t max_iter = a.n_int + 2;
-  int64_t iter = 0;
+  uint32_t iter_left = (uint32_t)(a.n_int + 2 < 0xFFFFFFFFll ? a.n_int + 2 : 0xFFFFFFFFll);
 
   for (;;) {
-    if (++iter > max_iter) {
+    if (iter_left-- == 0u) {
       if (lane == 0) atomicOr(a.err, DEV_ERR_STACK);
       break;
     }
@@ -552,7 +564,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     const bool done = sp == 0;
     if (done || nll > CHUNK_L - 32 || nlm > chunk_m<ACC>() - (ACC ? 64 : 32)) {
       if (nll + nlm > 0)
-        flush<ACC>(a, Ll, nll, Lm, nlm, lane, count, first, tf, acc, nleaf, nmono, nexact, neval);
+        flush<ACC>(a, Ll, nll, Lm, nlm, lane, count, first, tf, s0, s1, nexact, neval);
       __syncwarp();
       nll = 0;
       nlm = 0;
@@ -647,6 +659,10 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     }
   }
   __syncwarp();
+  __syncwarp();
+  const float4 S0 = s0[lane], S1 = s1[lane];
+  Acc acc = {S0.x, S0.y, S0.z, S0.w, S1.x, S1.y};
+  uint32_t nleaf = __float_as_uint(S1.z), nmono = __float_as_uint(S1.w);
   // fold the R pair-phase lanes of each target (lanes t + j count) into lane t
   const uint32_t nrep = 32u / count;
   for (uint32_t j = 1; j < nrep; ++j) {
@@ -686,9 +702,10 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
 }
 
 // per warp: the leaf and monopole lists, 32 staged undecided nodes (float4
-// position + uint4 mask / node / image flag), the child-owner bytes
+// position + uint4 mask / node / image flag), the lanes' running sums (two
+// float4 each), the child-owner bytes
 template <bool ACC> constexpr size_t walk_smem_per_warp() {
-  return sizeof(Entry) * (CHUNK_L + chunk_m<ACC>()) + 32 * (sizeof(float4) + sizeof(uint4)) + 32;
+  return sizeof(Entry) * (CHUNK_L + chunk_m<ACC>()) + 32 * (sizeof(float4) + sizeof(uint4)) + 64 * sizeof(float4) + 32;
 }
 
 template <int MIN_BLOCKS, int TPW, bool ACC>
@@ -700,7 +717,9 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
   Entry* list_m = list_l + CHUNK_L;
   float4* rpos = reinterpret_cast<float4*>(list_m + chunk_m<ACC>());
   uint4* rmask = reinterpret_cast<uint4*>(rpos + 32);
-  uint8_t* owner = reinterpret_cast<uint8_t*>(rmask + 32);
+  float4* s0 = reinterpret_cast<float4*>(rmask + 32);
+  float4* s1 = s0 + 32;
+  uint8_t* owner = reinterpret_cast<uint8_t*>(s1 + 32);
   const int64_t gw = (int64_t)blockIdx.x * WALK_WARPS + wid;
   StackEntry* stk = reinterpret_cast<StackEntry*>(a.stack) + gw * STACK_ENTRIES;
   for (;;) {
@@ -727,7 +746,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
     // one call site: the group at once, or its targets one at a time
     const uint32_t walks = wide ? count : 1u;
     for (uint32_t t = 0; t < walks; ++t)
-      walk_targets<TPW, ACC>(a, wide ? first + t : first, wide ? 1u : count, list_l, list_m, owner, stk, rpos, rmask);
+      walk_targets<TPW, ACC>(a, wide ? first + t : first, wide ? 1u : count, list_l, list_m, owner, stk, rpos, rmask, s0,
+                             s1);
   }
 }
 
@@ -809,20 +829,21 @@ __global__ void k_deferred(WalkArgs a, uint32_t n_items) {
 
 }  // namespace
 
-// Variants of the walk: the register budget for 4, 5 or 6 resident blocks of
-// 4 warps per SM (TPM_WALK_BLOCKS) and 32 or 16 targets per warp
-// (TPM_WALK_TARGETS; with 16, two lanes share each target).
-static int env_choice(const char* name, int dflt, int a, int b, int c) {
+// Variants of the walk: the register budget for 5 to 8 resident blocks of 4
+// warps per SM (TPM_WALK_BLOCKS; 7 = 72 registers by default: walk 69.3 ms at
+// 6 blocks, 68.3 at 7, 69.3 at 8 on the 256^3 workload) and 32 or 16 targets
+// per warp (TPM_WALK_TARGETS; with 16, two lanes share each target).
+static int env_choice(const char* name, int dflt, int lo, int hi) {
   const char* e = getenv(name);
   const int v = e ? atoi(e) : dflt;
-  return (v == a || v == b || v == c) ? v : dflt;
+  return (v >= lo && v <= hi) ? v : dflt;
 }
 static int walk_blocks_variant() {
-  static int v = env_choice("TPM_WALK_BLOCKS", 6, 4, 5, 6);
+  static int v = env_choice("TPM_WALK_BLOCKS", 7, 5, 8);
   return v;
 }
 int walk_targets_per_warp() {
-  static int v = env_choice("TPM_WALK_TARGETS", 32, 32, 16, 32);
+  static int v = env_choice("TPM_WALK_TARGETS", 32, 16, 32) == 16 ? 16 : 32;
   return v;
 }
 
@@ -835,14 +856,20 @@ static int blocks_for() {
   return nb < 1 ? 1 : nb;
 }
 
-// the accurate mode has one variant (5 blocks per SM)
+// the accurate mode: 6 (default) or 5 blocks per SM (TPM_WALK_BLOCKS_ACC)
+static int walk_blocks_acc_variant() {
+  static int v = env_choice("TPM_WALK_BLOCKS_ACC", 6, 5, 6);
+  return v;
+}
 template <int T>
 static int blocks_t(bool accurate) {
-  if (accurate) return blocks_for<5, T, true>();
+  if (accurate) return walk_blocks_acc_variant() == 6 ? blocks_for<6, T, true>() : blocks_for<5, T, true>();
   switch (walk_blocks_variant()) {
-    case 4: return blocks_for<4, T, false>();
+    case 5: return blocks_for<5, T, false>();
+    case 7: return blocks_for<7, T, false>();
     case 6: return blocks_for<6, T, false>();
-    default: return blocks_for<5, T, false>();
+    case 8: return blocks_for<8, T, false>();
+    default: return blocks_for<7, T, false>();
   }
 }
 
@@ -853,14 +880,18 @@ int walk_blocks_per_sm(bool accurate) {
 template <int T>
 static void launch_t(const WalkArgs& a, int grid, cudaStream_t s) {
   if (a.accurate) {
-    k_walk<5, T, true><<<grid, WALK_THREADS, walk_smem_per_warp<true>() * WALK_WARPS, s>>>(a);
+    const size_t smem = walk_smem_per_warp<true>() * WALK_WARPS;
+    if (walk_blocks_acc_variant() == 6) k_walk<6, T, true><<<grid, WALK_THREADS, smem, s>>>(a);
+    else k_walk<5, T, true><<<grid, WALK_THREADS, smem, s>>>(a);
     return;
   }
   const size_t smem = walk_smem_per_warp<false>() * WALK_WARPS;
   switch (walk_blocks_variant()) {
-    case 4: k_walk<4, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    case 5: k_walk<5, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    case 7: k_walk<7, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
     case 6: k_walk<6, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
-    default: k_walk<5, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    case 8: k_walk<8, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    default: k_walk<7, T, false><<<grid, WALK_THREADS, smem, s>>>(a); break;
   }
 }
 

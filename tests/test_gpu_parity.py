@@ -312,8 +312,11 @@ def test_nonfinite_rejected():
 
 def test_memory_cap_refuses_cleanly():
     t = treepm()
-    s = t.TreePmSolver(16, 100.0, memory_cap_bytes=64 << 20)
-    b = small_box(64, 100.0, 1.0, 71)  # 262144 particles: beyond 64 MiB of buffers
+    # the handle's fixed buffers (the walk's per-warp stacks: 66 MB at 7
+    # resident blocks of 4 warps on 148 SMs) fit under the cap; the particle
+    # buffers of 128^3 particles do not
+    s = t.TreePmSolver(16, 100.0, memory_cap_bytes=128 << 20)
+    b = small_box(128, 100.0, 1.0, 71)
     with pytest.raises(t.TreePmError) as e:
         s.accelerations_for_indices(b.positions(), b.mass, 1e-4, 1.0, [0])
     assert e.value.code == 3
