@@ -21,8 +21,10 @@
 // in shared memory; the lanes evaluate the list against the group's targets
 // with each target's own final test fused into the pair kernel (a group of c
 // targets gives every target 32 / c lanes, each on a share of the entries).
-// The running per-target sums stay in shared memory between list flushes, so
-// the traversal keeps its registers (and more resident warps).  Any decision
+// The running per-target sums, the targets' positions and the group box stay
+// in shared memory (read where a flush, a refinement or a classification
+// needs them), so the traversal keeps its registers: 7 resident blocks per SM
+// at 72 registers.  Any decision
 // that falls inside a narrow band around r_cut is re-evaluated in float64
 // with the reference's exact expression, so the interaction set equals the
 // reference's.  Pair arithmetic is FP32: exact fixed-point differences split
@@ -288,7 +290,7 @@ __device__ __noinline__ void resolve_list(const WalkArgs& a, const Entry* L, int
 // registers across the traversal.
 template <bool ACC>
 __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nll, const Entry* Lm, int nlm, int lane,
-                                      uint32_t count, uint32_t first, const float* tf, float4* s0, float4* s1,
+                                      uint32_t count, uint32_t first, const float4* tfs, float4* s0, float4* s1,
                                       uint32_t& nexact, uint32_t& neval) {
   const uint32_t lanes = pair_lanes(lane, count);  // recomputed here: one register less across the traversal
   uint32_t nleaf = 0, nmono = 0;
@@ -296,8 +298,8 @@ __device__ __forceinline__ void flush(const WalkArgs& a, const Entry* Ll, int nl
   bool amb_any = false;
   neval += (uint32_t)(nll + nlm);
   const int t = lanes & 0xffu;
-  const float tx = __shfl_sync(0xffffffffu, tf[0], t), ty = __shfl_sync(0xffffffffu, tf[1], t);
-  const float tz = __shfl_sync(0xffffffffu, tf[2], t);
+  const float4 T = tfs[t];
+  const float tx = T.x, ty = T.y, tz = T.z;
   flush_list<false, ACC>(a, Ll, nll, lanes, tx, ty, tz, fx, fy, fz, nleaf, amb_any);
   flush_list<true, ACC>(a, Lm, nlm, lanes, tx, ty, tz, fx, fy, fz, nmono, amb_any);
   if (!ACC && amb_any) {
@@ -332,7 +334,8 @@ constexpr uint32_t INFO_MAC = 0x40000000u;  // opening angle undecided for the g
 // Walk the tree for targets [first, first + count) (count <= TPW) with one warp.
 template <int TPW, bool ACC>
 __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, Entry* Ll, Entry* Lm, uint8_t* owner,
-                             StackEntry* stk, float4* rpos, uint4* rmask, float4* s0, float4* s1) {
+                             StackEntry* stk, float4* rpos, uint4* rmask, float4* s0, float4* s1, float4* tfs,
+                             float4* gbox) {
   const int lane = threadIdx.x & 31;
   const int tgt = lane & (TPW - 1);  // this lane's target within the group
   const uint32_t p = first + ((uint32_t)tgt < count ? (uint32_t)tgt : 0u);
@@ -354,6 +357,16 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     bmin[d] = (float)mn * a.u_inv;
     bmax[d] = (float)mx * a.u_inv;
   }
+  // the group box, its origin and the targets' positions wait in shared
+  // memory (read when a node is classified, refined or flushed): registers
+  // for the traversal
+  tfs[lane] = make_float4(tf[0], tf[1], tf[2], 0.f);
+  if (lane == 0) {
+    gbox[0] = make_float4(bmin[0], bmin[1], bmin[2], 0.f);
+    gbox[1] = make_float4(bmax[0], bmax[1], bmax[2], 0.f);
+    reinterpret_cast<uint4*>(gbox)[2] = make_uint4(oq[0], oq[1], oq[2], 0u);
+  }
+  __syncwarp();
   const uint32_t mask0 = __ballot_sync(0xffffffffu, has && lane < TPW);  // bit t: target t
   s0[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
   s1[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -391,6 +404,10 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       // mode) twice that, which holds the whole cell
       const float h = (leaf && a.periodic) ? 0.f : (ACC && !leaf ? 2.f * hnode : hnode);
       const uint32_t cq[3] = {r0.x, r0.y, r0.z};
+      const float4 GL = gbox[0], GH = gbox[1];
+      const uint4 GO = reinterpret_cast<const uint4*>(gbox)[2];
+      const float bmin[3] = {GL.x, GL.y, GL.z}, bmax[3] = {GH.x, GH.y, GH.z};
+      const uint32_t oq[3] = {GO.x, GO.y, GO.z};
       // Per axis, the targets see the node at the minimum image of S - t for t
       // in [bmin, bmax]: bound min / max of |wrap(S - t)| over that interval
       // (images at 0 and +-L), then the AABB gap.
@@ -517,6 +534,8 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     }
     __syncwarp();
     const int namb = __popc(amb);
+    const float4 TF = tfs[lane];
+    const float tfl[3] = {TF.x, TF.y, TF.z};
     for (int j = 0; j < namb; ++j) {
       const float4 R = rpos[j];
       const uint4 M = rmask[j];
@@ -526,7 +545,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
         float s = 0.f;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          float dd = rc[d] - tf[d];
+          float dd = rc[d] - tfl[d];
           if (M.z) dd -= a.box_u * rintf(dd / a.box_u);  // top levels: the nearest periodic image
           const float ee = fmaxf(fabsf(dd) - R.w, 0.f);
           s = fmaf(ee, ee, s);
@@ -564,7 +583,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
     const bool done = sp == 0;
     if (done || nll > CHUNK_L - 32 || nlm > chunk_m<ACC>() - (ACC ? 64 : 32)) {
       if (nll + nlm > 0)
-        flush<ACC>(a, Ll, nll, Lm, nlm, lane, count, first, tf, s0, s1, nexact, neval);
+        flush<ACC>(a, Ll, nll, Lm, nlm, lane, count, first, tfs, s0, s1, nexact, neval);
       __syncwarp();
       nll = 0;
       nlm = 0;
@@ -630,6 +649,8 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
       const uint32_t am = __ballot_sync(0xffffffffu, accept);
       if (am) {  // one monopole entry for the accepting targets (same slot on every lane)
         if (lane == src) {
+          const uint4 GO = reinterpret_cast<const uint4*>(gbox)[2];
+          const uint32_t oq[3] = {GO.x, GO.y, GO.z};
           float4* dst = reinterpret_cast<float4*>(&Lm[nlm]);
           dst[0] = make_float4((float)rel32(w.x, oq[0], a.periodic) * a.u_inv,
                                (float)rel32(w.y, oq[1], a.periodic) * a.u_inv,
@@ -705,7 +726,7 @@ __device__ void walk_targets(const WalkArgs& a, uint32_t first, uint32_t count, 
 // position + uint4 mask / node / image flag), the lanes' running sums (two
 // float4 each), the child-owner bytes
 template <bool ACC> constexpr size_t walk_smem_per_warp() {
-  return sizeof(Entry) * (CHUNK_L + chunk_m<ACC>()) + 32 * (sizeof(float4) + sizeof(uint4)) + 64 * sizeof(float4) + 32;
+  return sizeof(Entry) * (CHUNK_L + chunk_m<ACC>()) + 32 * (sizeof(float4) + sizeof(uint4)) + 100 * sizeof(float4) + 32;
 }
 
 template <int MIN_BLOCKS, int TPW, bool ACC>
@@ -719,7 +740,9 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
   uint4* rmask = reinterpret_cast<uint4*>(rpos + 32);
   float4* s0 = reinterpret_cast<float4*>(rmask + 32);
   float4* s1 = s0 + 32;
-  uint8_t* owner = reinterpret_cast<uint8_t*>(s1 + 32);
+  float4* tfs = s1 + 32;   // 32 target positions
+  float4* gbox = tfs + 32; // group box corners and origin (3, padded to 4)
+  uint8_t* owner = reinterpret_cast<uint8_t*>(gbox + 4);
   const int64_t gw = (int64_t)blockIdx.x * WALK_WARPS + wid;
   StackEntry* stk = reinterpret_cast<StackEntry*>(a.stack) + gw * STACK_ENTRIES;
   for (;;) {
@@ -747,7 +770,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MIN_BLOCKS) k_walk(WalkArgs a) {
     const uint32_t walks = wide ? count : 1u;
     for (uint32_t t = 0; t < walks; ++t)
       walk_targets<TPW, ACC>(a, wide ? first + t : first, wide ? 1u : count, list_l, list_m, owner, stk, rpos, rmask, s0,
-                             s1);
+                             s1, tfs, gbox);
   }
 }
 
@@ -830,9 +853,9 @@ __global__ void k_deferred(WalkArgs a, uint32_t n_items) {
 }  // namespace
 
 // Variants of the walk: the register budget for 5 to 8 resident blocks of 4
-// warps per SM (TPM_WALK_BLOCKS; 7 = 72 registers by default: walk 69.3 ms at
-// 6 blocks, 68.3 at 7, 69.3 at 8 on the 256^3 workload) and 32 or 16 targets
-// per warp (TPM_WALK_TARGETS; with 16, two lanes share each target).
+// warps per SM (TPM_WALK_BLOCKS; 7 = 72 registers by default: walk 64.7 ms at
+// 7 blocks, 64.8 at 8 on the 256^3 workload) and 32 or 16 targets per warp
+// (TPM_WALK_TARGETS; with 16, two lanes share each target).
 static int env_choice(const char* name, int dflt, int lo, int hi) {
   const char* e = getenv(name);
   const int v = e ? atoi(e) : dflt;
@@ -856,14 +879,21 @@ static int blocks_for() {
   return nb < 1 ? 1 : nb;
 }
 
-// the accurate mode: 6 (default) or 5 blocks per SM (TPM_WALK_BLOCKS_ACC)
+// the accurate mode: 5, 6 or 7 (default; 71 registers, no spills: accurate walk 88.6 ms
+// at 6, 85.5 at 7 on the 256^3 workload) blocks per SM (TPM_WALK_BLOCKS_ACC)
 static int walk_blocks_acc_variant() {
-  static int v = env_choice("TPM_WALK_BLOCKS_ACC", 6, 5, 6);
+  static int v = env_choice("TPM_WALK_BLOCKS_ACC", 7, 5, 7);
   return v;
 }
 template <int T>
 static int blocks_t(bool accurate) {
-  if (accurate) return walk_blocks_acc_variant() == 6 ? blocks_for<6, T, true>() : blocks_for<5, T, true>();
+  if (accurate) {
+    switch (walk_blocks_acc_variant()) {
+      case 5: return blocks_for<5, T, true>();
+      case 6: return blocks_for<6, T, true>();
+      default: return blocks_for<7, T, true>();
+    }
+  }
   switch (walk_blocks_variant()) {
     case 5: return blocks_for<5, T, false>();
     case 7: return blocks_for<7, T, false>();
@@ -881,8 +911,11 @@ template <int T>
 static void launch_t(const WalkArgs& a, int grid, cudaStream_t s) {
   if (a.accurate) {
     const size_t smem = walk_smem_per_warp<true>() * WALK_WARPS;
-    if (walk_blocks_acc_variant() == 6) k_walk<6, T, true><<<grid, WALK_THREADS, smem, s>>>(a);
-    else k_walk<5, T, true><<<grid, WALK_THREADS, smem, s>>>(a);
+    switch (walk_blocks_acc_variant()) {
+      case 5: k_walk<5, T, true><<<grid, WALK_THREADS, smem, s>>>(a); break;
+      case 6: k_walk<6, T, true><<<grid, WALK_THREADS, smem, s>>>(a); break;
+      default: k_walk<7, T, true><<<grid, WALK_THREADS, smem, s>>>(a); break;
+    }
     return;
   }
   const size_t smem = walk_smem_per_warp<false>() * WALK_WARPS;
