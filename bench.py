@@ -235,6 +235,33 @@ def cpu_full(box, mesh, phys, threads):
     return t_pm + t_build + t_walk, dict(pm_s=t_pm, build_s=t_build, walk_s=t_walk)
 
 
+def cpu_kick_drift(box, threads):
+    """The O(N) part of a KDK step on the host, timed over every particle:
+    opening half kick, drift with the periodic wrap, closing half kick
+    (leapfrog.rs:72-91), float64, split over `threads` numpy workers (the
+    accelerations are stand-ins of the right shape: the arithmetic does not
+    depend on their values).  Seconds."""
+    from concurrent.futures import ThreadPoolExecutor
+    x = box.positions()
+    v = np.zeros_like(x)
+    acc = np.random.default_rng(0).standard_normal(x.shape)
+    L = box.box_size
+    bounds = np.linspace(0, box.n, threads + 1).astype(np.int64)
+
+    def part(i):
+        s = slice(bounds[i], bounds[i + 1])
+        xs, vs, a = x[s], v[s], acc[s]
+        vs += 0.5 * a
+        xs += 0.01 * vs
+        np.mod(xs, L, out=xs)
+        vs += 0.5 * a
+
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        t0 = time.perf_counter()
+        list(pool.map(part, range(threads)))
+        return time.perf_counter() - t0
+
+
 def run_reference(args):
     rank, world, _ = env_rank()
     if rank != 0:
@@ -243,11 +270,13 @@ def run_reference(args):
     from treepm import ics
     phys = ics.physics(box, mesh, a0)
     threads = os.cpu_count() or 1
-    times = []
+    times, kd = [], []
     for i in range(args.warmup + args.steps):
         t_force, info = cpu_sample(box, mesh, phys, args.cpu_targets, threads)
+        t_kd = cpu_kick_drift(box, threads)
         if i >= args.warmup:
-            times.append(2.0 * t_force)  # the reference evaluates the force twice per KDK step
+            times.append(2.0 * t_force + t_kd)  # the reference evaluates the force twice per KDK step
+            kd.append(t_kd)
     step_s = float(np.mean(times))
     value = box.n / step_s
     full = None
@@ -256,6 +285,7 @@ def run_reference(args):
         full = {"seconds": t_full, "extrapolated_seconds": step_s / 2.0, "ratio_full_over_extrapolated":
                 t_full / (step_s / 2.0), **finfo,
                 "note": "one force evaluation with every particle's walk (no extrapolation), after the timed steps"}
+    kd_s = float(np.mean(kd)) if kd else 0.0
     line = {
         "impl": "reference", "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
@@ -267,7 +297,8 @@ def run_reference(args):
                                     f"and full insertion-octree build over {box.n} particles, periodic walk of "
                                     f"{info['targets']} seeded targets (one run of consecutive particles in each of 64 strata) extrapolated "
                                     f"to all; 2 force evaluations "
-                                    f"per KDK step as leapfrog.rs:79,86")},
+                                    f"per KDK step as leapfrog.rs:79,86, plus the kick-drift-kick over all particles "
+                                    f"(numpy float64, {threads} threads, {kd_s * 1e3:.1f} ms per step)")},
         "full_force_evaluation": full,
         "e2e": {"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
