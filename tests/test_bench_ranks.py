@@ -59,3 +59,15 @@ def test_single_rank_max_is_identity():
     import bench
     assert bench.max_over_ranks(3.5, "cpu") == 3.5
     assert bench.whole_job_rate(10, 2, 4.0, 1) == 5.0
+
+
+
+def test_host_kick_drift_times_every_particle():
+    """The reference arm's O(N) step part runs over all particles in any
+    split of the host threads (more threads than particles included)."""
+    sys.path.insert(0, REPO)
+    import bench
+    from treepm import ics
+    box = ics.lattice_box(4, 100.0, 1.0, 3)  # 64 particles
+    for threads in (1, 3, 100):
+        assert bench.cpu_kick_drift(box, threads) > 0.0
